@@ -1,0 +1,338 @@
+"""ctypes binding of libcpg_b200.so (the C ABI declared in include/cpg.h).
+
+A thin host-side mirror of the reference's ``gpucpg::CpGen`` operator surface
+(gpucpg/gpucpg.cuh:119-431) for Python callers, tests and the benchmark:
+``CpGen.read_input``, ``levelize``, ``report_paths``, ``get_slacks``,
+``get_pfxt_nodes``, ``reset``, ``num_verts``, ``num_edges``.
+
+The CUDA path is the only compute path: if the shared library is missing the
+import fails loudly; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libcpg_b200.so")
+HEADER_PATH = os.path.join(os.path.dirname(_HERE), "include", "cpg.h")
+
+CPG_OK = 0
+STATUS_NAMES = {
+    0: "CPG_OK", 1: "CPG_ERR_INVALID", 2: "CPG_ERR_IO", 3: "CPG_ERR_OOM",
+    4: "CPG_ERR_CAPACITY", 5: "CPG_ERR_TIMEOUT", 6: "CPG_ERR_CUDA",
+    7: "CPG_ERR_STATE", 8: "CPG_ERR_NO_DEVICE",
+}
+DIV_REFERENCE = 0
+DIV_IEEE = 1
+FRONTIER_AUTO, FRONTIER_CSR, FRONTIER_BVSS = 0, 1, 2
+
+
+class CpgError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+class Options(C.Structure):
+    _fields_ = [
+        ("device", C.c_int32), ("stream", C.c_void_p), ("division", C.c_int32),
+        ("frontier", C.c_int32), ("hbm_budget_bytes", C.c_int64),
+        ("spin_limit", C.c_uint32), ("reserved", C.c_int32 * 8),
+    ]
+
+
+class PathNode(C.Structure):
+    _fields_ = [
+        ("level", C.c_int32), ("from_", C.c_int32), ("to", C.c_int32),
+        ("parent", C.c_int32), ("num_children", C.c_int32), ("slack", C.c_float),
+    ]
+
+
+PATH_NODE_DTYPE = np.dtype([
+    ("level", "<i4"), ("from", "<i4"), ("to", "<i4"), ("parent", "<i4"),
+    ("num_children", "<i4"), ("slack", "<f4"),
+])
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("sfxt_ms", C.c_double), ("pfxt_ms", C.c_double), ("select_ms", C.c_double),
+        ("paths_accepted", C.c_int64), ("items_generated", C.c_int64),
+        ("pending_peak", C.c_int64), ("bytes_reserved", C.c_int64),
+        ("phases", C.c_int32), ("rounds", C.c_int32), ("levels", C.c_int32),
+        ("kernel_launches", C.c_int32), ("split", C.c_float),
+        ("frontier_used", C.c_int32),
+    ]
+
+
+class GenParams(C.Structure):
+    _fields_ = [
+        ("seed", C.c_uint64), ("n_pins", C.c_int32), ("n_levels", C.c_int32),
+        ("n_first", C.c_int32), ("n_last", C.c_int32), ("level_span", C.c_int32),
+        ("degree_kind", C.c_int32), ("deg_lo", C.c_int32), ("deg_hi", C.c_int32),
+        ("deg_mean", C.c_double), ("deg_cap", C.c_int32), ("weight_kind", C.c_int32),
+        ("w_lo", C.c_float), ("w_hi", C.c_float), ("iw_lo", C.c_int32),
+        ("iw_hi", C.c_int32), ("add_virtual", C.c_int32),
+    ]
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `make -C gpu-cpg_b200` "
+            "(there is no CPU fallback)")
+    lib = C.CDLL(LIB_PATH)
+    H = C.c_void_p
+    P = C.POINTER
+    sig = {
+        "cpg_abi_version": (C.c_int32, []),
+        "cpg_status_string": (C.c_char_p, [C.c_int]),
+        "cpg_options_init": (None, [P(Options)]),
+        "cpg_create": (C.c_int, [P(H), P(Options)]),
+        "cpg_destroy": (C.c_int, [H]),
+        "cpg_last_error": (C.c_char_p, [H]),
+        "cpg_load_text": (C.c_int, [H, C.c_char_p, C.c_int32]),
+        "cpg_load_edges": (C.c_int, [H, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
+        "cpg_load_csr": (C.c_int, [H, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
+        "cpg_num_verts": (C.c_int64, [H]),
+        "cpg_num_edges": (C.c_int64, [H]),
+        "cpg_get_csr": (C.c_int, [H, C.c_void_p, C.c_void_p, C.c_void_p]),
+        "cpg_levelize": (C.c_int, [H]),
+        "cpg_update_delays": (C.c_int, [H, C.c_int64, C.c_void_p, C.c_void_p]),
+        "cpg_get_sfxt": (C.c_int, [H, C.c_void_p, C.c_void_p, C.c_void_p]),
+        "cpg_num_levels": (C.c_int32, [H]),
+        "cpg_report_paths": (C.c_int, [H, C.c_int64]),
+        "cpg_get_costs": (C.c_int, [H, C.c_int64, C.c_void_p, P(C.c_int64)]),
+        "cpg_get_paths": (C.c_int, [H, C.c_int64, C.c_void_p, P(C.c_int64)]),
+        "cpg_get_costs_device": (C.c_int, [H, P(C.c_void_p), P(C.c_int64)]),
+        "cpg_get_path_vertices": (C.c_int, [H, C.c_int64, C.c_void_p, C.c_int64, P(C.c_int64)]),
+        "cpg_reset": (C.c_int, [H]),
+        "cpg_get_stats": (C.c_int, [H, P(Stats)]),
+        "cpg_sync": (C.c_int, [H]),
+        "cpg_gen_params_init": (None, [P(GenParams)]),
+        "cpg_dag_generate": (C.c_int, [P(GenParams), P(C.c_void_p)]),
+        "cpg_dag_sizes": (C.c_int, [C.c_void_p, P(C.c_int32), P(C.c_int32)]),
+        "cpg_dag_edges": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+        "cpg_dag_write_text": (C.c_int, [C.c_void_p, C.c_char_p]),
+        "cpg_load_dag": (C.c_int, [H, C.c_void_p]),
+        "cpg_dag_free": (None, [C.c_void_p]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def _ptr(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+# ------------------------------------------------------------------ generator
+@dataclass
+class Dag:
+    n: int
+    src: np.ndarray
+    dst: np.ndarray
+    w: np.ndarray
+
+    @property
+    def m(self) -> int:
+        return int(self.src.size)
+
+
+def gen_params(**kw) -> GenParams:
+    p = GenParams()
+    lib.cpg_gen_params_init(C.byref(p))
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise KeyError(k)
+        setattr(p, k, v)
+    return p
+
+
+def generate(params: GenParams, text_path: str | None = None) -> Dag:
+    """Seeded levelised DAG (host-only; no GPU needed)."""
+    h = C.c_void_p()
+    st = lib.cpg_dag_generate(C.byref(params), C.byref(h))
+    if st != CPG_OK:
+        raise CpgError(st, "generator rejected the parameters")
+    try:
+        n, m = C.c_int32(), C.c_int32()
+        lib.cpg_dag_sizes(h, C.byref(n), C.byref(m))
+        src = np.empty(m.value, np.int32)
+        dst = np.empty(m.value, np.int32)
+        w = np.empty(m.value, np.float32)
+        lib.cpg_dag_edges(h, _ptr(src), _ptr(dst), _ptr(w))
+        if text_path is not None:
+            st = lib.cpg_dag_write_text(h, text_path.encode())
+            if st != CPG_OK:
+                raise CpgError(st, f"cannot write {text_path}")
+        return Dag(n.value, src, dst, w)
+    finally:
+        lib.cpg_dag_free(h)
+
+
+def write_text(dag: Dag, path: str) -> None:
+    """Reference text format: N, N name lines, '"u" -> "v", w;' per edge."""
+    with open(path, "w") as f:
+        f.write(f"{dag.n}\n")
+        f.write("".join(f'"{i}";\n' for i in range(dag.n)))
+        f.write("".join(f'"{u}" -> "{v}", {float(x):.9g};\n'
+                        for u, v, x in zip(dag.src.tolist(), dag.dst.tolist(), dag.w.tolist())))
+
+
+# ------------------------------------------------------------------ handle
+class CpGen:
+    """Mirror of gpucpg::CpGen over the C ABI (one CUDA stream per handle)."""
+
+    def __init__(self, device: int = 0, stream: int | None = None,
+                 division: int = DIV_REFERENCE, frontier: int = FRONTIER_AUTO,
+                 hbm_budget_bytes: int = 0, spin_limit: int = 0):
+        o = Options()
+        lib.cpg_options_init(C.byref(o))
+        o.device = device
+        o.stream = stream
+        o.division = division
+        o.frontier = frontier
+        o.hbm_budget_bytes = hbm_budget_bytes
+        o.spin_limit = spin_limit
+        self._h = C.c_void_p()
+        st = lib.cpg_create(C.byref(self._h), C.byref(o))
+        if st != CPG_OK:
+            raise CpgError(st, "cpg_create failed")
+
+    def close(self):
+        if self._h:
+            lib.cpg_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, st: int, what: str):
+        if st != CPG_OK:
+            msg = lib.cpg_last_error(self._h)
+            raise CpgError(st, f"{what}: {msg.decode() if msg else ''}")
+
+    # ingestion
+    def read_input(self, path: str, ignore_wgts: bool = False):
+        self._check(lib.cpg_load_text(self._h, path.encode(), int(ignore_wgts)), "read_input")
+
+    def load_edges(self, n, src, dst, w):
+        src = np.ascontiguousarray(src, np.int32)
+        dst = np.ascontiguousarray(dst, np.int32)
+        w = np.ascontiguousarray(w, np.float32)
+        self._check(lib.cpg_load_edges(self._h, int(n), int(src.size), _ptr(src), _ptr(dst), _ptr(w)),
+                    "load_edges")
+
+    def load_dag(self, dag: Dag):
+        self.load_edges(dag.n, dag.src, dag.dst, dag.w)
+
+    def load_csr(self, n, adjp, adjncy, w):
+        adjp = np.ascontiguousarray(adjp, np.int32)
+        adjncy = np.ascontiguousarray(adjncy, np.int32)
+        w = np.ascontiguousarray(w, np.float32)
+        self._check(lib.cpg_load_csr(self._h, int(n), int(adjncy.size), _ptr(adjp), _ptr(adjncy), _ptr(w)),
+                    "load_csr")
+
+    def num_verts(self) -> int:
+        return int(lib.cpg_num_verts(self._h))
+
+    def num_edges(self) -> int:
+        return int(lib.cpg_num_edges(self._h))
+
+    def get_csr(self):
+        n, m = self.num_verts(), self.num_edges()
+        adjp = np.empty(n + 1, np.int32)
+        adj = np.empty(m, np.int32)
+        w = np.empty(m, np.float32)
+        self._check(lib.cpg_get_csr(self._h, _ptr(adjp), _ptr(adj), _ptr(w)), "get_csr")
+        return adjp, adj, w
+
+    # suffix tree
+    def levelize(self):
+        self._check(lib.cpg_levelize(self._h), "levelize")
+
+    def update_delays(self, eids, w):
+        eids = np.ascontiguousarray(eids, np.int32)
+        w = np.ascontiguousarray(w, np.float32)
+        self._check(lib.cpg_update_delays(self._h, int(eids.size), _ptr(eids), _ptr(w)), "update_delays")
+
+    def get_sfxt(self):
+        n = self.num_verts()
+        dist = np.empty(n, np.int32)
+        succ = np.empty(n, np.int32)
+        lvl = np.empty(n, np.int32)
+        self._check(lib.cpg_get_sfxt(self._h, _ptr(dist), _ptr(succ), _ptr(lvl)), "get_sfxt")
+        return dist, succ, lvl
+
+    def num_levels(self) -> int:
+        return int(lib.cpg_num_levels(self._h))
+
+    # prefix tree
+    def report_paths(self, k: int, *unused):
+        """report_paths(k, ...): the extra reference parameters are accepted
+        and ignored (the method is fixed to levelize-then-relax + G-PathGen)."""
+        self._check(lib.cpg_report_paths(self._h, int(k)), "report_paths")
+
+    def get_slacks(self, k: int) -> np.ndarray:
+        out = np.empty(max(int(k), 0), np.float32)
+        n = C.c_int64()
+        self._check(lib.cpg_get_costs(self._h, int(k), _ptr(out), C.byref(n)), "get_slacks")
+        return out[: n.value]
+
+    def get_pfxt_nodes(self, k: int) -> np.ndarray:
+        out = np.empty(max(int(k), 0), PATH_NODE_DTYPE)
+        n = C.c_int64()
+        self._check(lib.cpg_get_paths(self._h, int(k), _ptr(out), C.byref(n)), "get_pfxt_nodes")
+        return out[: n.value]
+
+    def costs_device(self):
+        p = C.c_void_p()
+        n = C.c_int64()
+        self._check(lib.cpg_get_costs_device(self._h, C.byref(p), C.byref(n)), "costs_device")
+        return p.value, n.value
+
+    def path_vertices(self, i: int) -> np.ndarray:
+        ln = C.c_int64()
+        self._check(lib.cpg_get_path_vertices(self._h, int(i), None, 0, C.byref(ln)), "path_vertices")
+        out = np.empty(ln.value, np.int32)
+        self._check(lib.cpg_get_path_vertices(self._h, int(i), _ptr(out), ln.value, C.byref(ln)),
+                    "path_vertices")
+        return out
+
+    def reset(self):
+        self._check(lib.cpg_reset(self._h), "reset")
+
+    def stats(self) -> dict:
+        s = Stats()
+        self._check(lib.cpg_get_stats(self._h, C.byref(s)), "stats")
+        return {f: getattr(s, f) for f, _ in Stats._fields_}
+
+    def sync(self):
+        self._check(lib.cpg_sync(self._h), "sync")
+
+
+def header_symbols(path: str = HEADER_PATH) -> list[str]:
+    """Function names declared in include/cpg.h."""
+    import re
+    src = open(path).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(cpg_[a-z0-9_]+)\s*\(", src)))

@@ -1,0 +1,953 @@
+// C ABI and host orchestration of the critical path generator.
+//
+// Host side of the reference's CpGen::report_paths (gpucpg/gpucpg.cu:
+// 16910-21366) for LEVELIZE_THEN_RELAX + SHORT_LONG: the graph and its suffix
+// tree stay resident on the device across queries; each query raises a cost
+// split until at least K non-zero paths cost <= split (the reference's
+// SHORT_LONG stopping rule, 19134-20850), then selects and sorts the K
+// cheapest.  Device work is in sfxt.cu, pfxt.cu and select_sort.cu.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "cpg_internal.hpp"
+
+using namespace cpg;
+
+namespace {
+
+struct DevMem {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+constexpr unsigned int kDefaultSpinLimit = 1u << 24;
+
+}  // namespace
+
+struct cpg_handle {
+  cpg_options opts{};
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::string err;
+
+  // graph
+  bool has_graph = false;
+  HostGraph g;
+  std::vector<int32_t> srcs;
+  int32_t max_outdeg = 0;
+  int64_t big_total = 0;
+  DevMem d_adjp, d_edges, d_iadjp, d_iadj, d_srcs, d_big_off, d_big_tmp;
+
+  // suffix tree
+  bool sfxt_valid = false;
+  int32_t levels = 0;
+  int32_t dirty_level = -1;  // lowest level whose delays changed
+  std::vector<int32_t> h_level_of, h_succ;
+  bool h_sfxt_cached = false;
+  DevMem d_order, d_lvlp, d_level_of, d_dist, d_succ, d_dev_cnt, d_dev,
+      d_ht_root, d_ht_size, d_hnodes, d_pool_mark, d_deps, d_sctr;
+  unsigned long long hnode_cap = 0;
+
+  // query
+  unsigned long long cap_paths = 0, cap_front = 0, cap_pend = 0;
+  DevMem d_pcost, d_pparent, d_pfrom, d_pto, d_plevel, d_front0, d_front1,
+      d_pend0, d_pend1, d_pctr, d_selstate, d_selhist, d_counts, d_keys,
+      d_vals, d_sorthist, d_cnt, d_rank, d_out_cost, d_out_nodes;
+  int64_t n_result = 0;
+  unsigned long long n_paths = 0;
+  bool result_valid = false;
+
+  // staging
+  void* pinned = nullptr;
+  cudaEvent_t ev[6] = {};
+  cpg_stats stats{};
+};
+
+namespace {
+
+Status fail(cpg_handle* h, Status s, const std::string& msg) {
+  if (h) h->err = msg;
+  return s;
+}
+
+Status cuda_fail(cpg_handle* h, int e, const char* what) {
+  const cudaError_t ce = static_cast<cudaError_t>(e);
+  if (ce == cudaErrorMemoryAllocation)
+    return fail(h, CPG_ERR_OOM, std::string(what) + ": out of device memory");
+  return fail(h, CPG_ERR_CUDA,
+              std::string(what) + ": " + cudaGetErrorString(ce));
+}
+
+#define CK(expr, what)                                   \
+  do {                                                   \
+    const int _e = static_cast<int>(expr);               \
+    if (_e != cudaSuccess) return cuda_fail(h, _e, what); \
+  } while (0)
+
+cudaError_t ensure(DevMem& b, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  if (b.bytes >= bytes) return cudaSuccess;
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.bytes = 0;
+  cudaError_t e = cudaMalloc(&b.p, bytes);
+  if (e == cudaSuccess) b.bytes = bytes;
+  return e;
+}
+
+void release(DevMem& b) {
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.bytes = 0;
+}
+
+template <typename T>
+T* P(DevMem& b) {
+  return static_cast<T*>(b.p);
+}
+
+Status check_handle(cpg_handle* h) {
+  if (!h) return CPG_ERR_INVALID;
+  return CPG_OK;
+}
+
+// Upload a host CSR graph and size the suffix-tree buffers.
+Status upload_graph(cpg_handle* h) {
+  const HostGraph& g = h->g;
+  const size_t n = static_cast<size_t>(g.n), m = static_cast<size_t>(g.m);
+  CK(cudaSetDevice(h->device), "cudaSetDevice");
+  h->srcs.clear();
+  h->max_outdeg = 0;
+  std::vector<int32_t> big_off(n, -1);
+  int64_t big_total = 0;
+  for (size_t v = 0; v < n; ++v) {
+    const int32_t od = g.adjp[v + 1] - g.adjp[v];
+    h->max_outdeg = std::max(h->max_outdeg, od);
+    if (g.iadjp[v + 1] == g.iadjp[v]) h->srcs.push_back(static_cast<int32_t>(v));
+    if (od > kSmemRow) {
+      big_off[v] = static_cast<int32_t>(big_total);
+      big_total += od;
+    }
+  }
+  h->big_total = big_total;
+  std::vector<DevEdge> edges(m);
+  for (size_t e = 0; e < m; ++e) {
+    edges[e].head = g.adj[e];
+    edges[e].w = g.w[e];
+  }
+  CK(ensure(h->d_adjp, (n + 1) * 4), "alloc adjp");
+  CK(ensure(h->d_edges, m * sizeof(DevEdge)), "alloc edges");
+  CK(ensure(h->d_iadjp, (n + 1) * 4), "alloc iadjp");
+  CK(ensure(h->d_iadj, m * 4), "alloc iadj");
+  CK(ensure(h->d_srcs, h->srcs.size() * 4), "alloc srcs");
+  CK(ensure(h->d_big_off, n * 4), "alloc big_off");
+  CK(ensure(h->d_big_tmp, static_cast<size_t>(big_total) * sizeof(DevSidetrack)),
+     "alloc big rows");
+  cudaStream_t s = h->stream;
+  CK(cudaMemcpyAsync(h->d_adjp.p, g.adjp.data(), (n + 1) * 4, cudaMemcpyHostToDevice, s), "H2D adjp");
+  if (m) {
+    CK(cudaMemcpyAsync(h->d_edges.p, edges.data(), m * sizeof(DevEdge), cudaMemcpyHostToDevice, s), "H2D edges");
+    CK(cudaMemcpyAsync(h->d_iadj.p, g.iadj.data(), m * 4, cudaMemcpyHostToDevice, s), "H2D iadj");
+  }
+  CK(cudaMemcpyAsync(h->d_iadjp.p, g.iadjp.data(), (n + 1) * 4, cudaMemcpyHostToDevice, s), "H2D iadjp");
+  if (!h->srcs.empty())
+    CK(cudaMemcpyAsync(h->d_srcs.p, h->srcs.data(), h->srcs.size() * 4, cudaMemcpyHostToDevice, s), "H2D srcs");
+  if (n) CK(cudaMemcpyAsync(h->d_big_off.p, big_off.data(), n * 4, cudaMemcpyHostToDevice, s), "H2D big_off");
+  // suffix tree storage
+  CK(ensure(h->d_order, n * 4), "alloc order");
+  CK(ensure(h->d_lvlp, (n + 2) * 4), "alloc lvlp");
+  CK(ensure(h->d_level_of, n * 4), "alloc level_of");
+  CK(ensure(h->d_dist, n * 4), "alloc dist");
+  CK(ensure(h->d_succ, n * 4), "alloc succ");
+  CK(ensure(h->d_dev_cnt, n * 4), "alloc dev_cnt");
+  CK(ensure(h->d_dev, m * sizeof(DevSidetrack)), "alloc deviations");
+  CK(ensure(h->d_ht_root, n * 4), "alloc ht_root");
+  CK(ensure(h->d_ht_size, n * 4), "alloc ht_size");
+  CK(ensure(h->d_pool_mark, (n + 2) * 8), "alloc pool_mark");
+  CK(ensure(h->d_deps, n * 4), "alloc deps");
+  CK(ensure(h->d_sctr, sizeof(SfxtCounters)), "alloc sfxt counters");
+  if (h->hnode_cap == 0) h->hnode_cap = n * 10ull + 1024;
+  CK(ensure(h->d_hnodes, h->hnode_cap * sizeof(HeapNode)), "alloc chain heaps");
+  CK(cudaStreamSynchronize(s), "upload");
+  h->has_graph = true;
+  h->sfxt_valid = false;
+  h->h_sfxt_cached = false;
+  h->dirty_level = -1;
+  h->result_valid = false;
+  h->n_result = 0;
+  return CPG_OK;
+}
+
+Status load_edgelist(cpg_handle* h, const EdgeList& el) {
+  HostGraph g;
+  Status st = edges_to_csr(el, g, h->err);
+  if (st != CPG_OK) return st;
+  h->g = std::move(g);
+  return upload_graph(h);
+}
+
+Status run_sfxt(cpg_handle* h, int32_t start_level) {
+  const int n = h->g.n;
+  cudaStream_t s = h->stream;
+  for (int attempt = 0; attempt < 8; ++attempt) {
+    SfxtCounters c{};
+    if (start_level > 0) {
+      unsigned long long mark = 0;
+      CK(cudaMemcpy(&mark, P<unsigned long long>(h->d_pool_mark) + start_level, 8,
+                    cudaMemcpyDeviceToHost), "read pool mark");
+      c.hnode_used = mark;
+    }
+    CK(cudaMemcpyAsync(h->d_sctr.p, &c, sizeof(c), cudaMemcpyHostToDevice, s), "H2D sfxt counters");
+    SfxtParams p{};
+    p.n = n;
+    p.adjp = P<int32_t>(h->d_adjp);
+    p.edges = P<DevEdge>(h->d_edges);
+    p.iadjp = P<int32_t>(h->d_iadjp);
+    p.iadj = P<int32_t>(h->d_iadj);
+    p.order = P<int32_t>(h->d_order);
+    p.lvlp = P<int32_t>(h->d_lvlp);
+    p.level_of = P<int32_t>(h->d_level_of);
+    p.dist = P<int32_t>(h->d_dist);
+    p.succ = P<int32_t>(h->d_succ);
+    p.dev_cnt = P<int32_t>(h->d_dev_cnt);
+    p.dev = P<DevSidetrack>(h->d_dev);
+    p.ht_root = P<int32_t>(h->d_ht_root);
+    p.ht_size = P<int32_t>(h->d_ht_size);
+    p.hnodes = P<HeapNode>(h->d_hnodes);
+    p.hnode_cap = h->hnode_cap;
+    p.pool_mark = P<unsigned long long>(h->d_pool_mark);
+    p.deps = P<int32_t>(h->d_deps);
+    p.big_off = P<int32_t>(h->d_big_off);
+    p.big_tmp = P<DevSidetrack>(h->d_big_tmp);
+    p.ctr = P<SfxtCounters>(h->d_sctr);
+    p.start_level = start_level;
+    p.known_levels = h->levels;
+    p.spin_limit = h->opts.spin_limit ? h->opts.spin_limit : kDefaultSpinLimit;
+    CK(cudaEventRecord(h->ev[0], s), "event");
+    int grid = 0;
+    CK(launch_sfxt(p, h->device, s, &grid), "sfxt launch");
+    CK(cudaEventRecord(h->ev[1], s), "event");
+    h->stats.kernel_launches += 1;
+    SfxtCounters* out = static_cast<SfxtCounters*>(h->pinned);
+    CK(cudaMemcpyAsync(out, h->d_sctr.p, sizeof(SfxtCounters), cudaMemcpyDeviceToHost, s), "D2H sfxt counters");
+    CK(cudaStreamSynchronize(s), "sfxt");
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, h->ev[0], h->ev[1]);
+    h->stats.sfxt_ms = ms;
+    if (out->err == kDevTimeout)
+      return fail(h, CPG_ERR_TIMEOUT, "suffix tree: grid barrier wait ran out");
+    if (out->err == kDevCapacity) {
+      // chain heaps outgrew their pool: grow and rebuild from scratch
+      release(h->d_hnodes);
+      h->hnode_cap *= 2;
+      CK(ensure(h->d_hnodes, h->hnode_cap * sizeof(HeapNode)), "alloc chain heaps");
+      start_level = 0;
+      continue;
+    }
+    if (start_level == 0) h->levels = out->levels;
+    h->stats.levels = h->levels;
+    h->stats.frontier_used = CPG_FRONTIER_CSR;
+    h->sfxt_valid = true;
+    h->h_sfxt_cached = false;
+    h->dirty_level = -1;
+    return CPG_OK;
+  }
+  return fail(h, CPG_ERR_CAPACITY, "suffix tree: chain heap pool cannot grow");
+}
+
+Status cache_sfxt_host(cpg_handle* h) {
+  if (h->h_sfxt_cached) return CPG_OK;
+  const size_t n = h->g.n;
+  h->h_level_of.resize(n);
+  h->h_succ.resize(n);
+  if (n) {
+    CK(cudaMemcpy(h->h_level_of.data(), h->d_level_of.p, n * 4, cudaMemcpyDeviceToHost), "D2H levels");
+    CK(cudaMemcpy(h->h_succ.data(), h->d_succ.p, n * 4, cudaMemcpyDeviceToHost), "D2H succ");
+  }
+  h->h_sfxt_cached = true;
+  return CPG_OK;
+}
+
+Status ensure_sfxt(cpg_handle* h) {
+  if (!h->has_graph) return fail(h, CPG_ERR_STATE, "no graph loaded");
+  if (h->sfxt_valid) return CPG_OK;
+  if (h->dirty_level > 0 && h->levels > 0)
+    return run_sfxt(h, h->dirty_level);
+  return run_sfxt(h, 0);
+}
+
+struct Counts {
+  unsigned long long le, nz;
+};
+
+Status counts(cpg_handle* h, const float* a, unsigned long long n, unsigned stride,
+              unsigned int t_key, Counts& out) {
+  cudaStream_t s = h->stream;
+  unsigned long long* dc = P<unsigned long long>(h->d_counts);
+  unsigned int* tk = reinterpret_cast<unsigned int*>(dc + 2);
+  CK(cudaMemsetAsync(dc, 0, 16, s), "memset counts");
+  CK(cudaMemcpyAsync(tk, &t_key, 4, cudaMemcpyHostToDevice, s), "H2D key");
+  CK(launch_count_le(a, n, stride, tk, dc, s), "count");
+  h->stats.kernel_launches += 1;
+  unsigned long long* hc = static_cast<unsigned long long*>(h->pinned);
+  CK(cudaMemcpyAsync(hc, dc, 16, cudaMemcpyDeviceToHost, s), "D2H counts");
+  CK(cudaStreamSynchronize(s), "counts");
+  out.le = hc[0];
+  out.nz = hc[1];
+  return CPG_OK;
+}
+
+Status select_kth(cpg_handle* h, const float* a, unsigned long long na,
+                  unsigned sa, const float* b, unsigned long long nb,
+                  unsigned sb, unsigned long long k, int skip_zero,
+                  float& value) {
+  cudaStream_t s = h->stream;
+  int launches = 0;
+  CK(launch_select_kth(a, na, sa, b, nb, sb, k, skip_zero, h->d_selstate.p,
+                       P<unsigned int>(h->d_selhist), s, &launches),
+     "select");
+  h->stats.kernel_launches += launches;
+  unsigned int* hk = static_cast<unsigned int*>(h->pinned);
+  CK(cudaMemcpyAsync(hk, h->d_selstate.p, 4, cudaMemcpyDeviceToHost, s), "D2H select");
+  CK(cudaStreamSynchronize(s), "select");
+  value = key_float_host(*hk);
+  return CPG_OK;
+}
+
+float margin_of(float t, float root_abs) {
+  const float a = std::max(std::max(std::fabs(t), root_abs), 1.0f);
+  return a * 0x1p-16f;
+}
+
+enum { kRetry = 1000 };
+
+Status alloc_query(cpg_handle* h, unsigned long long k) {
+  const size_t cp = h->cap_paths, cf = h->cap_front, cpd = h->cap_pend;
+  const size_t need =
+      cp * 20 + 2 * cf * sizeof(Item) + 2 * cpd * sizeof(Item) + k * 4 * 4 +
+      cp * 4 + k * (4 + sizeof(cpg_path_node)) + 256 * ((k + 2047) / 2048) * 4;
+  if (h->opts.hbm_budget_bytes > 0 &&
+      static_cast<int64_t>(need) > h->opts.hbm_budget_bytes)
+    return fail(h, CPG_ERR_CAPACITY, "query needs more device memory than hbm_budget_bytes");
+  h->stats.bytes_reserved = static_cast<int64_t>(need);
+  CK(ensure(h->d_pcost, cp * 4), "alloc paths");
+  CK(ensure(h->d_pparent, cp * 4), "alloc paths");
+  CK(ensure(h->d_pfrom, cp * 4), "alloc paths");
+  CK(ensure(h->d_pto, cp * 4), "alloc paths");
+  CK(ensure(h->d_plevel, cp * 4), "alloc paths");
+  CK(ensure(h->d_front0, cf * sizeof(Item)), "alloc frontier");
+  CK(ensure(h->d_front1, cf * sizeof(Item)), "alloc frontier");
+  CK(ensure(h->d_pend0, cpd * sizeof(Item)), "alloc pending");
+  CK(ensure(h->d_pend1, cpd * sizeof(Item)), "alloc pending");
+  CK(ensure(h->d_pctr, sizeof(PfxtCounters)), "alloc counters");
+  CK(ensure(h->d_selstate, 64), "alloc select");
+  CK(ensure(h->d_selhist, 2048 * 4), "alloc select");
+  CK(ensure(h->d_counts, 64), "alloc counts");
+  CK(ensure(h->d_keys, 2 * k * 4), "alloc sort");
+  CK(ensure(h->d_vals, 2 * k * 4), "alloc sort");
+  CK(ensure(h->d_sorthist, 256 * ((k + 2047) / 2048) * 4), "alloc sort");
+  CK(ensure(h->d_cnt, 16), "alloc sort");
+  CK(ensure(h->d_rank, cp * 4), "alloc rank");
+  CK(ensure(h->d_out_cost, k * 4), "alloc output");
+  CK(ensure(h->d_out_nodes, k * sizeof(cpg_path_node)), "alloc output");
+  CK(cudaMemsetAsync(h->d_selhist.p, 0, 2048 * 4, h->stream), "memset hist");
+  return CPG_OK;
+}
+
+PathStore path_store(cpg_handle* h) {
+  PathStore ps;
+  ps.cost = P<float>(h->d_pcost);
+  ps.parent = P<int32_t>(h->d_pparent);
+  ps.from = P<int32_t>(h->d_pfrom);
+  ps.to = P<int32_t>(h->d_pto);
+  ps.level = P<int32_t>(h->d_plevel);
+  ps.cap = h->cap_paths;
+  return ps;
+}
+
+Status read_pctr(cpg_handle* h, PfxtCounters& c) {
+  PfxtCounters* hc = static_cast<PfxtCounters*>(h->pinned);
+  CK(cudaMemcpyAsync(hc, h->d_pctr.p, sizeof(PfxtCounters), cudaMemcpyDeviceToHost, h->stream), "D2H counters");
+  CK(cudaStreamSynchronize(h->stream), "counters");
+  c = *hc;
+  return CPG_OK;
+}
+
+// One attempt at a query with the current capacities.  Returns kRetry when a
+// bounded buffer overflowed.
+int try_query(cpg_handle* h, unsigned long long k) {
+  Status st = alloc_query(h, k);
+  if (st != CPG_OK) return st;
+  cudaStream_t s = h->stream;
+  PfxtCounters zero{};
+  CK(cudaMemcpyAsync(h->d_pctr.p, &zero, sizeof(zero), cudaMemcpyHostToDevice, s), "H2D counters");
+  PfxtCounters* dctr = P<PfxtCounters>(h->d_pctr);
+  Item* pend_in = P<Item>(h->d_pend0);
+  Item* pend_out = P<Item>(h->d_pend1);
+  CK(launch_seed_roots(P<int32_t>(h->d_srcs), static_cast<int32_t>(h->srcs.size()),
+                       P<int32_t>(h->d_dist), pend_in, dctr, s), "seed roots");
+  h->stats.kernel_launches += 1;
+  PfxtCounters c{};
+  st = read_pctr(h, c);
+  if (st != CPG_OK) return st;
+  unsigned long long n_pend = c.pend_out;
+  if (n_pend > h->cap_pend) return kRetry;
+  float root_abs = 0.f;
+  {
+    std::vector<Item> roots(n_pend);
+    if (n_pend)
+      CK(cudaMemcpy(roots.data(), pend_in, n_pend * sizeof(Item), cudaMemcpyDeviceToHost), "D2H roots");
+    for (const Item& r : roots) root_abs = std::max(root_abs, std::fabs(r.cost));
+  }
+  unsigned long long n_paths = 0;
+  const float* pcost = P<float>(h->d_pcost);
+  const float* pend_cost_in = reinterpret_cast<const float*>(pend_in);
+  float t = 0.f;
+  int phases = 0;
+  CK(cudaEventRecord(h->ev[2], s), "event");
+  while (n_pend > 0) {
+    Counts cp{}, cq{};
+    pend_cost_in = reinterpret_cast<const float*>(pend_in);
+    st = counts(h, pcost, n_paths, 1, 0xffffffffu, cp);
+    if (st != CPG_OK) return st;
+    st = counts(h, pend_cost_in, n_pend, 4, 0xffffffffu, cq);
+    if (st != CPG_OK) return st;
+    if (cp.nz + cq.nz >= k) {
+      st = select_kth(h, pcost, n_paths, 1, pend_cost_in, n_pend, 4, k, 1, t);
+    } else {
+      st = select_kth(h, pend_cost_in, n_pend, 4, nullptr, 0, 1, n_pend, 0, t);
+    }
+    if (st != CPG_OK) return st;
+    const float lim = t + margin_of(t, root_abs);
+    // promote pending items under the split, then close over the frontier
+    CK(cudaMemsetAsync(&dctr->frontier[0], 0, 3 * sizeof(unsigned long long), s), "memset");
+    CK(cudaMemsetAsync(&dctr->pend_out, 0, sizeof(unsigned long long), s), "memset");
+    CK(launch_promote(pend_in, n_pend, lim, P<Item>(h->d_front0), h->cap_front,
+                      pend_out, h->cap_pend, dctr, s), "promote");
+    ClosureParams cpar{};
+    cpar.g.adjp = P<int32_t>(h->d_adjp);
+    cpar.g.dist = P<int32_t>(h->d_dist);
+    cpar.g.dev_cnt = P<int32_t>(h->d_dev_cnt);
+    cpar.g.dev = P<DevSidetrack>(h->d_dev);
+    cpar.g.ht_root = P<int32_t>(h->d_ht_root);
+    cpar.g.hnodes = P<HeapNode>(h->d_hnodes);
+    cpar.g.division = h->opts.division;
+    cpar.ps = path_store(h);
+    cpar.front[0] = P<Item>(h->d_front0);
+    cpar.front[1] = P<Item>(h->d_front1);
+    cpar.front_cap = h->cap_front;
+    cpar.pend = pend_out;
+    cpar.pend_cap = h->cap_pend;
+    cpar.lim = lim;
+    cpar.ctr = dctr;
+    cpar.spin_limit = h->opts.spin_limit ? h->opts.spin_limit : kDefaultSpinLimit;
+    int grid = 0;
+    CK(launch_closure(cpar, h->device, s, &grid), "closure launch");
+    h->stats.kernel_launches += 2;
+    st = read_pctr(h, c);
+    if (st != CPG_OK) return st;
+    ++phases;
+    if (c.err == kDevTimeout)
+      return fail(h, CPG_ERR_TIMEOUT, "prefix tree: grid barrier wait ran out");
+    if (c.err == kDevCapacity || c.paths > h->cap_paths || c.pend_out > h->cap_pend)
+      return kRetry;
+    n_paths = c.paths;
+    n_pend = c.pend_out;
+    std::swap(pend_in, pend_out);
+    Counts le{};
+    st = counts(h, pcost, n_paths, 1, float_key_host(t), le);
+    if (st != CPG_OK) return st;
+    h->stats.pending_peak = std::max<int64_t>(h->stats.pending_peak, n_pend);
+    if (le.le >= k) break;
+  }
+  CK(cudaEventRecord(h->ev[3], s), "event");
+  // final: the k smallest non-zero accepted costs, sorted
+  Counts all{};
+  st = counts(h, pcost, n_paths, 1, 0xffffffffu, all);
+  if (st != CPG_OK) return st;
+  const unsigned long long k_out = std::min<unsigned long long>(k, all.nz);
+  CK(cudaEventRecord(h->ev[4], s), "event");
+  if (k_out > 0) {
+    float kth = 0.f;
+    st = select_kth(h, pcost, n_paths, 1, nullptr, 0, 1, k_out, 1, kth);
+    if (st != CPG_OK) return st;
+    int launches = 0;
+    CK(launch_emit_topk(path_store(h), n_paths, h->d_selstate.p, k_out,
+                        P<unsigned int>(h->d_keys), P<unsigned int>(h->d_vals),
+                        P<unsigned int>(h->d_sorthist),
+                        P<unsigned long long>(h->d_cnt), P<int32_t>(h->d_rank),
+                        P<float>(h->d_out_cost),
+                        P<cpg_path_node>(h->d_out_nodes), s, &launches),
+       "emit");
+    h->stats.kernel_launches += launches;
+  }
+  CK(cudaEventRecord(h->ev[5], s), "event");
+  CK(cudaStreamSynchronize(s), "query");
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, h->ev[2], h->ev[3]);
+  h->stats.pfxt_ms = ms;
+  cudaEventElapsedTime(&ms, h->ev[4], h->ev[5]);
+  h->stats.select_ms = ms;
+  h->stats.paths_accepted = static_cast<int64_t>(n_paths);
+  h->stats.items_generated = static_cast<int64_t>(n_paths + n_pend);
+  h->stats.phases = phases;
+  h->stats.rounds = c.rounds;
+  h->stats.split = t;
+  h->n_paths = n_paths;
+  h->n_result = static_cast<int64_t>(k_out);
+  h->result_valid = true;
+  return CPG_OK;
+}
+
+}  // namespace
+
+float cpg::key_float_host(unsigned int k) {
+  unsigned int u = (k & 0x80000000u) ? (k & 0x7fffffffu) : ~k;
+  float f;
+  std::memcpy(&f, &u, 4);
+  return f;
+}
+
+unsigned int cpg::float_key_host(float f) {
+  unsigned int u;
+  std::memcpy(&u, &f, 4);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+// ====================================================================== ABI
+
+extern "C" {
+
+int32_t cpg_abi_version(void) { return CPG_ABI_VERSION; }
+
+const char* cpg_status_string(cpg_status s) {
+  switch (s) {
+    case CPG_OK: return "ok";
+    case CPG_ERR_INVALID: return "invalid argument";
+    case CPG_ERR_IO: return "i/o error";
+    case CPG_ERR_OOM: return "out of memory";
+    case CPG_ERR_CAPACITY: return "capacity exceeded";
+    case CPG_ERR_TIMEOUT: return "device wait timed out";
+    case CPG_ERR_CUDA: return "cuda error";
+    case CPG_ERR_STATE: return "bad call order";
+    case CPG_ERR_NO_DEVICE: return "no cuda device";
+  }
+  return "unknown";
+}
+
+void cpg_options_init(cpg_options* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->division = CPG_DIV_REFERENCE;
+  o->frontier = CPG_FRONTIER_AUTO;
+}
+
+cpg_status cpg_create(cpg_handle** out, const cpg_options* opts) {
+  if (!out) return CPG_ERR_INVALID;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return CPG_ERR_NO_DEVICE;
+  }
+  cpg_handle* h = new (std::nothrow) cpg_handle();
+  if (!h) return CPG_ERR_OOM;
+  if (opts) h->opts = *opts;
+  else cpg_options_init(&h->opts);
+  if (h->opts.division != CPG_DIV_REFERENCE && h->opts.division != CPG_DIV_IEEE) {
+    delete h;
+    return CPG_ERR_INVALID;
+  }
+  h->device = h->opts.device;
+  if (h->device < 0 || h->device >= ndev) {
+    delete h;
+    return CPG_ERR_INVALID;
+  }
+  if (cudaSetDevice(h->device) != cudaSuccess) {
+    delete h;
+    return CPG_ERR_CUDA;
+  }
+  if (h->opts.stream) {
+    h->stream = static_cast<cudaStream_t>(h->opts.stream);
+  } else {
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      delete h;
+      return CPG_ERR_CUDA;
+    }
+    h->own_stream = true;
+  }
+  if (cudaMallocHost(&h->pinned, 4096) != cudaSuccess) {
+    if (h->own_stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return CPG_ERR_OOM;
+  }
+  for (auto& e : h->ev) cudaEventCreate(&e);
+  *out = h;
+  return CPG_OK;
+}
+
+cpg_status cpg_destroy(cpg_handle* h) {
+  if (!h) return CPG_ERR_INVALID;
+  cudaSetDevice(h->device);
+  cudaStreamSynchronize(h->stream);
+  DevMem* all[] = {&h->d_adjp, &h->d_edges, &h->d_iadjp, &h->d_iadj, &h->d_srcs,
+                   &h->d_big_off, &h->d_big_tmp, &h->d_order, &h->d_lvlp,
+                   &h->d_level_of, &h->d_dist, &h->d_succ, &h->d_dev_cnt,
+                   &h->d_dev, &h->d_ht_root, &h->d_ht_size, &h->d_hnodes,
+                   &h->d_pool_mark, &h->d_deps, &h->d_sctr, &h->d_pcost,
+                   &h->d_pparent, &h->d_pfrom, &h->d_pto, &h->d_plevel,
+                   &h->d_front0, &h->d_front1, &h->d_pend0, &h->d_pend1,
+                   &h->d_pctr, &h->d_selstate, &h->d_selhist, &h->d_counts,
+                   &h->d_keys, &h->d_vals, &h->d_sorthist, &h->d_cnt,
+                   &h->d_rank, &h->d_out_cost, &h->d_out_nodes};
+  for (DevMem* b : all) release(*b);
+  for (auto& e : h->ev)
+    if (e) cudaEventDestroy(e);
+  if (h->pinned) cudaFreeHost(h->pinned);
+  if (h->own_stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return CPG_OK;
+}
+
+const char* cpg_last_error(const cpg_handle* h) {
+  return h ? h->err.c_str() : "null handle";
+}
+
+cpg_status cpg_load_text(cpg_handle* h, const char* path, int32_t ignore_wgts) {
+  if (check_handle(h) != CPG_OK || !path) return CPG_ERR_INVALID;
+  EdgeList el;
+  Status st = read_text_graph(path, ignore_wgts != 0, el, h->err);
+  if (st != CPG_OK) return st;
+  return load_edgelist(h, el);
+}
+
+cpg_status cpg_load_edges(cpg_handle* h, int32_t n, int32_t m,
+                          const int32_t* src, const int32_t* dst,
+                          const float* w) {
+  if (check_handle(h) != CPG_OK || n < 0 || m < 0) return CPG_ERR_INVALID;
+  if (m > 0 && (!src || !dst || !w)) return fail(h, CPG_ERR_INVALID, "null edge buffer");
+  EdgeList el;
+  el.n = n;
+  el.src.assign(src, src + m);
+  el.dst.assign(dst, dst + m);
+  el.w.assign(w, w + m);
+  return load_edgelist(h, el);
+}
+
+cpg_status cpg_load_csr(cpg_handle* h, int32_t n, int32_t m,
+                        const int32_t* adjp, const int32_t* adjncy,
+                        const float* w) {
+  if (check_handle(h) != CPG_OK) return CPG_ERR_INVALID;
+  HostGraph g;
+  Status st = csr_to_graph(n, m, adjp, adjncy, w, g, h->err);
+  if (st != CPG_OK) return st;
+  h->g = std::move(g);
+  return upload_graph(h);
+}
+
+int64_t cpg_num_verts(const cpg_handle* h) { return h && h->has_graph ? h->g.n : 0; }
+int64_t cpg_num_edges(const cpg_handle* h) { return h && h->has_graph ? h->g.m : 0; }
+
+cpg_status cpg_get_csr(const cpg_handle* h, int32_t* adjp, int32_t* adjncy,
+                       float* w) {
+  if (!h) return CPG_ERR_INVALID;
+  if (!h->has_graph) return CPG_ERR_STATE;
+  if (adjp) std::memcpy(adjp, h->g.adjp.data(), (h->g.n + 1) * 4);
+  if (adjncy && h->g.m) std::memcpy(adjncy, h->g.adj.data(), h->g.m * 4);
+  if (w && h->g.m) std::memcpy(w, h->g.w.data(), h->g.m * 4);
+  return CPG_OK;
+}
+
+cpg_status cpg_levelize(cpg_handle* h) {
+  if (check_handle(h) != CPG_OK) return CPG_ERR_INVALID;
+  if (!h->has_graph) return fail(h, CPG_ERR_STATE, "no graph loaded");
+  CK(cudaSetDevice(h->device), "cudaSetDevice");
+  h->stats.kernel_launches = 0;
+  h->sfxt_valid = false;
+  return ensure_sfxt(h);
+}
+
+cpg_status cpg_update_delays(cpg_handle* h, int64_t count, const int32_t* eids,
+                             const float* w) {
+  if (check_handle(h) != CPG_OK || count < 0) return CPG_ERR_INVALID;
+  if (!h->has_graph) return fail(h, CPG_ERR_STATE, "no graph loaded");
+  if (count == 0) return CPG_OK;
+  if (!eids || !w) return fail(h, CPG_ERR_INVALID, "null delay buffer");
+  CK(cudaSetDevice(h->device), "cudaSetDevice");
+  int32_t lowest = INT32_MAX;
+  const bool have_levels = h->sfxt_valid || h->dirty_level > 0;
+  if (have_levels) {
+    Status st = cache_sfxt_host(h);
+    if (st != CPG_OK) return st;
+  }
+  // tail of each fan-out edge, by binary search over the CSR offsets
+  for (int64_t i = 0; i < count; ++i) {
+    const int32_t e = eids[i];
+    if (e < 0 || e >= h->g.m) return fail(h, CPG_ERR_INVALID, "edge id out of range");
+    h->g.w[e] = w[i];
+    if (have_levels) {
+      const auto it = std::upper_bound(h->g.adjp.begin(), h->g.adjp.end(), e);
+      const int32_t tail = static_cast<int32_t>(it - h->g.adjp.begin()) - 1;
+      const int32_t lv = h->h_level_of[tail];
+      if (lv >= 0) lowest = std::min(lowest, lv);
+    }
+  }
+  DevMem tmp_e, tmp_w;
+  CK(ensure(tmp_e, count * 4), "alloc delay update");
+  CK(ensure(tmp_w, count * 4), "alloc delay update");
+  CK(cudaMemcpy(tmp_e.p, eids, count * 4, cudaMemcpyHostToDevice), "H2D eids");
+  CK(cudaMemcpy(tmp_w.p, w, count * 4, cudaMemcpyHostToDevice), "H2D delays");
+  CK(launch_scatter_delays(P<DevEdge>(h->d_edges), P<int32_t>(tmp_e),
+                           P<float>(tmp_w), count, h->stream), "scatter delays");
+  CK(cudaStreamSynchronize(h->stream), "scatter delays");
+  release(tmp_e);
+  release(tmp_w);
+  // incremental rebuild from the lowest changed level (levels never change
+  // with delays); without levels a full rebuild follows
+  if (have_levels && lowest != INT32_MAX && lowest >= 1)
+    h->dirty_level = h->dirty_level > 0 ? std::min(h->dirty_level, lowest) : lowest;
+  else if (!(have_levels && lowest == INT32_MAX))
+    h->dirty_level = -1;
+  h->sfxt_valid = false;
+  h->h_sfxt_cached = false;
+  h->result_valid = false;
+  return CPG_OK;
+}
+
+cpg_status cpg_get_sfxt(cpg_handle* h, int32_t* dist, int32_t* succ,
+                        int32_t* level) {
+  if (check_handle(h) != CPG_OK) return CPG_ERR_INVALID;
+  CK(cudaSetDevice(h->device), "cudaSetDevice");
+  Status st = ensure_sfxt(h);
+  if (st != CPG_OK) return st;
+  const size_t n = h->g.n;
+  if (n == 0) return CPG_OK;
+  if (dist) CK(cudaMemcpy(dist, h->d_dist.p, n * 4, cudaMemcpyDeviceToHost), "D2H dist");
+  if (succ) CK(cudaMemcpy(succ, h->d_succ.p, n * 4, cudaMemcpyDeviceToHost), "D2H succ");
+  if (level) CK(cudaMemcpy(level, h->d_level_of.p, n * 4, cudaMemcpyDeviceToHost), "D2H level");
+  return CPG_OK;
+}
+
+int32_t cpg_num_levels(const cpg_handle* h) { return h ? h->levels : 0; }
+
+cpg_status cpg_report_paths(cpg_handle* h, int64_t k) {
+  if (check_handle(h) != CPG_OK || k < 0) return CPG_ERR_INVALID;
+  if (!h->has_graph) return fail(h, CPG_ERR_STATE, "no graph loaded");
+  if (k > (int64_t{1} << 30)) return fail(h, CPG_ERR_INVALID, "k too large");
+  CK(cudaSetDevice(h->device), "cudaSetDevice");
+  if (!h->sfxt_valid) h->stats.kernel_launches = 0;
+  Status st = ensure_sfxt(h);
+  if (st != CPG_OK) return st;
+  h->result_valid = false;
+  h->n_result = 0;
+  h->stats.pending_peak = 0;
+  h->stats.phases = 0;
+  h->stats.rounds = 0;
+  if (k == 0) {
+    h->result_valid = true;
+    return CPG_OK;
+  }
+  const unsigned long long uk = static_cast<unsigned long long>(k);
+  const unsigned long long nsrc = h->srcs.size();
+  h->cap_paths = std::max(h->cap_paths, std::max<unsigned long long>(4 * uk, 1 << 16) + nsrc);
+  h->cap_front = std::max(h->cap_front, std::max<unsigned long long>(2 * uk, 1 << 16));
+  h->cap_pend = std::max(h->cap_pend, std::max<unsigned long long>(8 * uk, 1 << 17) + nsrc);
+  for (int attempt = 0; attempt < 12; ++attempt) {
+    const int r = try_query(h, uk);
+    if (r == kRetry) {
+      h->cap_paths *= 2;
+      h->cap_front *= 2;
+      h->cap_pend *= 2;
+      continue;
+    }
+    return static_cast<cpg_status>(r);
+  }
+  return fail(h, CPG_ERR_CAPACITY, "prefix tree buffers cannot grow further");
+}
+
+cpg_status cpg_get_costs(const cpg_handle* hc, int64_t k, float* out,
+                         int64_t* n_out) {
+  cpg_handle* h = const_cast<cpg_handle*>(hc);
+  if (!h || k < 0) return CPG_ERR_INVALID;
+  if (!h->result_valid) return fail(h, CPG_ERR_STATE, "no result");
+  const int64_t n = std::min(k, h->n_result);
+  if (n_out) *n_out = n;
+  if (n > 0) {
+    if (!out) return fail(h, CPG_ERR_INVALID, "null output");
+    CK(cudaMemcpy(out, h->d_out_cost.p, n * 4, cudaMemcpyDeviceToHost), "D2H costs");
+  }
+  return CPG_OK;
+}
+
+cpg_status cpg_get_paths(const cpg_handle* hc, int64_t k, cpg_path_node* out,
+                         int64_t* n_out) {
+  cpg_handle* h = const_cast<cpg_handle*>(hc);
+  if (!h || k < 0) return CPG_ERR_INVALID;
+  if (!h->result_valid) return fail(h, CPG_ERR_STATE, "no result");
+  const int64_t n = std::min(k, h->n_result);
+  if (n_out) *n_out = n;
+  if (n > 0) {
+    if (!out) return fail(h, CPG_ERR_INVALID, "null output");
+    CK(cudaMemcpy(out, h->d_out_nodes.p, n * sizeof(cpg_path_node), cudaMemcpyDeviceToHost), "D2H paths");
+  }
+  return CPG_OK;
+}
+
+cpg_status cpg_get_costs_device(const cpg_handle* h, const float** d_costs,
+                                int64_t* n_out) {
+  if (!h || !d_costs) return CPG_ERR_INVALID;
+  if (!h->result_valid) return CPG_ERR_STATE;
+  *d_costs = static_cast<const float*>(h->d_out_cost.p);
+  if (n_out) *n_out = h->n_result;
+  return CPG_OK;
+}
+
+cpg_status cpg_get_path_vertices(cpg_handle* h, int64_t i, int32_t* verts,
+                                 int64_t cap, int64_t* len) {
+  if (check_handle(h) != CPG_OK || i < 0 || cap < 0) return CPG_ERR_INVALID;
+  if (!h->result_valid || i >= h->n_result) return fail(h, CPG_ERR_STATE, "no such result");
+  Status st = cache_sfxt_host(h);
+  if (st != CPG_OK) return st;
+  unsigned int idx = 0;
+  CK(cudaMemcpy(&idx, P<unsigned int>(h->d_vals) + i, 4, cudaMemcpyDeviceToHost), "D2H index");
+  // deviations from the leaf back to the root
+  std::vector<std::pair<int32_t, int32_t>> devs;
+  int32_t cur = static_cast<int32_t>(idx), src = -1;
+  for (int guard = 0; guard < (1 << 24); ++guard) {
+    int32_t par = 0, from = 0, to = 0;
+    CK(cudaMemcpy(&par, P<int32_t>(h->d_pparent) + cur, 4, cudaMemcpyDeviceToHost), "D2H path");
+    CK(cudaMemcpy(&from, P<int32_t>(h->d_pfrom) + cur, 4, cudaMemcpyDeviceToHost), "D2H path");
+    CK(cudaMemcpy(&to, P<int32_t>(h->d_pto) + cur, 4, cudaMemcpyDeviceToHost), "D2H path");
+    if (par < 0) {
+      src = to;
+      break;
+    }
+    devs.emplace_back(from, to);
+    cur = par;
+  }
+  std::reverse(devs.begin(), devs.end());
+  std::vector<int32_t> seq;
+  int32_t v = src;
+  size_t d = 0;
+  while (v >= 0) {
+    seq.push_back(v);
+    if (d < devs.size() && devs[d].first == v) {
+      v = devs[d].second;
+      ++d;
+    } else {
+      v = h->h_succ[v];
+    }
+    if (seq.size() > static_cast<size_t>(h->g.n) + 1)
+      return fail(h, CPG_ERR_STATE, "path walk did not terminate");
+  }
+  if (len) *len = static_cast<int64_t>(seq.size());
+  if (verts) {
+    const int64_t c = std::min<int64_t>(cap, seq.size());
+    std::memcpy(verts, seq.data(), c * 4);
+  }
+  return CPG_OK;
+}
+
+cpg_status cpg_reset(cpg_handle* h) {
+  if (check_handle(h) != CPG_OK) return CPG_ERR_INVALID;
+  h->sfxt_valid = false;
+  h->h_sfxt_cached = false;
+  h->dirty_level = -1;
+  h->result_valid = false;
+  h->n_result = 0;
+  h->stats = cpg_stats{};
+  return CPG_OK;
+}
+
+cpg_status cpg_get_stats(const cpg_handle* h, cpg_stats* out) {
+  if (!h || !out) return CPG_ERR_INVALID;
+  *out = h->stats;
+  return CPG_OK;
+}
+
+cpg_status cpg_sync(cpg_handle* h) {
+  if (check_handle(h) != CPG_OK) return CPG_ERR_INVALID;
+  CK(cudaStreamSynchronize(h->stream), "sync");
+  return CPG_OK;
+}
+
+// ---------------------------------------------------------------- generator
+
+struct cpg_dag {
+  EdgeList el;
+};
+
+void cpg_gen_params_init(cpg_gen_params* p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->seed = 1;
+  p->n_pins = 20000;
+  p->n_levels = 60;
+  p->n_first = 64;
+  p->n_last = 64;
+  p->level_span = 3;
+  p->degree_kind = 0;
+  p->deg_lo = 1;
+  p->deg_hi = 4;
+  p->deg_mean = 20.0;
+  p->deg_cap = 256;
+  p->weight_kind = 0;
+  p->w_lo = 0.1f;
+  p->w_hi = 10.0f;
+  p->iw_lo = 1;
+  p->iw_hi = 100;
+  p->add_virtual = 1;
+}
+
+cpg_status cpg_dag_generate(const cpg_gen_params* p, cpg_dag** out) {
+  if (!p || !out) return CPG_ERR_INVALID;
+  cpg_dag* d = new (std::nothrow) cpg_dag();
+  if (!d) return CPG_ERR_OOM;
+  std::string err;
+  Status st = generate_dag(*p, d->el, err);
+  if (st != CPG_OK) {
+    delete d;
+    return st;
+  }
+  *out = d;
+  return CPG_OK;
+}
+
+cpg_status cpg_dag_sizes(const cpg_dag* d, int32_t* n, int32_t* m) {
+  if (!d) return CPG_ERR_INVALID;
+  if (n) *n = d->el.n;
+  if (m) *m = static_cast<int32_t>(d->el.src.size());
+  return CPG_OK;
+}
+
+cpg_status cpg_dag_edges(const cpg_dag* d, int32_t* src, int32_t* dst, float* w) {
+  if (!d) return CPG_ERR_INVALID;
+  const size_t m = d->el.src.size();
+  if (src) std::memcpy(src, d->el.src.data(), m * 4);
+  if (dst) std::memcpy(dst, d->el.dst.data(), m * 4);
+  if (w) std::memcpy(w, d->el.w.data(), m * 4);
+  return CPG_OK;
+}
+
+cpg_status cpg_dag_write_text(const cpg_dag* d, const char* path) {
+  if (!d || !path) return CPG_ERR_INVALID;
+  std::string err;
+  return write_text_graph(d->el, path, err);
+}
+
+cpg_status cpg_load_dag(cpg_handle* h, const cpg_dag* d) {
+  if (check_handle(h) != CPG_OK || !d) return CPG_ERR_INVALID;
+  return load_edgelist(h, d->el);
+}
+
+void cpg_dag_free(cpg_dag* d) { delete d; }
+
+}  // extern "C"

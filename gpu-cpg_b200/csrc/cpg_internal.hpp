@@ -1,0 +1,227 @@
+// Internal declarations shared by the host orchestration (C++) and the CUDA
+// translation units.  Nothing here is part of the public ABI (include/cpg.h).
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/cpg.h"
+
+namespace cpg {
+
+using Status = cpg_status;
+
+// Fixed-point scale of the suffix distances: dist = sum of (int)(w * 10000.0f)
+// (SCALE_UP, gpucpg/gpucpg.cuh:34).
+constexpr int kScaleUp = 10000;
+
+// ---------------------------------------------------------------- host graph
+struct EdgeList {
+  int32_t n = 0;
+  std::vector<int32_t> src, dst;
+  std::vector<float> w;
+};
+
+struct HostGraph {
+  int32_t n = 0, m = 0;
+  std::vector<int32_t> adjp, adj;  // fan-out CSR, rows in file order
+  std::vector<float> w;
+  std::vector<int32_t> iadjp, iadj;  // fan-in CSR
+};
+
+Status read_text_graph(const char* path, bool ignore_wgts, EdgeList& out,
+                       std::string& err);
+Status edges_to_csr(const EdgeList& el, HostGraph& g, std::string& err);
+Status csr_to_graph(int32_t n, int32_t m, const int32_t* adjp,
+                    const int32_t* adjncy, const float* w, HostGraph& g,
+                    std::string& err);
+Status generate_dag(const cpg_gen_params& p, EdgeList& out, std::string& err);
+Status write_text_graph(const EdgeList& el, const char* path, std::string& err);
+
+// ---------------------------------------------------------------- device data
+// One fan-out edge: head vertex and delay, loaded as one 8-byte word.
+struct alignas(8) DevEdge {
+  int32_t head;
+  float w;
+};
+
+// One deviation ("sidetrack") edge (v, head) with head != succ[v]: the delay,
+// the head's fixed-point distance and the sort key (its cost increase).  Each
+// vertex's deviations are stored ascending by key in its own fan-out slots, so
+// the list is also a binary min-heap (children 2j+1, 2j+2).
+struct alignas(16) DevSidetrack {
+  int32_t head;
+  float w;
+  int32_t dist_head;
+  float key;
+};
+
+// Node of the persistent chain heap: the heap of vertex v holds, for every
+// vertex u on v's suffix chain that has deviations, u's cheapest deviation
+// key.  The heap of v shares every node but one root-to-leaf path with the
+// heap of succ[v].
+struct alignas(16) HeapNode {
+  int32_t vtx;
+  int32_t left;
+  int32_t right;
+  float key;
+};
+
+// A path-graph item: the path "parent + the j-th deviation of vertex
+// heap[node].vtx", or, when node <= -2, the root path that starts at source
+// -(node + 2).  cost is the path's cost.
+struct alignas(16) Item {
+  float cost;
+  int32_t parent;
+  int32_t node;
+  int32_t j;
+};
+
+struct GridBarrier {
+  unsigned int count;
+  unsigned int gen;
+};
+
+// Device error codes, written to a status word by kernels and mapped to
+// cpg_status on the host.
+enum DevErr : int {
+  kDevOk = 0,
+  kDevTimeout = 1,
+  kDevCapacity = 2,
+};
+
+struct SfxtCounters {
+  int tail;                  // order[] append cursor
+  int err;
+  int levels;
+  int pad;
+  unsigned long long hnode_used;
+  GridBarrier bar;
+};
+
+struct SfxtParams {
+  int32_t n;
+  const int32_t* adjp;
+  const DevEdge* edges;
+  const int32_t* iadjp;
+  const int32_t* iadj;
+  int32_t* order;
+  int32_t* lvlp;
+  int32_t* level_of;
+  int32_t* dist;
+  int32_t* succ;
+  int32_t* dev_cnt;
+  DevSidetrack* dev;
+  int32_t* ht_root;
+  int32_t* ht_size;
+  HeapNode* hnodes;
+  unsigned long long hnode_cap;
+  unsigned long long* pool_mark;  // per level: heap nodes in use at its start
+  int32_t* deps;
+  const int32_t* big_off;  // scratch offset of rows longer than kSmemRow
+  DevSidetrack* big_tmp;
+  SfxtCounters* ctr;
+  int32_t start_level;     // 0: full levelise + relax; > 0: relax from here
+  int32_t known_levels;    // level count when start_level > 0
+  unsigned int spin_limit;
+};
+
+constexpr int kSfxtThreads = 256;
+constexpr int kSmemRow = 256;  // deviation rows up to this length sort in smem
+
+// Launch the persistent SFXT kernel (cooperative).  Returns a cudaError_t.
+int launch_sfxt(const SfxtParams& p, int device, void* stream, int* grid_out);
+
+// ---------------------------------------------------------------- PFXT
+struct PfxtCounters {
+  int err;
+  int pad0;
+  unsigned long long paths;       // accepted paths (store cursor)
+  unsigned long long frontier[3]; // rotating round counters
+  unsigned long long pend_out;    // pending append cursor
+  unsigned long long generated;
+  int rounds;
+  int pad1;
+  GridBarrier bar;
+};
+
+struct PathStore {
+  float* cost;
+  int32_t* parent;
+  int32_t* from;
+  int32_t* to;
+  int32_t* level;
+  unsigned long long cap;
+};
+
+struct PfxtGraph {
+  const int32_t* adjp;
+  const int32_t* dist;
+  const int32_t* dev_cnt;
+  const DevSidetrack* dev;
+  const int32_t* ht_root;
+  const HeapNode* hnodes;
+  int32_t division;  // cpg_division
+};
+
+struct ClosureParams {
+  PfxtGraph g;
+  PathStore ps;
+  Item* front[2];
+  unsigned long long front_cap;
+  unsigned long long front_start;  // items already in front[0]
+  Item* pend;                      // pending output
+  unsigned long long pend_cap;
+  float lim;                       // accept items with cost <= lim
+  PfxtCounters* ctr;
+  unsigned int spin_limit;
+};
+
+int launch_closure(const ClosureParams& p, int device, void* stream,
+                   int* grid_out);
+
+// Seed root items for every source with a finite distance.
+int launch_seed_roots(const int32_t* srcs, int32_t n_srcs, const int32_t* dist,
+                      Item* pend, PfxtCounters* ctr, void* stream);
+
+// Move pending items with cost <= lim into the frontier, the rest into
+// pend_out.  Counts go to ctr->frontier[0] and ctr->pend_out.
+int launch_promote(const Item* pend_in, unsigned long long n_in, float lim,
+                   Item* front, unsigned long long front_cap, Item* pend_out,
+                   unsigned long long pend_cap, PfxtCounters* ctr,
+                   void* stream);
+
+// ---------------------------------------------------------------- select/sort
+size_t select_state_bytes();
+// k-th smallest (1-based) value among the union of a (stride sa floats) and b
+// (stride sb floats), zeros skipped if skip_zero.  *state receives the
+// orderable key of that value (first 4 bytes) and its rank among equal keys
+// (8-byte field at offset 8).  hist needs 2048 zeroed words.
+int launch_select_kth(const float* a, unsigned long long na, unsigned sa,
+                      const float* b, unsigned long long nb, unsigned sb,
+                      unsigned long long k, int skip_zero, void* state,
+                      unsigned int* hist, void* stream, int* launches);
+// out[0] += #(x != 0 && key(x) <= *t_key), out[1] += #(x != 0).
+int launch_count_le(const float* a, unsigned long long n, unsigned stride_f,
+                    const unsigned int* t_key, unsigned long long* out,
+                    void* stream);
+// Sorted emission of the k smallest non-zero accepted paths (state from
+// launch_select_kth over the accepted costs with k).  keys/vals: 2k words;
+// hist: 256*ceil(k/2048) words; rank_of: n_paths; cnt: 2 words.
+int launch_emit_topk(const PathStore& ps, unsigned long long n_paths,
+                     const void* state, unsigned long long k,
+                     unsigned int* keys, unsigned int* vals, unsigned int* hist,
+                     unsigned long long* cnt, int32_t* rank_of, float* out_cost,
+                     cpg_path_node* out_nodes, void* stream, int* launches);
+
+// Host copies of the orderable float key map (device versions live in
+// device_common.cuh).
+float key_float_host(unsigned int k);
+unsigned int float_key_host(float f);
+
+// Scatter new delays into the device fan-out edges.
+int launch_scatter_delays(DevEdge* edges, const int32_t* eids, const float* w,
+                          int64_t count, void* stream);
+
+}  // namespace cpg

@@ -1,0 +1,300 @@
+// Suffix tree (SFXT) for sm_100a: reverse levelisation, fixed-point relax,
+// successors, sorted deviation lists and persistent chain heaps, all in one
+// persistent cooperative kernel that walks the levels with a bounded grid
+// barrier between them (no host round trip per level).
+//
+// Reference behaviour reproduced (gpucpg/gpucpg.cu):
+//   levelize   bfs_td_step_privatized 2215-2283, loop 17642-17677: Kahn over
+//              the fan-in CSR, deps = out-degree, sinks are level 0
+//   relax      relax_bu_step 1167-1188: dist[v] = min dist[n] + (int)(w*10000)
+//   successor  update_successors_bu 2606-2628: largest n among the arg-mins
+// The deviation lists restate the reference's static deviation CSR
+// (tc_pfxt_candidates.cuh:713-750: every fan-out edge except the successor
+// edge, with its cost delta), sorted by delta.
+//
+// This file is compiled with --use_fast_math like the reference library.
+#include <climits>
+
+#include "device_common.cuh"
+
+namespace cpg {
+
+namespace {
+
+__device__ __forceinline__ bool heap_less(int va, float ka, int vb, float kb) {
+  return ka < kb || (ka == kb && va < vb);
+}
+
+// Cost increase of deviation (v, head) in delay units.  Exact integer and
+// delay parts are summed in double so ties between deviations stay ties.
+__device__ __forceinline__ float deviation_key(int dist_head, int dist_v,
+                                               float w) {
+  const double d = (static_cast<double>(dist_head) - static_cast<double>(dist_v)) +
+                   static_cast<double>(w) * 10000.0;
+  return static_cast<float>(d * 1e-4);
+}
+
+__device__ __forceinline__ int fixed_delay(float w) {
+  // relax_bu_step: const int wgt = owgts[e]*SCALE_UP;
+  const int wgt = w * kScaleUp;
+  return wgt;
+}
+
+// One warp builds vertex v at level lvl.
+__device__ void build_vertex(const SfxtParams& p, int v, int lvl,
+                             DevSidetrack* sbuf, bool do_kahn) {
+  const int lane = threadIdx.x & 31;
+  const int rb = p.adjp[v];
+  const int re = p.adjp[v + 1];
+  const int deg = re - rb;
+  int best = INT_MAX;
+  int s = -1;
+  if (lvl == 0) {
+    best = 0;  // sinks (out-degree 0) start at distance 0 (gpucpg.cu:17034-17038)
+  } else {
+    for (int e = rb + lane; e < re; e += 32) {
+      const DevEdge ed = p.edges[e];
+      const int c = static_cast<int>(static_cast<unsigned>(__ldcg(p.dist + ed.head)) +
+                                     static_cast<unsigned>(fixed_delay(ed.w)));
+      best = min(best, c);
+    }
+    best = warp_min_i(best);
+    for (int e = rb + lane; e < re; e += 32) {
+      const DevEdge ed = p.edges[e];
+      const int c = static_cast<int>(static_cast<unsigned>(__ldcg(p.dist + ed.head)) +
+                                     static_cast<unsigned>(fixed_delay(ed.w)));
+      if (c == best) s = max(s, ed.head);
+    }
+    s = warp_max_i(s);
+  }
+
+  // deviations: every fan-out edge whose head is not the successor and has a
+  // finite distance, in edge order, staged then ranked by key
+  const bool big = deg > kSmemRow;
+  DevSidetrack* stage = big ? (p.big_tmp + p.big_off[v]) : sbuf;
+  int cnt = 0;
+  float kmin = __int_as_float(0x7f800000);  // +inf
+  for (int base = rb; base < re; base += 32) {
+    const int e = base + lane;
+    bool valid = false;
+    DevSidetrack rec;
+    if (e < re) {
+      const DevEdge ed = p.edges[e];
+      const int dh = __ldcg(p.dist + ed.head);
+      valid = ed.head != s && dh != INT_MAX;
+      rec.head = ed.head;
+      rec.w = ed.w;
+      rec.dist_head = dh;
+      rec.key = deviation_key(dh, best, ed.w);
+    }
+    const unsigned bal = __ballot_sync(0xffffffffu, valid);
+    if (valid) {
+      stage[cnt + __popc(bal & lanemask_lt())] = rec;
+      kmin = fminf(kmin, rec.key);
+    }
+    cnt += __popc(bal);
+  }
+  __syncwarp();
+  for (int i = lane; i < cnt; i += 32) {
+    const DevSidetrack ri = stage[i];
+    int r = 0;
+    for (int j = 0; j < cnt; ++j) {
+      const float kj = stage[j].key;
+      r += (kj < ri.key) || (kj == ri.key && j < i);
+    }
+    p.dev[rb + r] = ri;
+  }
+  __syncwarp();
+  // warp-wide minimum key (the rank-0 deviation)
+  for (int o = 16; o > 0; o >>= 1) kmin = fminf(kmin, __shfl_xor_sync(0xffffffffu, kmin, o));
+
+  if (lane == 0) {
+    p.dist[v] = best;
+    p.succ[v] = s;
+    p.dev_cnt[v] = cnt;
+    const int base_root = s >= 0 ? __ldcg(p.ht_root + s) : -1;
+    const int base_size = s >= 0 ? __ldcg(p.ht_size + s) : 0;
+    if (cnt == 0) {
+      p.ht_root[v] = base_root;
+      p.ht_size[v] = base_size;
+    } else {
+      // persistent insert at position base_size+1 of a complete binary heap:
+      // copy the root-to-position path, carrying the larger element down
+      const unsigned pos = static_cast<unsigned>(base_size) + 1u;
+      const int depth = 31 - __clz(pos);
+      const unsigned long long a =
+          atomicAdd(&p.ctr->hnode_used, static_cast<unsigned long long>(depth + 1));
+      if (a + depth + 1 > p.hnode_cap) {
+        atomicCAS(&p.ctr->err, kDevOk, kDevCapacity);
+        p.ht_root[v] = -1;
+        p.ht_size[v] = 0;
+      } else {
+        int cv = v;
+        float ck = kmin;
+        int cur = base_root;
+        for (int d = depth - 1; d >= 0; --d) {
+          HeapNode old;
+          {
+            const int4 raw = __ldcg(reinterpret_cast<const int4*>(p.hnodes + cur));
+            old.vtx = raw.x;
+            old.left = raw.y;
+            old.right = raw.z;
+            old.key = __int_as_float(raw.w);
+          }
+          const int bit = (pos >> d) & 1u;
+          HeapNode nn;
+          if (heap_less(cv, ck, old.vtx, old.key)) {
+            nn.vtx = cv;
+            nn.key = ck;
+            cv = old.vtx;
+            ck = old.key;
+          } else {
+            nn.vtx = old.vtx;
+            nn.key = old.key;
+          }
+          const int next = static_cast<int>(a) + (depth - d);
+          nn.left = bit ? old.left : next;
+          nn.right = bit ? next : old.right;
+          p.hnodes[a + (depth - 1 - d)] = nn;
+          cur = bit ? old.right : old.left;
+        }
+        HeapNode leaf;
+        leaf.vtx = cv;
+        leaf.key = ck;
+        leaf.left = -1;
+        leaf.right = -1;
+        p.hnodes[a + depth] = leaf;
+        p.ht_root[v] = static_cast<int>(a);
+        p.ht_size[v] = static_cast<int>(pos);
+      }
+    }
+  }
+
+  if (do_kahn) {
+    // every fan-in neighbour loses one pending fan-out; the last one to
+    // reach zero joins the next level
+    const int ib = p.iadjp[v];
+    const int ie = p.iadjp[v + 1];
+    for (int base = ib; base < ie; base += 32) {
+      const int e = base + lane;
+      int u = -1;
+      bool ready = false;
+      if (e < ie) {
+        u = p.iadj[e];
+        ready = atomicSub(&p.deps[u], 1) == 1;
+      }
+      const int slot = warp_append(&p.ctr->tail, ready);
+      if (ready) {
+        p.order[slot] = u;
+        p.level_of[u] = lvl + 1;
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kSfxtThreads)
+sfxt_persistent_kernel(SfxtParams p) {
+  __shared__ DevSidetrack sbuf_all[kSfxtThreads / 32][kSmemRow];
+  const int warp_in_block = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  DevSidetrack* sbuf = sbuf_all[warp_in_block];
+  const int gwarp = blockIdx.x * (blockDim.x >> 5) + warp_in_block;
+  const int nwarps = gridDim.x * (blockDim.x >> 5);
+  const bool full = p.start_level == 0;
+
+  int beg, end, lvl;
+  if (full) {
+    // phase 0: reset per-vertex state, seed level 0 with the sinks
+    for (int base = blockIdx.x * blockDim.x; base < p.n;
+         base += gridDim.x * blockDim.x) {
+      const int v = base + threadIdx.x;
+      bool sink = false;
+      if (v < p.n) {
+        const int od = p.adjp[v + 1] - p.adjp[v];
+        p.deps[v] = od;
+        p.dist[v] = INT_MAX;
+        p.succ[v] = -1;
+        p.dev_cnt[v] = 0;
+        p.ht_root[v] = -1;
+        p.ht_size[v] = 0;
+        p.level_of[v] = od == 0 ? 0 : -1;
+        sink = od == 0;
+      }
+      const int slot = warp_append(&p.ctr->tail, sink);
+      if (sink) p.order[slot] = v;
+    }
+    if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit)) return;
+    beg = 0;
+    end = *reinterpret_cast<volatile int*>(&p.ctr->tail);
+    lvl = 0;
+  } else {
+    lvl = p.start_level;
+    beg = p.lvlp[lvl];
+    end = p.lvlp[lvl + 1];
+  }
+
+  while (beg < end) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      p.lvlp[lvl] = beg;
+      p.lvlp[lvl + 1] = end;
+      p.pool_mark[lvl] = *reinterpret_cast<volatile unsigned long long*>(&p.ctr->hnode_used);
+    }
+    for (int i = beg + gwarp; i < end; i += nwarps) {
+      build_vertex(p, __ldcg(p.order + i), lvl, sbuf, full);
+    }
+    (void)lane;
+    if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit)) return;
+    ++lvl;
+    beg = end;
+    if (full) {
+      end = *reinterpret_cast<volatile int*>(&p.ctr->tail);
+    } else {
+      end = lvl < p.known_levels ? p.lvlp[lvl + 1] : beg;
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    p.ctr->levels = lvl;
+    p.lvlp[lvl] = beg;
+  }
+}
+
+}  // namespace
+
+int launch_sfxt(const SfxtParams& p, int device, void* stream, int* grid_out) {
+  int sms = 0, per_sm = 0;
+  cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  if (e != cudaSuccess) return e;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sfxt_persistent_kernel,
+                                                    kSfxtThreads, 0);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) per_sm = 1;
+  int grid = sms * per_sm;
+  if (grid_out) *grid_out = grid;
+  SfxtParams pp = p;
+  void* args[] = {&pp};
+  return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(sfxt_persistent_kernel),
+                                     dim3(grid), dim3(kSfxtThreads), args, 0,
+                                     static_cast<cudaStream_t>(stream));
+}
+
+}  // namespace cpg
+
+namespace cpg {
+namespace {
+__global__ void scatter_delays_kernel(DevEdge* edges, const int32_t* eids,
+                                      const float* w, int64_t count) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < count) edges[eids[i]].w = w[i];
+}
+}  // namespace
+
+int launch_scatter_delays(DevEdge* edges, const int32_t* eids, const float* w,
+                          int64_t count, void* stream) {
+  if (count <= 0) return cudaSuccess;
+  const int threads = 256;
+  const int64_t blocks = (count + threads - 1) / threads;
+  scatter_delays_kernel<<<static_cast<unsigned>(blocks), threads, 0,
+                          static_cast<cudaStream_t>(stream)>>>(edges, eids, w, count);
+  return cudaGetLastError();
+}
+}  // namespace cpg

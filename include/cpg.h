@@ -1,0 +1,203 @@
+/*
+ * cpg.h -- C ABI of the B200-native critical path generator (libcpg_b200.so).
+ *
+ * The library reports the K lowest-cost source-to-sink paths of a timing DAG,
+ * the operation of the reference gpu-cpg library's C++ class gpucpg::CpGen
+ * (gpucpg/gpucpg.cuh:119-431).  The reference has no C ABI; each entry point
+ * below names the CpGen member (or the part of report_paths) it replaces.
+ * The header-only C++ shim include/gpucpg/cpgen.hpp rebuilds the CpGen surface
+ * on top of these calls.
+ *
+ * Conventions: every call returns a cpg_status; nothing exits or throws across
+ * the ABI; buffers passed in are copied (the caller keeps ownership); output
+ * buffers belong to the caller.  One handle must not be used from two threads
+ * at once; separate handles are independent.
+ */
+#ifndef CPG_B200_H
+#define CPG_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CPG_ABI_VERSION 1
+
+/* Replaces exit(1) in cudaCheckErrors / checkError_t (gpucpg.cu:87-98,
+ * 269-275) and the std::runtime_error throws of read_input (gpucpg.cu:457). */
+typedef enum {
+  CPG_OK = 0,
+  CPG_ERR_INVALID = 1,   /* bad argument or graph */
+  CPG_ERR_IO = 2,        /* file could not be read or parsed */
+  CPG_ERR_OOM = 3,       /* device or host allocation failed */
+  CPG_ERR_CAPACITY = 4,  /* a bounded buffer or the HBM budget was exceeded */
+  CPG_ERR_TIMEOUT = 5,   /* a bounded device-side wait ran out */
+  CPG_ERR_CUDA = 6,      /* CUDA runtime error */
+  CPG_ERR_STATE = 7,     /* call out of order (e.g. no graph loaded) */
+  CPG_ERR_NO_DEVICE = 8  /* no CUDA device / extension not usable */
+} cpg_status;
+
+/* Division used in the child-cost expression dist/10000.  The reference's
+ * device code is compiled with --use_fast_math (CMakeLists.txt:38); REFERENCE
+ * evaluates the same source expression under the same flag so the costs match
+ * the reference's G-PathGen bit for bit.  IEEE uses round-to-nearest division,
+ * matching the reference's host-side (SEQUENTIAL) arithmetic. */
+typedef enum { CPG_DIV_REFERENCE = 0, CPG_DIV_IEEE = 1 } cpg_division;
+
+/* Kahn step of the levelisation: CSR push with warp-aggregated enqueue, or the
+ * BVSS bit-packed pull (binary AND-popc tensor-core tiles where dense enough,
+ * scalar popc elsewhere).  AUTO picks by the measured frontier density. */
+typedef enum {
+  CPG_FRONTIER_AUTO = 0,
+  CPG_FRONTIER_CSR = 1,
+  CPG_FRONTIER_BVSS = 2
+} cpg_frontier;
+
+typedef struct {
+  int32_t device;           /* CUDA device ordinal */
+  void* stream;             /* cudaStream_t to run on; NULL = handle-owned */
+  int32_t division;         /* cpg_division */
+  int32_t frontier;         /* cpg_frontier */
+  int64_t hbm_budget_bytes; /* cap on per-query device memory; 0 = none */
+  uint32_t spin_limit;      /* grid-barrier poll limit; 0 = default */
+  int32_t reserved[8];
+} cpg_options;
+
+typedef struct cpg_handle cpg_handle;
+
+/* PfxtNode (gpucpg.cuh:74-107), same field order and 24-byte layout.
+ * parent indexes the list returned by cpg_get_paths (-1 for a root, or when
+ * the parent is not in the list); num_children is 0 as in G-PathGen. */
+typedef struct {
+  int32_t level;
+  int32_t from;
+  int32_t to;
+  int32_t parent;
+  int32_t num_children;
+  float slack;
+} cpg_path_node;
+
+typedef struct {
+  double sfxt_ms;          /* device time of the last SFXT build */
+  double pfxt_ms;          /* device time of the last enumeration */
+  double select_ms;        /* device time of the final select + sort + emit */
+  int64_t paths_accepted;  /* paths materialised by the closure */
+  int64_t items_generated; /* path-graph items written (accepted + pending) */
+  int64_t pending_peak;    /* largest pending pile */
+  int64_t bytes_reserved;  /* device bytes held for the last query */
+  int32_t phases;          /* split raises */
+  int32_t rounds;          /* closure rounds */
+  int32_t levels;          /* SFXT levels */
+  int32_t kernel_launches; /* kernels launched by the last levelize+report */
+  float split;             /* final split (cost threshold) */
+  int32_t frontier_used;   /* cpg_frontier actually used by the levelisation */
+} cpg_stats;
+
+/* ------------------------------------------------------------ lifecycle */
+void cpg_options_init(cpg_options* opts);
+/* CpGen::CpGen (gpucpg.cu:7400-7404). */
+cpg_status cpg_create(cpg_handle** out, const cpg_options* opts);
+/* CpGen::~CpGen. */
+cpg_status cpg_destroy(cpg_handle* h);
+const char* cpg_last_error(const cpg_handle* h);
+const char* cpg_status_string(cpg_status s);
+int32_t cpg_abi_version(void);
+
+/* ------------------------------------------------------------ ingestion */
+/* CpGen::read_input(filename, ignore_wgts) (gpucpg.cu:453-548). */
+cpg_status cpg_load_text(cpg_handle* h, const char* path, int32_t ignore_wgts);
+/* Same graph from an edge list in file order (no text round trip). */
+cpg_status cpg_load_edges(cpg_handle* h, int32_t n, int32_t m,
+                          const int32_t* src, const int32_t* dst,
+                          const float* w);
+/* Same graph from a fan-out CSR (_h_fanout_adjp/_adjncy/_wgts). */
+cpg_status cpg_load_csr(cpg_handle* h, int32_t n, int32_t m,
+                        const int32_t* adjp, const int32_t* adjncy,
+                        const float* w);
+/* CpGen::num_verts / num_edges (gpucpg.cu:286-292). */
+int64_t cpg_num_verts(const cpg_handle* h);
+int64_t cpg_num_edges(const cpg_handle* h);
+/* Copy the fan-out CSR back (host buffers of n+1, m, m; any may be NULL). */
+cpg_status cpg_get_csr(const cpg_handle* h, int32_t* adjp, int32_t* adjncy,
+                       float* w);
+
+/* ------------------------------------------------------------ suffix tree */
+/* LEVELIZE_THEN_RELAX + update_successors_bu (gpucpg.cu:17642-17963,
+ * 18421-18432): levels, fixed-point distances, successors and the sorted
+ * deviation heaps.  Always recomputes. */
+cpg_status cpg_levelize(cpg_handle* h);
+/* Re-sample delays of fan-out edges (indices in CSR order).  Only the levels
+ * at or above the lowest changed tail are recomputed at the next levelize. */
+cpg_status cpg_update_delays(cpg_handle* h, int64_t count, const int32_t* eids,
+                             const float* w);
+/* Per-vertex distance (fixed point, INT32_MAX if unreachable), successor
+ * (-1 at sinks) and reverse level (sinks 0, -1 if never levelled).  Host
+ * buffers of n entries; any may be NULL.  Runs cpg_levelize if needed. */
+cpg_status cpg_get_sfxt(cpg_handle* h, int32_t* dist, int32_t* succ,
+                        int32_t* level);
+int32_t cpg_num_levels(const cpg_handle* h);
+
+/* ------------------------------------------------------------ prefix tree */
+/* report_paths(k, ...) with LEVELIZE_THEN_RELAX and SHORT_LONG
+ * (gpucpg.cu:16910-21366): the k smallest non-zero path costs, sorted
+ * ascending, kept on the device until fetched.  Builds the suffix tree first
+ * if it is not current.  Fewer than k paths are returned if fewer exist. */
+cpg_status cpg_report_paths(cpg_handle* h, int64_t k);
+/* get_slacks(k) (gpucpg.cu:21409-21420): copies min(k, available) costs. */
+cpg_status cpg_get_costs(const cpg_handle* h, int64_t k, float* out,
+                         int64_t* n_out);
+/* get_pfxt_nodes(k) (gpucpg.cu:21422-21440). */
+cpg_status cpg_get_paths(const cpg_handle* h, int64_t k, cpg_path_node* out,
+                         int64_t* n_out);
+/* Device pointer of the last result's costs (valid until the next report or
+ * reset) and its length; lets callers keep results resident in HBM. */
+cpg_status cpg_get_costs_device(const cpg_handle* h, const float** d_costs,
+                                int64_t* n_out);
+/* Full vertex sequence of result path i (0-based rank): walks the parent
+ * links and suffix chains.  Writes at most cap vertices, *len = full length. */
+cpg_status cpg_get_path_vertices(cpg_handle* h, int64_t i, int32_t* verts,
+                                 int64_t cap, int64_t* len);
+/* CpGen::reset() (gpucpg.cuh:211-250): drops results and the suffix tree,
+ * keeps the graph. */
+cpg_status cpg_reset(cpg_handle* h);
+cpg_status cpg_get_stats(const cpg_handle* h, cpg_stats* out);
+/* Synchronise the handle's stream. */
+cpg_status cpg_sync(cpg_handle* h);
+
+/* ------------------------------------------------------------ generator */
+/* Seeded levelised timing DAG in the reference's text format conventions:
+ * explicit virtual super-source (id n_pins) and super-sink (id n_pins+1) with
+ * zero-delay edges when add_virtual is set.  Host-only. */
+typedef struct {
+  uint64_t seed;
+  int32_t n_pins;
+  int32_t n_levels;
+  int32_t n_first;        /* pins at level 0 */
+  int32_t n_last;         /* pins at the last level */
+  int32_t level_span;     /* edges go from level i to i+1..i+level_span */
+  int32_t degree_kind;    /* 0: uniform {deg_lo..deg_hi}; 1: geometric */
+  int32_t deg_lo, deg_hi;
+  double deg_mean;        /* geometric mean (support 1, 2, ...) */
+  int32_t deg_cap;
+  int32_t weight_kind;    /* 0: fp32 uniform [w_lo, w_hi]; 1: integer */
+  float w_lo, w_hi;
+  int32_t iw_lo, iw_hi;
+  int32_t add_virtual;
+} cpg_gen_params;
+
+typedef struct cpg_dag cpg_dag;
+void cpg_gen_params_init(cpg_gen_params* p);
+cpg_status cpg_dag_generate(const cpg_gen_params* p, cpg_dag** out);
+cpg_status cpg_dag_sizes(const cpg_dag* d, int32_t* n, int32_t* m);
+cpg_status cpg_dag_edges(const cpg_dag* d, int32_t* src, int32_t* dst,
+                         float* w);
+cpg_status cpg_dag_write_text(const cpg_dag* d, const char* path);
+cpg_status cpg_load_dag(cpg_handle* h, const cpg_dag* d);
+void cpg_dag_free(cpg_dag* d);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,111 @@
+/*
+ * CPU oracle for the critical-path-generation hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Nothing in the product (the gpu-cpg_b200 library,
+ * its C ABI or its C++ shim) links, loads or calls this code.  Only tests/,
+ * __graft_entry__.smoke() and bench.py's CPU-baseline leg use it, and only as
+ * the checker or the timed CPU port.
+ *
+ * It restates, in plain C, the reference gpu-cpg algorithm for this path
+ * (file:line cites are into the reference tree, gpucpg/gpucpg.cu unless noted):
+ *   - text ingestion                      CpGen::read_input        453-548
+ *   - reverse levelisation (CPU Kahn)     CpGen::levelize          21368-21407
+ *   - fixed-point relax                   relax_bu_step            1167-1188
+ *   - successor (max id among arg-mins)   update_successors_bu     2606-2628
+ *   - root seeding                        report_paths             18502-18520
+ *   - child cost, left-to-right fp32      expand_short_pile        3234-3306
+ *   - SEQUENTIAL priority-queue PFXT      report_paths             21230-21300
+ *   - closure at a split (the set GPG's   SHORT_LONG driver        19134-20850
+ *     short pile holds when it stops:
+ *     every path whose ancestors and itself cost <= split)
+ *   - zero-cost filter + ascending sort   report_paths             21323-21360
+ *
+ * Division: (float)dist / 10000 is IEEE round-to-nearest here (the reference's
+ * host-side root seeding uses the same); the reference's device kernels are
+ * built with --use_fast_math, so device-side quotients may differ in the last
+ * bit.  Parity against the device is therefore exact only where the device is
+ * asked for IEEE division, and within tolerance otherwise.
+ */
+#ifndef CPG_ORACLE_H
+#define CPG_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ORC_SCALE_UP 10000
+
+typedef struct {
+  int32_t n, m;
+  int32_t* adjp;   /* fan-out row offsets, n+1 */
+  int32_t* adj;    /* fan-out heads, m */
+  float* w;        /* fan-out delays, m */
+  int32_t* iadjp;  /* fan-in row offsets, n+1 */
+  int32_t* iadj;   /* fan-in tails, m */
+} orc_graph;
+
+/* PfxtNode (gpucpg.cuh:74-107) with a parent index valid in the output list. */
+typedef struct {
+  int32_t level, from, to, parent, num_children;
+  float slack;
+} orc_node;
+
+/* Parse the reference's text format ("N", N name lines, "u" -> "v"[, w];).
+ * Returns 0 on success, -1 on I/O error, -2 on a malformed line. */
+int orc_read_text(const char* path, int ignore_wgts, orc_graph* g);
+
+/* Build both CSRs from an edge list in file order (row order = file order). */
+int orc_build_csr(int32_t n, int32_t m, const int32_t* src, const int32_t* dst,
+                  const float* w, orc_graph* g);
+void orc_free_graph(orc_graph* g);
+
+/* Reverse levelisation: sinks are level 0.  order[] lists vertices level by
+ * level, lvlp[0..n_levels] are the level offsets.  Vertices never levelled
+ * (on or above a cycle) are left out.  Returns the number of levels. */
+int32_t orc_levelize(const orc_graph* g, int32_t* order, int32_t* lvlp,
+                     int32_t* level_of);
+
+/* dist[v] = min over out-edges (v,n) of dist[n] + (int)(w*10000.0f). */
+void orc_relax(const orc_graph* g, const int32_t* order, const int32_t* lvlp,
+               int32_t n_levels, int32_t* dist);
+/* succ[v] = max n with dist[v] == dist[n] + (int)(w*10000.0f), else -1. */
+void orc_successors(const orc_graph* g, const int32_t* dist, int32_t* succ);
+/* All three in one call. */
+int32_t orc_sfxt(const orc_graph* g, int32_t* dist, int32_t* succ,
+                 int32_t* level_of);
+
+/* The reference's SEQUENTIAL path: K pops of a min-heap, children pushed
+ * before the pop exactly as gpucpg.cu:21249-21296 does.  Writes at most k
+ * nodes sorted ascending with zero-cost nodes removed; returns the count. */
+int64_t orc_sequential(const orc_graph* g, const int32_t* dist,
+                       const int32_t* succ, int64_t k, orc_node* out);
+
+/* Closure at a split: the k smallest non-zero costs among all paths, found by
+ * expanding every path whose cost is <= split + margin with the reference's
+ * suffix-chain walk and raising the split until >= k paths cost <= split.
+ * Writes at most k nodes sorted ascending, parents indexed into out[] (-1 if
+ * the parent is a root or not in the list).  Returns the count, or -1 on
+ * allocation failure.  *split_out receives the final split. */
+int64_t orc_closure_topk(const orc_graph* g, const int32_t* dist,
+                         const int32_t* succ, int64_t k, orc_node* out,
+                         float* split_out);
+
+/* Deviation edges of every vertex: fan-out edges whose head is not the
+ * successor and whose head and tail distances are finite, with their cost
+ * delta dist_head/10000 + w - dist_tail/10000 (build_compact_static_deviation_csr,
+ * tc_pfxt_candidates.cuh:713-750).  offsets has n+1 entries; dsts/deltas at
+ * most m.  Returns the number of deviation edges. */
+int32_t orc_deviation_csr(int32_t n, const int32_t* adjp, const int32_t* adj,
+                          const float* w, const int32_t* succ,
+                          const int32_t* dist, int32_t* offsets, int32_t* dsts,
+                          float* deltas);
+
+/* Cost of one child, left to right as expand_short_pile writes it. */
+float orc_child_cost(float parent, int32_t dist_n, float w, int32_t dist_v);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

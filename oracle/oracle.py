@@ -1,0 +1,157 @@
+"""ctypes binding of the CPU oracle (oracle/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py, never by the product.  See cpg_oracle.h for the
+reference file:line each function restates.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+
+NODE_DTYPE = np.dtype([
+    ("level", "<i4"), ("from", "<i4"), ("to", "<i4"), ("parent", "<i4"),
+    ("num_children", "<i4"), ("slack", "<f4"),
+])
+
+
+class Graph(C.Structure):
+    _fields_ = [("n", C.c_int32), ("m", C.c_int32), ("adjp", C.c_void_p),
+                ("adj", C.c_void_p), ("w", C.c_void_p), ("iadjp", C.c_void_p),
+                ("iadj", C.c_void_p)]
+
+
+def build() -> None:
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def _lib():
+    if not os.path.exists(LIB):
+        build()
+    lib = C.CDLL(LIB)
+    G = C.POINTER(Graph)
+    lib.orc_read_text.argtypes = [C.c_char_p, C.c_int, G]
+    lib.orc_build_csr.argtypes = [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, G]
+    lib.orc_free_graph.argtypes = [G]
+    lib.orc_sfxt.argtypes = [G, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.orc_sfxt.restype = C.c_int32
+    lib.orc_sequential.argtypes = [G, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]
+    lib.orc_sequential.restype = C.c_int64
+    lib.orc_closure_topk.argtypes = [G, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
+                                     C.POINTER(C.c_float)]
+    lib.orc_closure_topk.restype = C.c_int64
+    lib.orc_deviation_csr.argtypes = [C.c_int32] + [C.c_void_p] * 8
+    lib.orc_deviation_csr.restype = C.c_int32
+    lib.orc_child_cost.argtypes = [C.c_float, C.c_int32, C.c_float, C.c_int32]
+    lib.orc_child_cost.restype = C.c_float
+    return lib
+
+
+_L = None
+
+
+def lib():
+    global _L
+    if _L is None:
+        _L = _lib()
+    return _L
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class OracleGraph:
+    def __init__(self, g: Graph):
+        self.g = g
+        self.dist = None
+        self.succ = None
+        self.level = None
+
+    @classmethod
+    def from_text(cls, path: str, ignore_wgts: bool = False) -> "OracleGraph":
+        g = Graph()
+        rc = lib().orc_read_text(path.encode(), int(ignore_wgts), C.byref(g))
+        if rc != 0:
+            raise IOError(f"oracle cannot read {path} ({rc})")
+        return cls(g)
+
+    @classmethod
+    def from_edges(cls, n, src, dst, w) -> "OracleGraph":
+        src = np.ascontiguousarray(src, np.int32)
+        dst = np.ascontiguousarray(dst, np.int32)
+        w = np.ascontiguousarray(w, np.float32)
+        g = Graph()
+        rc = lib().orc_build_csr(int(n), int(src.size), _p(src), _p(dst), _p(w), C.byref(g))
+        if rc != 0:
+            raise ValueError("bad edge list")
+        return cls(g)
+
+    def __del__(self):
+        try:
+            lib().orc_free_graph(C.byref(self.g))
+        except Exception:
+            pass
+
+    @property
+    def n(self):
+        return self.g.n
+
+    def csr(self):
+        n, m = self.g.n, self.g.m
+        adjp = np.ctypeslib.as_array(C.cast(self.g.adjp, C.POINTER(C.c_int32)), (n + 1,)).copy()
+        adj = np.ctypeslib.as_array(C.cast(self.g.adj, C.POINTER(C.c_int32)), (max(m, 1),))[:m].copy()
+        w = np.ctypeslib.as_array(C.cast(self.g.w, C.POINTER(C.c_float)), (max(m, 1),))[:m].copy()
+        return adjp, adj, w
+
+    def sfxt(self):
+        if self.dist is None:
+            n = self.g.n
+            self.dist = np.empty(max(n, 1), np.int32)
+            self.succ = np.empty(max(n, 1), np.int32)
+            self.level = np.empty(max(n, 1), np.int32)
+            lib().orc_sfxt(C.byref(self.g), _p(self.dist), _p(self.succ), _p(self.level))
+            self.dist, self.succ, self.level = self.dist[:n], self.succ[:n], self.level[:n]
+        return self.dist, self.succ, self.level
+
+    def sequential(self, k: int) -> np.ndarray:
+        d, s, _ = self.sfxt()
+        out = np.empty(max(k, 1), NODE_DTYPE)
+        n = lib().orc_sequential(C.byref(self.g), _p(d), _p(s), int(k), _p(out))
+        if n < 0:
+            raise MemoryError("oracle sequential failed")
+        return out[:n]
+
+    def closure_topk(self, k: int) -> tuple[np.ndarray, float]:
+        d, s, _ = self.sfxt()
+        out = np.empty(max(k, 1), NODE_DTYPE)
+        split = C.c_float()
+        n = lib().orc_closure_topk(C.byref(self.g), _p(d), _p(s), int(k), _p(out), C.byref(split))
+        if n < 0:
+            raise MemoryError("oracle closure failed")
+        return out[:n], split.value
+
+
+def deviation_csr(adjp, adj, w, succ, dist):
+    adjp = np.ascontiguousarray(adjp, np.int32)
+    adj = np.ascontiguousarray(adj, np.int32)
+    w = np.ascontiguousarray(w, np.float32)
+    succ = np.ascontiguousarray(succ, np.int32)
+    dist = np.ascontiguousarray(dist, np.int32)
+    n = adjp.size - 1
+    off = np.empty(n + 1, np.int32)
+    dsts = np.empty(max(adj.size, 1), np.int32)
+    deltas = np.empty(max(adj.size, 1), np.float32)
+    c = lib().orc_deviation_csr(n, _p(adjp), _p(adj), _p(w), _p(succ), _p(dist), _p(off),
+                                _p(dsts), _p(deltas))
+    return off, dsts[:c], deltas[:c]
+
+
+def child_cost(parent: float, dist_n: int, w: float, dist_v: int) -> float:
+    return lib().orc_child_cost(parent, dist_n, w, dist_v)

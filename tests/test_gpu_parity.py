@@ -1,0 +1,235 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle.
+
+Bars: suffix tree (distance, successor, level) bit-exact; path costs bit-exact
+in IEEE division mode and within rtol 1e-5 in the reference's fast-division
+mode; returned paths structurally valid and their costs reproducible from
+their vertex sequence.
+"""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import cases
+import cpg_b200
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-5  # fp32 delays, reference (fast) division
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _load(name):
+    return cases.load_case(name)
+
+
+def _gen(name, **over):
+    return cpg_b200.generate(cpg_b200.gen_params(**{**cases.CASES[name]["gen"], **over}))
+
+
+def _run(n, src, dst, w, k, division=cpg_b200.DIV_IEEE):
+    with cpg_b200.CpGen(division=division) as g:
+        g.load_edges(n, src, dst, w)
+        g.report_paths(k)
+        return g.get_slacks(k), g.get_pfxt_nodes(k), g.get_sfxt(), g.stats()
+
+
+SMALL_CASES = ["simple", "dac21_paper_example", "tv80_unit_wgts", "single20k_f32",
+               "single20k_int", "small_f32_s11", "small_f32_s12", "small_int_s13",
+               "small_int_s14"]
+
+
+@pytest.mark.parametrize("name", SMALL_CASES)
+def test_sfxt_bit_exact(name):
+    n, src, dst, w = _load(name)
+    og = oracle.OracleGraph.from_edges(n, src, dst, w)
+    od, os_, ol = og.sfxt()
+    with cpg_b200.CpGen() as g:
+        g.load_edges(n, src, dst, w)
+        g.levelize()
+        d, s, lvl = g.get_sfxt()
+        assert g.num_levels() == ol.max() + 1
+    np.testing.assert_array_equal(d, od)
+    np.testing.assert_array_equal(s, os_)
+    np.testing.assert_array_equal(lvl, ol)
+
+
+@pytest.mark.parametrize("name", SMALL_CASES)
+@pytest.mark.parametrize("k", [1, 100, 3000])
+def test_costs_ieee_bit_exact(name, k):
+    n, src, dst, w = _load(name)
+    og = oracle.OracleGraph.from_edges(n, src, dst, w)
+    want = og.closure_topk(k)[0]["slack"]
+    got, nodes, _, _ = _run(n, src, dst, w, k, cpg_b200.DIV_IEEE)
+    assert len(got) == len(want)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+@pytest.mark.parametrize("name", SMALL_CASES)
+def test_costs_reference_division_within_tolerance(name):
+    k = 5000
+    n, src, dst, w = _load(name)
+    og = oracle.OracleGraph.from_edges(n, src, dst, w)
+    want = og.closure_topk(k)[0]["slack"]
+    got, _, _, _ = _run(n, src, dst, w, k, cpg_b200.DIV_REFERENCE)
+    assert len(got) == len(want)
+    np.testing.assert_allclose(got, want, rtol=RTOL, atol=0)
+
+
+@pytest.mark.parametrize("name", ["small_f32_s11", "small_int_s13", "simple"])
+def test_against_reference_sequential_path(name):
+    """The reference's own CPU path (SEQUENTIAL, restated) at small K."""
+    k = 2000
+    n, src, dst, w = _load(name)
+    want = oracle.OracleGraph.from_edges(n, src, dst, w).sequential(k)["slack"]
+    got, _, _, _ = _run(n, src, dst, w, k, cpg_b200.DIV_IEEE)
+    assert len(got) == len(want)
+    np.testing.assert_allclose(got, want, rtol=RTOL, atol=0)
+
+
+def test_paths_are_valid_and_reproducible():
+    n, src, dst, w = _load("small_f32_s12")
+    k = 4000
+    og = oracle.OracleGraph.from_edges(n, src, dst, w)
+    d, s, _ = og.sfxt()
+    adjp, adj, ww = og.csr()
+    with cpg_b200.CpGen(division=cpg_b200.DIV_IEEE) as g:
+        g.load_edges(n, src, dst, w)
+        g.report_paths(k)
+        costs = g.get_slacks(k)
+        nodes = g.get_pfxt_nodes(k)
+        assert np.all(np.diff(costs) >= 0)
+        assert np.array_equal(nodes["slack"], costs)
+        for i in range(0, len(nodes), 37):
+            nd = nodes[i]
+            if nd["level"] == 0:
+                assert nd["parent"] == -1 and nd["from"] == -1
+            else:
+                p = nd["parent"]
+                assert p >= 0 and nodes[p]["level"] == nd["level"] - 1
+                row = adj[adjp[nd["from"]]:adjp[nd["from"] + 1]]
+                assert nd["to"] in row and nd["to"] != s[nd["from"]]
+            # rebuild the cost from the vertex sequence: the reference's
+            # left-to-right recurrence over the deviation edges
+            verts = g.path_vertices(i)
+            assert adjp[verts[-1]] == adjp[verts[-1] + 1]   # ends at a sink
+            c = np.float32(np.float32(d[verts[0]]) / np.float32(10000))
+            for a, b in zip(verts[:-1], verts[1:]):
+                if s[a] != b:
+                    e = adjp[a] + int(np.flatnonzero(adj[adjp[a]:adjp[a + 1]] == b)[0])
+                    c = oracle.child_cost(float(c), int(d[b]), float(ww[e]), int(d[a]))
+                    c = np.float32(c)
+            assert c == costs[i]
+
+
+def test_k_larger_than_path_count():
+    n, src, dst, w = _load("dac21_paper_example")
+    got, _, _, _ = _run(n, src, dst, w, 1000)
+    assert len(got) == 13
+
+
+def test_k_zero_and_empty_graph():
+    with cpg_b200.CpGen() as g:
+        g.load_edges(5, [], [], [])
+        g.report_paths(0)
+        assert g.get_slacks(10).size == 0
+        g.report_paths(10)        # five isolated vertices: zero-cost paths only
+        assert g.get_slacks(10).size == 0
+
+
+def test_zero_cost_paths_are_dropped():
+    # 0 -> 1 (0.0), 0 -> 2 (1.5), 1 -> 3 (0.0), 2 -> 3 (0.5): costs {0, 2}
+    got, _, _, _ = _run(4, [0, 0, 1, 2], [1, 2, 3, 3], [0.0, 1.5, 0.0, 0.5], 10)
+    assert got.tolist() == [np.float32(2.0)]
+
+
+def test_duplicate_edges_and_multiple_sources():
+    src = [0, 0, 0, 1, 2, 2, 3]
+    dst = [2, 2, 3, 3, 4, 4, 4]
+    w = [1.0, 2.0, 5.0, 1.0, 1.0, 3.0, 2.0]
+    og = oracle.OracleGraph.from_edges(5, src, dst, w)
+    want = og.closure_topk(100)[0]["slack"]
+    got, _, _, _ = _run(5, src, dst, w, 100)
+    assert np.array_equal(got, want)
+
+
+def test_unweighted_text_input(tmp_path):
+    # edges without a delay default to 1.0 (gpucpg.cu:485); ignore_wgts too
+    p = tmp_path / "g.txt"
+    p.write_text('4\n"0";\n"1";\n"2";\n"3";\n"0" -> "1";\n"0" -> "2", 2.5;\n'
+                 '"1" -> "3", 0.25;\n"2" -> "3";\n')
+    with cpg_b200.CpGen() as g:
+        g.read_input(str(p))
+        g.report_paths(10)
+        assert np.allclose(g.get_slacks(10), [1.25, 3.5])
+        g.read_input(str(p), ignore_wgts=True)
+        g.report_paths(10)
+        assert np.allclose(g.get_slacks(10), [2.0, 2.0])
+
+
+def test_repeat_queries_are_identical():
+    n, src, dst, w = _load("single20k_f32")
+    with cpg_b200.CpGen() as g:
+        g.load_edges(n, src, dst, w)
+        g.report_paths(5000)
+        a = g.get_slacks(5000)
+        g.report_paths(1000)
+        b = g.get_slacks(1000)
+        g.reset()
+        g.report_paths(5000)
+        c = g.get_slacks(5000)
+    assert np.array_equal(a, c)
+    assert np.array_equal(a[:1000], b)
+
+
+def test_incremental_delay_update_matches_fresh_build():
+    n, src, dst, w = _load("small_f32_s11")
+    rng = np.random.default_rng(5)
+    with cpg_b200.CpGen() as g:
+        g.load_edges(n, src, dst, w)
+        g.report_paths(2000)
+        adjp, adj, ww = g.get_csr()
+        eids = rng.choice(adj.size, size=adj.size // 100, replace=False).astype(np.int32)
+        neww = rng.uniform(0.1, 10.0, size=eids.size).astype(np.float32)
+        g.update_delays(eids, neww)
+        g.report_paths(2000)
+        inc = g.get_slacks(2000)
+        d_inc, s_inc, _ = g.get_sfxt()
+    ww = ww.copy()
+    ww[eids] = neww
+    with cpg_b200.CpGen() as g2:
+        g2.load_csr(n, adjp, adj, ww)
+        g2.report_paths(2000)
+        fresh = g2.get_slacks(2000)
+        d_f, s_f, _ = g2.get_sfxt()
+    assert np.array_equal(d_inc, d_f) and np.array_equal(s_inc, s_f)
+    assert np.array_equal(inc, fresh)
+
+
+def test_hbm_budget_is_enforced():
+    n, src, dst, w = _load("single20k_f32")
+    with cpg_b200.CpGen(hbm_budget_bytes=1 << 16) as g:
+        g.load_edges(n, src, dst, w)
+        with pytest.raises(cpg_b200.CpgError) as e:
+            g.report_paths(100000)
+        assert e.value.status == 4
+
+
+def test_cpp_shim_runs(tmp_path):
+    exe = tmp_path / "shim"
+    r = subprocess.run(["g++", "-std=c++17", "-O1", "-I", os.path.join(ROOT, "include"),
+                        os.path.join(ROOT, "tests", "cpp", "shim_example.cpp"),
+                        os.path.join(ROOT, "gpu-cpg_b200", "libcpg_b200.so"),
+                        "-Wl,-rpath," + os.path.join(ROOT, "gpu-cpg_b200"), "-o", str(exe)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    n, src, dst, w = _load("tv80_unit_wgts")
+    path = tmp_path / "tv80.txt"
+    cpg_b200.write_text(cpg_b200.Dag(n, src, dst, w), str(path))
+    out = subprocess.run([str(exe), str(path), "500"], capture_output=True, text=True)
+    assert out.returncode == 0, out.stderr
+    got = np.array([float(x) for x in out.stdout.split()], np.float32)
+    want = oracle.OracleGraph.from_edges(n, src, dst, w).closure_topk(500)[0]["slack"]
+    np.testing.assert_allclose(got, want, rtol=RTOL)

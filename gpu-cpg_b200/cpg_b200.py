@@ -29,6 +29,7 @@ STATUS_NAMES = {
 DIV_REFERENCE = 0
 DIV_IEEE = 1
 FRONTIER_AUTO, FRONTIER_CSR, FRONTIER_BVSS = 0, 1, 2
+ROOTS_REFERENCE, ROOTS_ALL = 0, 1
 
 
 class CpgError(RuntimeError):
@@ -41,7 +42,8 @@ class Options(C.Structure):
     _fields_ = [
         ("device", C.c_int32), ("stream", C.c_void_p), ("division", C.c_int32),
         ("frontier", C.c_int32), ("hbm_budget_bytes", C.c_int64),
-        ("spin_limit", C.c_uint32), ("reserved", C.c_int32 * 8),
+        ("spin_limit", C.c_uint32), ("root_seeding", C.c_int32),
+        ("reserved", C.c_int32 * 7),
     ]
 
 
@@ -195,7 +197,8 @@ class CpGen:
 
     def __init__(self, device: int = 0, stream: int | None = None,
                  division: int = DIV_REFERENCE, frontier: int = FRONTIER_AUTO,
-                 hbm_budget_bytes: int = 0, spin_limit: int = 0):
+                 hbm_budget_bytes: int = 0, spin_limit: int = 0,
+                 root_seeding: int = ROOTS_REFERENCE):
         o = Options()
         lib.cpg_options_init(C.byref(o))
         o.device = device
@@ -204,6 +207,7 @@ class CpGen:
         o.frontier = frontier
         o.hbm_budget_bytes = hbm_budget_bytes
         o.spin_limit = spin_limit
+        o.root_seeding = root_seeding
         self._h = C.c_void_p()
         st = lib.cpg_create(C.byref(self._h), C.byref(o))
         if st != CPG_OK:

@@ -400,11 +400,39 @@ int try_query(cpg_handle* h, unsigned long long k) {
   if (st != CPG_OK) return st;
   unsigned long long n_pend = c.pend_out;
   if (n_pend > h->cap_pend) return kRetry;
+  // roots back on the host, in source-id order, for the seeding rule
   float root_abs = 0.f;
   {
     std::vector<Item> roots(n_pend);
     if (n_pend)
       CK(cudaMemcpy(roots.data(), pend_in, n_pend * sizeof(Item), cudaMemcpyDeviceToHost), "D2H roots");
+    std::sort(roots.begin(), roots.end(),
+              [](const Item& a, const Item& b) { return a.node > b.node; });
+    if (h->opts.root_seeding == CPG_ROOTS_REFERENCE && !roots.empty()) {
+      // G-PathGen's initial split (gpucpg.cu:19136-19179): split = cost at
+      // sorted index (size_t)(0.005f*R); the short pile keeps only the first
+      // (int)(0.005f*R + 1) roots at or below it
+      const float perc = 0.005f;
+      const size_t r = roots.size();
+      std::vector<float> sorted(r);
+      for (size_t i = 0; i < r; ++i) sorted[i] = roots[i].cost;
+      std::sort(sorted.begin(), sorted.end());
+      const float split = sorted[static_cast<size_t>(perc * r)];
+      const int n_short = static_cast<int>(perc * r + 1);
+      std::vector<Item> kept;
+      int seen = 0;
+      for (const Item& it : roots) {
+        if (it.cost > split) kept.push_back(it);
+        else if (seen < n_short) {
+          ++seen;
+          kept.push_back(it);
+        }
+      }
+      roots.swap(kept);
+      n_pend = roots.size();
+      if (n_pend)
+        CK(cudaMemcpy(pend_in, roots.data(), n_pend * sizeof(Item), cudaMemcpyHostToDevice), "H2D roots");
+    }
     for (const Item& r : roots) root_abs = std::max(root_abs, std::fabs(r.cost));
   }
   unsigned long long n_paths = 0;

@@ -95,7 +95,7 @@ struct SfxtCounters {
   int tail;                  // order[] append cursor
   int err;
   int levels;
-  int pad;
+  int level_end;             // tail snapshot taken at each level barrier
   unsigned long long hnode_used;
   GridBarrier bar;
 };

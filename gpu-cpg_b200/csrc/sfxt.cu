@@ -223,9 +223,11 @@ sfxt_persistent_kernel(SfxtParams p) {
       const int slot = warp_append(&p.ctr->tail, sink);
       if (sink) p.order[slot] = v;
     }
-    if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit)) return;
+    if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit, &p.ctr->tail,
+                   &p.ctr->level_end))
+      return;
     beg = 0;
-    end = *reinterpret_cast<volatile int*>(&p.ctr->tail);
+    end = *reinterpret_cast<volatile int*>(&p.ctr->level_end);
     lvl = 0;
   } else {
     lvl = p.start_level;
@@ -243,11 +245,15 @@ sfxt_persistent_kernel(SfxtParams p) {
       build_vertex(p, __ldcg(p.order + i), lvl, sbuf, full);
     }
     (void)lane;
-    if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit)) return;
+    // the tail keeps growing as soon as the next level starts appending, so
+    // the level bound is the snapshot the last arriving block took
+    if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit, &p.ctr->tail,
+                   &p.ctr->level_end))
+      return;
     ++lvl;
     beg = end;
     if (full) {
-      end = *reinterpret_cast<volatile int*>(&p.ctr->tail);
+      end = *reinterpret_cast<volatile int*>(&p.ctr->level_end);
     } else {
       end = lvl < p.known_levels ? p.lvlp[lvl + 1] : beg;
     }

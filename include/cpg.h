@@ -55,6 +55,15 @@ typedef enum {
   CPG_FRONTIER_BVSS = 2
 } cpg_frontier;
 
+/* Root seeding.  REFERENCE reproduces G-PathGen's initial split
+ * (gpucpg.cu:19136-19179): with R reachable sources, the split is the cost at
+ * sorted index (size_t)(0.005f*R) and only the first (int)(0.005f*R+1) roots
+ * at or below it (in source-id order) are kept, so on graphs with many tied
+ * cheap sources some paths are never reported, exactly as in the reference.
+ * ALL seeds every reachable source: the exact K cheapest paths.  The two
+ * agree whenever the graph has a single source (e.g. a super-source). */
+typedef enum { CPG_ROOTS_REFERENCE = 0, CPG_ROOTS_ALL = 1 } cpg_root_seeding;
+
 typedef struct {
   int32_t device;           /* CUDA device ordinal */
   void* stream;             /* cudaStream_t to run on; NULL = handle-owned */
@@ -62,7 +71,8 @@ typedef struct {
   int32_t frontier;         /* cpg_frontier */
   int64_t hbm_budget_bytes; /* cap on per-query device memory; 0 = none */
   uint32_t spin_limit;      /* grid-barrier poll limit; 0 = default */
-  int32_t reserved[8];
+  int32_t root_seeding;     /* cpg_root_seeding */
+  int32_t reserved[7];
 } cpg_options;
 
 typedef struct cpg_handle cpg_handle;

@@ -390,7 +390,6 @@ static int closure(const orc_graph* g, const int32_t* dist, const int32_t* succ,
   acc->n = 0;
   *complete = 1;
   for (int32_t i = 0; i < ns; ++i) {
-    if (dist[srcs[i]] == INT_MAX) continue;
     orc_node r = {0, -1, srcs[i], -1, 0, dist_to_float(dist[srcs[i]])};
     if (!(r.slack <= lim)) {
       *complete = 0;
@@ -440,19 +439,67 @@ static int cmp_rank(const void* pa, const void* pb) {
   return (a->idx > b->idx) - (a->idx < b->idx);
 }
 
+static int cmp_float(const void* pa, const void* pb) {
+  float a = *(const float*)pa, b = *(const float*)pb;
+  return (a > b) - (a < b);
+}
+
+/* Roots in source-id order with finite distance; with ref_roots, the
+ * reference's initial-split truncation applied (gpucpg.cu:19136-19179). */
+static int32_t* seed_roots(const orc_graph* g, const int32_t* dist, int ref_roots,
+                           int32_t* ns_out) {
+  int32_t ns = 0;
+  int32_t* all = find_sources(g, &ns);
+  if (!all) return NULL;
+  int32_t r = 0;
+  for (int32_t i = 0; i < ns; ++i)
+    if (dist[all[i]] != INT_MAX) all[r++] = all[i];
+  if (ref_roots && r > 0) {
+    float* sorted = malloc(sizeof(float) * (size_t)r);
+    if (!sorted) {
+      free(all);
+      return NULL;
+    }
+    for (int32_t i = 0; i < r; ++i) sorted[i] = dist_to_float(dist[all[i]]);
+    qsort(sorted, (size_t)r, sizeof(float), cmp_float);
+    const float perc = 0.005f;
+    const float split = sorted[(size_t)(perc * r)];
+    const int32_t n_short = (int32_t)(perc * r + 1);
+    free(sorted);
+    int32_t kept = 0, short_seen = 0;
+    for (int32_t i = 0; i < r; ++i) {
+      float c = dist_to_float(dist[all[i]]);
+      if (c > split) {
+        all[kept++] = all[i];
+      } else if (short_seen < n_short) {
+        ++short_seen;
+        all[kept++] = all[i];
+      }
+    }
+    r = kept;
+  }
+  *ns_out = r;
+  return all;
+}
+
 int64_t orc_closure_topk(const orc_graph* g, const int32_t* dist,
                          const int32_t* succ, int64_t k, orc_node* out,
                          float* split_out) {
+  return orc_closure_topk_ex(g, dist, succ, k, 0, out, split_out);
+}
+
+int64_t orc_closure_topk_ex(const orc_graph* g, const int32_t* dist,
+                            const int32_t* succ, int64_t k, int ref_roots,
+                            orc_node* out, float* split_out) {
   if (k <= 0) return 0;
   int32_t ns = 0;
-  int32_t* srcs = find_sources(g, &ns);
+  int32_t* srcs = seed_roots(g, dist, ref_roots, &ns);
   if (!srcs) return -1;
   float c0 = INFINITY, dmax = 1.0f;
-  for (int32_t i = 0; i < ns; ++i)
-    if (dist[srcs[i]] != INT_MAX) {
-      float c = dist_to_float(dist[srcs[i]]);
-      if (c < c0) c0 = c;
-    }
+  for (int32_t i = 0; i < ns; ++i) {
+    float c = dist_to_float(dist[srcs[i]]);
+    if (c < c0) c0 = c;
+  }
   for (int32_t v = 0; v < g->n; ++v)
     if (dist[v] != INT_MAX && fabsf(dist_to_float(dist[v])) > dmax)
       dmax = fabsf(dist_to_float(dist[v]));

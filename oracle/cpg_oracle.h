@@ -92,6 +92,15 @@ int64_t orc_closure_topk(const orc_graph* g, const int32_t* dist,
                          const int32_t* succ, int64_t k, orc_node* out,
                          float* split_out);
 
+/* Same, with the reference G-PathGen's root seeding when ref_roots != 0:
+ * the roots are sorted, split = cost at index (size_t)(0.005f * R), the short
+ * pile is resized to (int)(0.005f * R + 1) after removing the roots above the
+ * split, so roots at or below the split beyond that count (in source-id
+ * order) are dropped (gpucpg.cu:19134-19179). */
+int64_t orc_closure_topk_ex(const orc_graph* g, const int32_t* dist,
+                            const int32_t* succ, int64_t k, int ref_roots,
+                            orc_node* out, float* split_out);
+
 /* Deviation edges of every vertex: fan-out edges whose head is not the
  * successor and whose head and tail distances are finite, with their cost
  * delta dist_head/10000 + w - dist_tail/10000 (build_compact_static_deviation_csr,

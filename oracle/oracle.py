@@ -46,6 +46,9 @@ def _lib():
     lib.orc_closure_topk.argtypes = [G, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
                                      C.POINTER(C.c_float)]
     lib.orc_closure_topk.restype = C.c_int64
+    lib.orc_closure_topk_ex.argtypes = [G, C.c_void_p, C.c_void_p, C.c_int64, C.c_int,
+                                        C.c_void_p, C.POINTER(C.c_float)]
+    lib.orc_closure_topk_ex.restype = C.c_int64
     lib.orc_deviation_csr.argtypes = [C.c_int32] + [C.c_void_p] * 8
     lib.orc_deviation_csr.restype = C.c_int32
     lib.orc_child_cost.argtypes = [C.c_float, C.c_int32, C.c_float, C.c_int32]
@@ -128,11 +131,14 @@ class OracleGraph:
             raise MemoryError("oracle sequential failed")
         return out[:n]
 
-    def closure_topk(self, k: int) -> tuple[np.ndarray, float]:
+    def closure_topk(self, k: int, ref_roots: bool = True) -> tuple[np.ndarray, float]:
+        """k cheapest non-zero paths; ref_roots applies the reference
+        G-PathGen's root seeding (the default, as the reference behaves)."""
         d, s, _ = self.sfxt()
         out = np.empty(max(k, 1), NODE_DTYPE)
         split = C.c_float()
-        n = lib().orc_closure_topk(C.byref(self.g), _p(d), _p(s), int(k), _p(out), C.byref(split))
+        n = lib().orc_closure_topk_ex(C.byref(self.g), _p(d), _p(s), int(k), int(ref_roots),
+                                      _p(out), C.byref(split))
         if n < 0:
             raise MemoryError("oracle closure failed")
         return out[:n], split.value

@@ -29,8 +29,8 @@ def _gen(name, **over):
     return cpg_b200.generate(cpg_b200.gen_params(**{**cases.CASES[name]["gen"], **over}))
 
 
-def _run(n, src, dst, w, k, division=cpg_b200.DIV_IEEE):
-    with cpg_b200.CpGen(division=division) as g:
+def _run(n, src, dst, w, k, division=cpg_b200.DIV_IEEE, roots=cpg_b200.ROOTS_REFERENCE):
+    with cpg_b200.CpGen(division=division, root_seeding=roots) as g:
         g.load_edges(n, src, dst, w)
         g.report_paths(k)
         return g.get_slacks(k), g.get_pfxt_nodes(k), g.get_sfxt(), g.stats()
@@ -84,9 +84,21 @@ def test_against_reference_sequential_path(name):
     k = 2000
     n, src, dst, w = _load(name)
     want = oracle.OracleGraph.from_edges(n, src, dst, w).sequential(k)["slack"]
-    got, _, _, _ = _run(n, src, dst, w, k, cpg_b200.DIV_IEEE)
+    got, _, _, _ = _run(n, src, dst, w, k, cpg_b200.DIV_IEEE, cpg_b200.ROOTS_ALL)
     assert len(got) == len(want)
     np.testing.assert_allclose(got, want, rtol=RTOL, atol=0)
+
+
+@pytest.mark.parametrize("name", ["tv80_unit_wgts", "simple"])
+def test_all_roots_mode_is_exact(name):
+    """Seeding every source gives the exact K cheapest paths (the reference's
+    G-PathGen drops tied cheap roots on multi-source graphs)."""
+    k = 5000
+    n, src, dst, w = _load(name)
+    og = oracle.OracleGraph.from_edges(n, src, dst, w)
+    want = og.closure_topk(k, ref_roots=False)[0]["slack"]
+    got, _, _, _ = _run(n, src, dst, w, k, cpg_b200.DIV_IEEE, cpg_b200.ROOTS_ALL)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
 
 
 def test_paths_are_valid_and_reproducible():

@@ -125,22 +125,26 @@ GOLD = os.path.join(os.path.dirname(__file__), "golden", "ref_goldens.npz")
 
 @pytest.mark.skipif(not os.path.exists(GOLD), reason="reference goldens not packed")
 def test_oracle_against_reference_goldens():
+    """The oracle reproduces the reference's own outputs, run on a B200: the
+    suffix tree bit for bit, and G-PathGen's costs within the fast-division
+    tolerance (the oracle divides in IEEE, the reference's device code with
+    --use_fast_math)."""
     z = np.load(GOLD)
-    checked = 0
+    sfxt_checked = costs_checked = 0
     for name, c in cases.CASES.items():
-        if c.get("large"):
-            continue
-        key = f"{name}/sfxt_dist"
-        if key not in z:
+        if c.get("large") or f"{name}/sfxt_dist" not in z:
             continue
         g = _graph(name)
         d, s, _ = g.sfxt()
         np.testing.assert_array_equal(d, z[f"{name}/sfxt_dist"])
         np.testing.assert_array_equal(s, z[f"{name}/sfxt_succ"])
-        k = c["ks"][0]
+        sfxt_checked += 1
+        if f"{name}/costs" not in z:
+            continue
         ref = z[f"{name}/costs"]
+        k = int(z[f"{name}/k"])
         clo = g.closure_topk(k)[0]["slack"]
         assert len(clo) == len(ref)
-        np.testing.assert_allclose(clo, ref, rtol=1e-5, atol=1e-6)
-        checked += 1
-    assert checked > 0
+        np.testing.assert_allclose(clo, ref, rtol=1e-5, atol=0)
+        costs_checked += 1
+    assert sfxt_checked >= 4 and costs_checked >= 3

@@ -71,7 +71,7 @@ def test_tiny_fixtures_against_brute_force(name):
     want = want[want != 0.0]
     g = oracle.OracleGraph.from_edges(n, src, dst, w)
     seq = g.sequential(1000)["slack"]
-    clo = g.closure_topk(1000)[0]["slack"]
+    clo = g.closure_topk(1000, ref_roots=False)[0]["slack"]
     assert len(seq) == len(clo) == len(want)
     np.testing.assert_allclose(seq, want, rtol=1e-5)
     np.testing.assert_allclose(clo, want, rtol=1e-5)
@@ -82,7 +82,7 @@ def test_tiny_fixtures_against_brute_force(name):
 def test_sequential_matches_closure(name, k):
     g = _graph(name)
     seq = g.sequential(k)["slack"]
-    clo = g.closure_topk(k)[0]["slack"]
+    clo = g.closure_topk(k, ref_roots=False)[0]["slack"]
     assert len(seq) == len(clo)
     np.testing.assert_allclose(seq, clo, rtol=1e-5, atol=0)
 
@@ -143,7 +143,7 @@ def test_oracle_against_reference_goldens():
             continue
         ref = z[f"{name}/costs"]
         k = int(z[f"{name}/k"])
-        clo = g.closure_topk(k)[0]["slack"]
+        clo = g.closure_topk(k, ref_roots=True)[0]["slack"]
         assert len(clo) == len(ref)
         np.testing.assert_allclose(clo, ref, rtol=1e-5, atol=0)
         costs_checked += 1

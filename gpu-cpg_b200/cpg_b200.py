@@ -67,7 +67,7 @@ class Stats(C.Structure):
         ("pending_peak", C.c_int64), ("bytes_reserved", C.c_int64),
         ("phases", C.c_int32), ("rounds", C.c_int32), ("levels", C.c_int32),
         ("kernel_launches", C.c_int32), ("split", C.c_float),
-        ("frontier_used", C.c_int32),
+        ("frontier_used", C.c_int32), ("retries", C.c_int32),
     ]
 
 

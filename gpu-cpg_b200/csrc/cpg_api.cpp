@@ -449,9 +449,16 @@ int try_query(cpg_handle* h, unsigned long long k) {
     st = counts(h, pend_cost_in, n_pend, 4, 0xffffffffu, cq);
     if (st != CPG_OK) return st;
     if (cp.nz + cq.nz >= k) {
+      // enough known candidates: the k-th smallest of paths and pending
+      // bounds the answer, so one more closure finishes the query
       st = select_kth(h, pcost, n_paths, 1, pend_cost_in, n_pend, 4, k, 1, t);
     } else {
-      st = select_kth(h, pend_cost_in, n_pend, 4, nullptr, 0, 1, n_pend, 0, t);
+      // too few known: grow geometrically by count.  Promoting the j cheapest
+      // pending items (j ~ twice the accepted paths) keeps the split away
+      // from expensive outliers, whose closure could be exponentially large.
+      const unsigned long long j =
+          std::min<unsigned long long>(n_pend, std::max<unsigned long long>(64, 2 * (n_paths + 1)));
+      st = select_kth(h, pend_cost_in, n_pend, 4, nullptr, 0, 1, j, 0, t);
     }
     if (st != CPG_OK) return st;
     const float lim = t + margin_of(t, root_abs);
@@ -779,6 +786,7 @@ cpg_status cpg_report_paths(cpg_handle* h, int64_t k) {
   h->stats.pending_peak = 0;
   h->stats.phases = 0;
   h->stats.rounds = 0;
+  h->stats.retries = 0;
   if (k == 0) {
     h->result_valid = true;
     return CPG_OK;
@@ -788,9 +796,10 @@ cpg_status cpg_report_paths(cpg_handle* h, int64_t k) {
   h->cap_paths = std::max(h->cap_paths, std::max<unsigned long long>(4 * uk, 1 << 16) + nsrc);
   h->cap_front = std::max(h->cap_front, std::max<unsigned long long>(2 * uk, 1 << 16));
   h->cap_pend = std::max(h->cap_pend, std::max<unsigned long long>(8 * uk, 1 << 17) + nsrc);
-  for (int attempt = 0; attempt < 12; ++attempt) {
+  for (int attempt = 0; attempt < 6; ++attempt) {
     const int r = try_query(h, uk);
     if (r == kRetry) {
+      h->stats.retries += 1;
       h->cap_paths *= 2;
       h->cap_front *= 2;
       h->cap_pend *= 2;

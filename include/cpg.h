@@ -103,6 +103,7 @@ typedef struct {
   int32_t kernel_launches; /* kernels launched by the last levelize+report */
   float split;             /* final split (cost threshold) */
   int32_t frontier_used;   /* cpg_frontier actually used by the levelisation */
+  int32_t retries;         /* query restarts after a bounded buffer overflowed */
 } cpg_stats;
 
 /* ------------------------------------------------------------ lifecycle */

@@ -28,6 +28,7 @@ struct DevMem {
 };
 
 constexpr unsigned int kDefaultSpinLimit = 1u << 24;
+constexpr int32_t kMaxRow = 16384;  // longest deviation row the row sort takes
 
 }  // namespace
 
@@ -40,11 +41,13 @@ struct cpg_handle {
 
   // graph
   bool has_graph = false;
-  HostGraph g;
-  std::vector<int32_t> srcs;
+  HostGraph g;          // n, m and the fan-out row offsets only
+  int32_t n_srcs = 0;
   int32_t max_outdeg = 0;
   int64_t big_total = 0;
-  DevMem d_adjp, d_edges, d_iadjp, d_iadj, d_srcs, d_big_off, d_big_tmp;
+  int32_t big_rows = 0, big_cap = 1;
+  DevMem d_adjp, d_edges, d_iadjp, d_iadj, d_srcs, d_big_off, d_big_tmp,
+      d_big_rows;
 
   // suffix tree
   bool sfxt_valid = false;
@@ -119,64 +122,96 @@ Status check_handle(cpg_handle* h) {
   return CPG_OK;
 }
 
-// Upload a host CSR graph and size the suffix-tree buffers.
-Status upload_graph(cpg_handle* h) {
-  const HostGraph& g = h->g;
-  const size_t n = static_cast<size_t>(g.n), m = static_cast<size_t>(g.m);
+// Upload a fan-out CSR and build the rest of the graph on the device: edge
+// words, fan-in CSR and source list.  The host keeps only the row offsets.
+Status upload_graph(cpg_handle* h, int32_t n, int32_t m, const int32_t* adjp,
+                    const int32_t* adj, const float* w) {
+  if (n < 0 || m < 0 || !adjp || (m > 0 && (!adj || !w)))
+    return fail(h, CPG_ERR_INVALID, "null CSR buffer");
+  if (adjp[0] != 0 || adjp[n] != m)
+    return fail(h, CPG_ERR_INVALID, "CSR offsets must start at 0 and end at m");
   CK(cudaSetDevice(h->device), "cudaSetDevice");
-  h->srcs.clear();
-  h->max_outdeg = 0;
-  std::vector<int32_t> big_off(n, -1);
+  int32_t max_deg = 0;
+  for (int32_t v = 0; v < n; ++v) {
+    const int32_t d = adjp[v + 1] - adjp[v];
+    if (d < 0) return fail(h, CPG_ERR_INVALID, "CSR offsets must be non-decreasing");
+    max_deg = std::max(max_deg, d);
+  }
+  for (int64_t e = 0; e < m; ++e)
+    if (static_cast<uint32_t>(adj[e]) >= static_cast<uint32_t>(n))
+      return fail(h, CPG_ERR_INVALID, "edge head out of range");
+  if (max_deg > kMaxRow)
+    return fail(h, CPG_ERR_INVALID, "out-degree above 16384 is not supported");
+  h->has_graph = false;
+  h->g.n = n;
+  h->g.m = m;
+  h->g.adjp.assign(adjp, adjp + n + 1);
+  h->g.adj.clear();
+  h->g.w.clear();
+  h->max_outdeg = max_deg;
+  std::vector<int32_t> big_off(n, -1), big_rows;
   int64_t big_total = 0;
-  for (size_t v = 0; v < n; ++v) {
-    const int32_t od = g.adjp[v + 1] - g.adjp[v];
-    h->max_outdeg = std::max(h->max_outdeg, od);
-    if (g.iadjp[v + 1] == g.iadjp[v]) h->srcs.push_back(static_cast<int32_t>(v));
+  int32_t big_cap = 1;
+  for (int32_t v = 0; v < n; ++v) {
+    const int32_t od = adjp[v + 1] - adjp[v];
     if (od > kSmemRow) {
       big_off[v] = static_cast<int32_t>(big_total);
       big_total += od;
+      big_rows.push_back(v);
+      while (big_cap < od) big_cap <<= 1;
     }
   }
   h->big_total = big_total;
-  std::vector<DevEdge> edges(m);
-  for (size_t e = 0; e < m; ++e) {
-    edges[e].head = g.adj[e];
-    edges[e].w = g.w[e];
-  }
-  CK(ensure(h->d_adjp, (n + 1) * 4), "alloc adjp");
-  CK(ensure(h->d_edges, m * sizeof(DevEdge)), "alloc edges");
-  CK(ensure(h->d_iadjp, (n + 1) * 4), "alloc iadjp");
-  CK(ensure(h->d_iadj, m * 4), "alloc iadj");
-  CK(ensure(h->d_srcs, h->srcs.size() * 4), "alloc srcs");
-  CK(ensure(h->d_big_off, n * 4), "alloc big_off");
+  h->big_rows = static_cast<int32_t>(big_rows.size());
+  h->big_cap = big_cap;
+  const size_t nn = static_cast<size_t>(n), mm = static_cast<size_t>(m);
+  CK(ensure(h->d_adjp, (nn + 1) * 4), "alloc adjp");
+  CK(ensure(h->d_edges, mm * sizeof(DevEdge)), "alloc edges");
+  CK(ensure(h->d_iadjp, (nn + 1) * 4), "alloc iadjp");
+  CK(ensure(h->d_iadj, mm * 4), "alloc iadj");
+  CK(ensure(h->d_srcs, nn * 4 + 4), "alloc srcs");
+  CK(ensure(h->d_big_off, nn * 4), "alloc big_off");
+  CK(ensure(h->d_big_rows, big_rows.size() * 4), "alloc big rows");
   CK(ensure(h->d_big_tmp, static_cast<size_t>(big_total) * sizeof(DevSidetrack)),
      "alloc big rows");
-  cudaStream_t s = h->stream;
-  CK(cudaMemcpyAsync(h->d_adjp.p, g.adjp.data(), (n + 1) * 4, cudaMemcpyHostToDevice, s), "H2D adjp");
-  if (m) {
-    CK(cudaMemcpyAsync(h->d_edges.p, edges.data(), m * sizeof(DevEdge), cudaMemcpyHostToDevice, s), "H2D edges");
-    CK(cudaMemcpyAsync(h->d_iadj.p, g.iadj.data(), m * 4, cudaMemcpyHostToDevice, s), "H2D iadj");
-  }
-  CK(cudaMemcpyAsync(h->d_iadjp.p, g.iadjp.data(), (n + 1) * 4, cudaMemcpyHostToDevice, s), "H2D iadjp");
-  if (!h->srcs.empty())
-    CK(cudaMemcpyAsync(h->d_srcs.p, h->srcs.data(), h->srcs.size() * 4, cudaMemcpyHostToDevice, s), "H2D srcs");
-  if (n) CK(cudaMemcpyAsync(h->d_big_off.p, big_off.data(), n * 4, cudaMemcpyHostToDevice, s), "H2D big_off");
-  // suffix tree storage
-  CK(ensure(h->d_order, n * 4), "alloc order");
-  CK(ensure(h->d_lvlp, (n + 2) * 4), "alloc lvlp");
-  CK(ensure(h->d_level_of, n * 4), "alloc level_of");
-  CK(ensure(h->d_dist, n * 4), "alloc dist");
-  CK(ensure(h->d_succ, n * 4), "alloc succ");
-  CK(ensure(h->d_dev_cnt, n * 4), "alloc dev_cnt");
-  CK(ensure(h->d_dev, m * sizeof(DevSidetrack)), "alloc deviations");
-  CK(ensure(h->d_ht_root, n * 4), "alloc ht_root");
-  CK(ensure(h->d_ht_size, n * 4), "alloc ht_size");
-  CK(ensure(h->d_pool_mark, (n + 2) * 8), "alloc pool_mark");
-  CK(ensure(h->d_deps, n * 4), "alloc deps");
+  // suffix tree storage (the deviation array doubles as upload staging)
+  CK(ensure(h->d_order, nn * 4), "alloc order");
+  CK(ensure(h->d_lvlp, (nn + 2) * 4), "alloc lvlp");
+  CK(ensure(h->d_level_of, nn * 4), "alloc level_of");
+  CK(ensure(h->d_dist, nn * 4), "alloc dist");
+  CK(ensure(h->d_succ, nn * 4), "alloc succ");
+  CK(ensure(h->d_dev_cnt, nn * 4), "alloc dev_cnt");
+  CK(ensure(h->d_dev, mm * sizeof(DevSidetrack)), "alloc deviations");
+  CK(ensure(h->d_ht_root, nn * 4), "alloc ht_root");
+  CK(ensure(h->d_ht_size, nn * 4), "alloc ht_size");
+  CK(ensure(h->d_pool_mark, (nn + 2) * 8), "alloc pool_mark");
+  CK(ensure(h->d_deps, std::max(nn, build_scratch_words(n)) * 4), "alloc deps");
   CK(ensure(h->d_sctr, sizeof(SfxtCounters)), "alloc sfxt counters");
-  if (h->hnode_cap == 0) h->hnode_cap = n * 10ull + 1024;
+  if (h->hnode_cap < nn * 10ull + 1024) {
+    h->hnode_cap = nn * 10ull + 1024;
+    release(h->d_hnodes);
+  }
   CK(ensure(h->d_hnodes, h->hnode_cap * sizeof(HeapNode)), "alloc chain heaps");
+  cudaStream_t s = h->stream;
+  int32_t* stage_adj = reinterpret_cast<int32_t*>(h->d_dev.p);
+  float* stage_w = reinterpret_cast<float*>(stage_adj + mm);
+  CK(cudaMemcpyAsync(h->d_adjp.p, adjp, (nn + 1) * 4, cudaMemcpyHostToDevice, s), "H2D adjp");
+  if (m) {
+    CK(cudaMemcpyAsync(stage_adj, adj, mm * 4, cudaMemcpyHostToDevice, s), "H2D adjncy");
+    CK(cudaMemcpyAsync(stage_w, w, mm * 4, cudaMemcpyHostToDevice, s), "H2D delays");
+  }
+  if (n) CK(cudaMemcpyAsync(h->d_big_off.p, big_off.data(), nn * 4, cudaMemcpyHostToDevice, s), "H2D big_off");
+  if (!big_rows.empty())
+    CK(cudaMemcpyAsync(h->d_big_rows.p, big_rows.data(), big_rows.size() * 4, cudaMemcpyHostToDevice, s), "H2D big rows");
+  int32_t* nsrc_dev = P<int32_t>(h->d_srcs) + nn;
+  CK(launch_build_graph(P<int32_t>(h->d_adjp), stage_adj, stage_w, n, m,
+                        P<DevEdge>(h->d_edges), P<int32_t>(h->d_iadjp),
+                        P<int32_t>(h->d_iadj), P<int32_t>(h->d_srcs), nsrc_dev,
+                        P<int32_t>(h->d_deps), s), "build graph");
+  int32_t* hn = static_cast<int32_t*>(h->pinned);
+  CK(cudaMemcpyAsync(hn, nsrc_dev, 4, cudaMemcpyDeviceToHost, s), "D2H sources");
   CK(cudaStreamSynchronize(s), "upload");
+  h->n_srcs = *hn;
   h->has_graph = true;
   h->sfxt_valid = false;
   h->h_sfxt_cached = false;
@@ -190,8 +225,7 @@ Status load_edgelist(cpg_handle* h, const EdgeList& el) {
   HostGraph g;
   Status st = edges_to_csr(el, g, h->err);
   if (st != CPG_OK) return st;
-  h->g = std::move(g);
-  return upload_graph(h);
+  return upload_graph(h, g.n, g.m, g.adjp.data(), g.adj.data(), g.w.data());
 }
 
 Status run_sfxt(cpg_handle* h, int32_t start_level) {
@@ -227,15 +261,18 @@ Status run_sfxt(cpg_handle* h, int32_t start_level) {
     p.deps = P<int32_t>(h->d_deps);
     p.big_off = P<int32_t>(h->d_big_off);
     p.big_tmp = P<DevSidetrack>(h->d_big_tmp);
+    p.big_rows = P<int32_t>(h->d_big_rows);
+    p.n_big_rows = h->big_rows;
+    p.big_row_cap = h->big_cap;
     p.ctr = P<SfxtCounters>(h->d_sctr);
     p.start_level = start_level;
     p.known_levels = h->levels;
     p.spin_limit = h->opts.spin_limit ? h->opts.spin_limit : kDefaultSpinLimit;
     CK(cudaEventRecord(h->ev[0], s), "event");
-    int grid = 0;
-    CK(launch_sfxt(p, h->device, s, &grid), "sfxt launch");
+    int grid = 0, launches = 0;
+    CK(launch_sfxt(p, h->device, s, &grid, &launches), "sfxt launch");
     CK(cudaEventRecord(h->ev[1], s), "event");
-    h->stats.kernel_launches += 1;
+    h->stats.kernel_launches += launches;
     SfxtCounters* out = static_cast<SfxtCounters*>(h->pinned);
     CK(cudaMemcpyAsync(out, h->d_sctr.p, sizeof(SfxtCounters), cudaMemcpyDeviceToHost, s), "D2H sfxt counters");
     CK(cudaStreamSynchronize(s), "sfxt");
@@ -392,7 +429,7 @@ int try_query(cpg_handle* h, unsigned long long k) {
   PfxtCounters* dctr = P<PfxtCounters>(h->d_pctr);
   Item* pend_in = P<Item>(h->d_pend0);
   Item* pend_out = P<Item>(h->d_pend1);
-  CK(launch_seed_roots(P<int32_t>(h->d_srcs), static_cast<int32_t>(h->srcs.size()),
+  CK(launch_seed_roots(P<int32_t>(h->d_srcs), h->n_srcs,
                        P<int32_t>(h->d_dist), pend_in, dctr, s), "seed roots");
   h->stats.kernel_launches += 1;
   PfxtCounters c{};
@@ -448,20 +485,34 @@ int try_query(cpg_handle* h, unsigned long long k) {
     if (st != CPG_OK) return st;
     st = counts(h, pend_cost_in, n_pend, 4, 0xffffffffu, cq);
     if (st != CPG_OK) return st;
+    float lim, tie = std::nanf("");
+    bool final_phase = false;
     if (cp.nz + cq.nz >= k) {
-      // enough known candidates: the k-th smallest of paths and pending
-      // bounds the answer, so one more closure finishes the query
+      // enough known candidates: the k-th smallest of paths and pending is
+      // >= the answer's k-th cost, so one more closure finishes the query.
+      // Paths costing exactly t are reported but not expanded.
       st = select_kth(h, pcost, n_paths, 1, pend_cost_in, n_pend, 4, k, 1, t);
+      if (st != CPG_OK) return st;
+      lim = t + margin_of(t, root_abs);
+      tie = t;
+      final_phase = true;
     } else {
       // too few known: grow geometrically by count.  Promoting the j cheapest
       // pending items (j ~ twice the accepted paths) keeps the split away
-      // from expensive outliers, whose closure could be exponentially large.
+      // from expensive outliers, whose closure could be exponentially large;
+      // accepting only costs strictly below the j-th keeps a tie group at
+      // that cost for a later phase.
       const unsigned long long j =
           std::min<unsigned long long>(n_pend, std::max<unsigned long long>(64, 2 * (n_paths + 1)));
       st = select_kth(h, pend_cost_in, n_pend, 4, nullptr, 0, 1, j, 0, t);
+      if (st != CPG_OK) return st;
+      const float below = std::nextafter(t, -INFINITY);
+      Counts lt{};
+      st = counts(h, pend_cost_in, n_pend, 4, float_key_host(below), lt);
+      if (st != CPG_OK) return st;
+      // zeros are not counted by counts(); a zero-cost minimum promotes as is
+      lim = (lt.le > 0) ? below : t;
     }
-    if (st != CPG_OK) return st;
-    const float lim = t + margin_of(t, root_abs);
     // promote pending items under the split, then close over the frontier
     CK(cudaMemsetAsync(&dctr->frontier[0], 0, 3 * sizeof(unsigned long long), s), "memset");
     CK(cudaMemsetAsync(&dctr->pend_out, 0, sizeof(unsigned long long), s), "memset");
@@ -482,6 +533,7 @@ int try_query(cpg_handle* h, unsigned long long k) {
     cpar.pend = pend_out;
     cpar.pend_cap = h->cap_pend;
     cpar.lim = lim;
+    cpar.tie = tie;
     cpar.ctr = dctr;
     cpar.spin_limit = h->opts.spin_limit ? h->opts.spin_limit : kDefaultSpinLimit;
     int grid = 0;
@@ -497,11 +549,8 @@ int try_query(cpg_handle* h, unsigned long long k) {
     n_paths = c.paths;
     n_pend = c.pend_out;
     std::swap(pend_in, pend_out);
-    Counts le{};
-    st = counts(h, pcost, n_paths, 1, float_key_host(t), le);
-    if (st != CPG_OK) return st;
     h->stats.pending_peak = std::max<int64_t>(h->stats.pending_peak, n_pend);
-    if (le.le >= k) break;
+    if (final_phase) break;
   }
   CK(cudaEventRecord(h->ev[3], s), "event");
   // final: the k smallest non-zero accepted costs, sorted
@@ -634,7 +683,7 @@ cpg_status cpg_destroy(cpg_handle* h) {
   cudaSetDevice(h->device);
   cudaStreamSynchronize(h->stream);
   DevMem* all[] = {&h->d_adjp, &h->d_edges, &h->d_iadjp, &h->d_iadj, &h->d_srcs,
-                   &h->d_big_off, &h->d_big_tmp, &h->d_order, &h->d_lvlp,
+                   &h->d_big_off, &h->d_big_tmp, &h->d_big_rows, &h->d_order, &h->d_lvlp,
                    &h->d_level_of, &h->d_dist, &h->d_succ, &h->d_dev_cnt,
                    &h->d_dev, &h->d_ht_root, &h->d_ht_size, &h->d_hnodes,
                    &h->d_pool_mark, &h->d_deps, &h->d_sctr, &h->d_pcost,
@@ -681,23 +730,26 @@ cpg_status cpg_load_csr(cpg_handle* h, int32_t n, int32_t m,
                         const int32_t* adjp, const int32_t* adjncy,
                         const float* w) {
   if (check_handle(h) != CPG_OK) return CPG_ERR_INVALID;
-  HostGraph g;
-  Status st = csr_to_graph(n, m, adjp, adjncy, w, g, h->err);
-  if (st != CPG_OK) return st;
-  h->g = std::move(g);
-  return upload_graph(h);
+  return upload_graph(h, n, m, adjp, adjncy, w);
 }
 
 int64_t cpg_num_verts(const cpg_handle* h) { return h && h->has_graph ? h->g.n : 0; }
 int64_t cpg_num_edges(const cpg_handle* h) { return h && h->has_graph ? h->g.m : 0; }
 
-cpg_status cpg_get_csr(const cpg_handle* h, int32_t* adjp, int32_t* adjncy,
+cpg_status cpg_get_csr(const cpg_handle* hc, int32_t* adjp, int32_t* adjncy,
                        float* w) {
+  cpg_handle* h = const_cast<cpg_handle*>(hc);
   if (!h) return CPG_ERR_INVALID;
   if (!h->has_graph) return CPG_ERR_STATE;
   if (adjp) std::memcpy(adjp, h->g.adjp.data(), (h->g.n + 1) * 4);
-  if (adjncy && h->g.m) std::memcpy(adjncy, h->g.adj.data(), h->g.m * 4);
-  if (w && h->g.m) std::memcpy(w, h->g.w.data(), h->g.m * 4);
+  if ((adjncy || w) && h->g.m) {
+    std::vector<DevEdge> e(h->g.m);
+    CK(cudaMemcpy(e.data(), h->d_edges.p, e.size() * sizeof(DevEdge), cudaMemcpyDeviceToHost), "D2H edges");
+    for (int32_t i = 0; i < h->g.m; ++i) {
+      if (adjncy) adjncy[i] = e[i].head;
+      if (w) w[i] = e[i].w;
+    }
+  }
   return CPG_OK;
 }
 
@@ -727,7 +779,6 @@ cpg_status cpg_update_delays(cpg_handle* h, int64_t count, const int32_t* eids,
   for (int64_t i = 0; i < count; ++i) {
     const int32_t e = eids[i];
     if (e < 0 || e >= h->g.m) return fail(h, CPG_ERR_INVALID, "edge id out of range");
-    h->g.w[e] = w[i];
     if (have_levels) {
       const auto it = std::upper_bound(h->g.adjp.begin(), h->g.adjp.end(), e);
       const int32_t tail = static_cast<int32_t>(it - h->g.adjp.begin()) - 1;
@@ -792,7 +843,7 @@ cpg_status cpg_report_paths(cpg_handle* h, int64_t k) {
     return CPG_OK;
   }
   const unsigned long long uk = static_cast<unsigned long long>(k);
-  const unsigned long long nsrc = h->srcs.size();
+  const unsigned long long nsrc = static_cast<unsigned long long>(h->n_srcs);
   h->cap_paths = std::max(h->cap_paths, std::max<unsigned long long>(4 * uk, 1 << 16) + nsrc);
   h->cap_front = std::max(h->cap_front, std::max<unsigned long long>(2 * uk, 1 << 16));
   h->cap_pend = std::max(h->cap_pend, std::max<unsigned long long>(8 * uk, 1 << 17) + nsrc);

@@ -96,6 +96,8 @@ struct SfxtCounters {
   int err;
   int levels;
   int level_end;             // tail snapshot taken at each level barrier
+  int sort_beg;              // order[] range whose deviation rows were rebuilt
+  int sort_end;
   unsigned long long hnode_used;
   GridBarrier bar;
 };
@@ -121,6 +123,9 @@ struct SfxtParams {
   int32_t* deps;
   const int32_t* big_off;  // scratch offset of rows longer than kSmemRow
   DevSidetrack* big_tmp;
+  const int32_t* big_rows; // vertices with more than kSmemRow fan-out edges
+  int32_t n_big_rows;
+  int32_t big_row_cap;     // longest such row, rounded up to a power of two
   SfxtCounters* ctr;
   int32_t start_level;     // 0: full levelise + relax; > 0: relax from here
   int32_t known_levels;    // level count when start_level > 0
@@ -130,8 +135,10 @@ struct SfxtParams {
 constexpr int kSfxtThreads = 256;
 constexpr int kSmemRow = 256;  // deviation rows up to this length sort in smem
 
-// Launch the persistent SFXT kernel (cooperative).  Returns a cudaError_t.
-int launch_sfxt(const SfxtParams& p, int device, void* stream, int* grid_out);
+// Launch the persistent SFXT kernel (cooperative) and the row sorts that
+// follow it.  Returns a cudaError_t; *launches counts the kernels.
+int launch_sfxt(const SfxtParams& p, int device, void* stream, int* grid_out,
+                int* launches);
 
 // ---------------------------------------------------------------- PFXT
 struct PfxtCounters {
@@ -174,6 +181,8 @@ struct ClosureParams {
   Item* pend;                      // pending output
   unsigned long long pend_cap;
   float lim;                       // accept items with cost <= lim
+  float tie;                       // accepted paths costing exactly this are
+                                   // not expanded (NaN: expand all)
   PfxtCounters* ctr;
   unsigned int spin_limit;
 };
@@ -219,6 +228,13 @@ int launch_emit_topk(const PathStore& ps, unsigned long long n_paths,
 // device_common.cuh).
 float key_float_host(unsigned int k);
 unsigned int float_key_host(float f);
+
+// Device-side graph build from an uploaded fan-out CSR (graph_build.cu).
+size_t build_scratch_words(int32_t n);
+int launch_build_graph(const int32_t* adjp, const int32_t* adj, const float* w,
+                       int32_t n, int64_t m, DevEdge* edges, int32_t* iadjp,
+                       int32_t* iadj, int32_t* srcs, int32_t* n_srcs,
+                       int32_t* scratch, void* stream);
 
 // Scatter new delays into the device fan-out edges.
 int launch_scatter_delays(DevEdge* edges, const int32_t* eids, const float* w,

@@ -164,7 +164,11 @@ closure_kernel(ClosureParams p) {
           atomicCAS(&p.ctr->err, kDevOk, kDevCapacity);
         }
       }
-      const bool sib = stored && it.node >= 0;
+      // A path costing exactly the final split is reported but not expanded:
+      // its descendants cost at least as much, so with tied costs (integer
+      // delays) they could only add to the tie group at the split.
+      const bool expand = stored && !(it.cost == p.tie);
+      const bool sib = expand && it.node >= 0;
       const float pcost = sib ? __ldcg(p.ps.cost + it.parent) : 0.f;
       // siblings: heap children of this deviation among the parent's options
       {
@@ -192,9 +196,9 @@ closure_kernel(ClosureParams p) {
       {
         Item c;
         c.parent = static_cast<int>(q);
-        c.node = stored ? __ldg(p.g.ht_root + to) : -1;
+        c.node = expand ? __ldg(p.g.ht_root + to) : -1;
         c.j = 0;
-        const bool ex = stored && make_candidate(p.g, c.node, 0, it.cost, c.cost);
+        const bool ex = expand && make_candidate(p.g, c.node, 0, it.cost, c.cost);
         route(p, out, out_cnt, ex, c);
       }
     }

@@ -40,26 +40,40 @@ __device__ __forceinline__ int fixed_delay(float w) {
   return wgt;
 }
 
-// One warp builds vertex v at level lvl.
-__device__ void build_vertex(const SfxtParams& p, int v, int lvl,
-                             DevSidetrack* sbuf, bool do_kahn) {
+// One warp builds vertex v at level lvl: fixed-point distance, successor,
+// its deviation list (unsorted here; sort_rows_kernel orders it), its chain
+// heap, and the Kahn step for its fan-in neighbours.
+__device__ void build_vertex(const SfxtParams& p, int v, int lvl, bool do_kahn) {
   const int lane = threadIdx.x & 31;
   const int rb = p.adjp[v];
   const int re = p.adjp[v + 1];
-  const int deg = re - rb;
   int best = INT_MAX;
   int s = -1;
+  // the first 32 edges stay in registers; longer rows reload (L1/L2 hits)
+  DevEdge e0;
+  e0.head = -1;
+  e0.w = 0.f;
+  int dh0 = INT_MAX;
+  if (rb + lane < re) {
+    e0 = p.edges[rb + lane];
+    dh0 = __ldcg(p.dist + e0.head);
+  }
   if (lvl == 0) {
     best = 0;  // sinks (out-degree 0) start at distance 0 (gpucpg.cu:17034-17038)
   } else {
-    for (int e = rb + lane; e < re; e += 32) {
+    if (rb + lane < re)
+      best = static_cast<int>(static_cast<unsigned>(dh0) + static_cast<unsigned>(fixed_delay(e0.w)));
+    for (int e = rb + 32 + lane; e < re; e += 32) {
       const DevEdge ed = p.edges[e];
       const int c = static_cast<int>(static_cast<unsigned>(__ldcg(p.dist + ed.head)) +
                                      static_cast<unsigned>(fixed_delay(ed.w)));
       best = min(best, c);
     }
     best = warp_min_i(best);
-    for (int e = rb + lane; e < re; e += 32) {
+    if (rb + lane < re &&
+        static_cast<int>(static_cast<unsigned>(dh0) + static_cast<unsigned>(fixed_delay(e0.w))) == best)
+      s = e0.head;
+    for (int e = rb + 32 + lane; e < re; e += 32) {
       const DevEdge ed = p.edges[e];
       const int c = static_cast<int>(static_cast<unsigned>(__ldcg(p.dist + ed.head)) +
                                      static_cast<unsigned>(fixed_delay(ed.w)));
@@ -69,9 +83,7 @@ __device__ void build_vertex(const SfxtParams& p, int v, int lvl,
   }
 
   // deviations: every fan-out edge whose head is not the successor and has a
-  // finite distance, in edge order, staged then ranked by key
-  const bool big = deg > kSmemRow;
-  DevSidetrack* stage = big ? (p.big_tmp + p.big_off[v]) : sbuf;
+  // finite distance, compacted in edge order into v's own fan-out slots
   int cnt = 0;
   float kmin = __int_as_float(0x7f800000);  // +inf
   for (int base = rb; base < re; base += 32) {
@@ -79,8 +91,15 @@ __device__ void build_vertex(const SfxtParams& p, int v, int lvl,
     bool valid = false;
     DevSidetrack rec;
     if (e < re) {
-      const DevEdge ed = p.edges[e];
-      const int dh = __ldcg(p.dist + ed.head);
+      DevEdge ed;
+      int dh;
+      if (base == rb) {
+        ed = e0;
+        dh = dh0;
+      } else {
+        ed = p.edges[e];
+        dh = __ldcg(p.dist + ed.head);
+      }
       valid = ed.head != s && dh != INT_MAX;
       rec.head = ed.head;
       rec.w = ed.w;
@@ -89,23 +108,11 @@ __device__ void build_vertex(const SfxtParams& p, int v, int lvl,
     }
     const unsigned bal = __ballot_sync(0xffffffffu, valid);
     if (valid) {
-      stage[cnt + __popc(bal & lanemask_lt())] = rec;
+      p.dev[rb + cnt + __popc(bal & lanemask_lt())] = rec;
       kmin = fminf(kmin, rec.key);
     }
     cnt += __popc(bal);
   }
-  __syncwarp();
-  for (int i = lane; i < cnt; i += 32) {
-    const DevSidetrack ri = stage[i];
-    int r = 0;
-    for (int j = 0; j < cnt; ++j) {
-      const float kj = stage[j].key;
-      r += (kj < ri.key) || (kj == ri.key && j < i);
-    }
-    p.dev[rb + r] = ri;
-  }
-  __syncwarp();
-  // warp-wide minimum key (the rank-0 deviation)
   for (int o = 16; o > 0; o >>= 1) kmin = fminf(kmin, __shfl_xor_sync(0xffffffffu, kmin, o));
 
   if (lane == 0) {
@@ -194,15 +201,14 @@ __device__ void build_vertex(const SfxtParams& p, int v, int lvl,
 
 __global__ void __launch_bounds__(kSfxtThreads)
 sfxt_persistent_kernel(SfxtParams p) {
-  __shared__ DevSidetrack sbuf_all[kSfxtThreads / 32][kSmemRow];
   const int warp_in_block = threadIdx.x >> 5;
-  const int lane = threadIdx.x & 31;
-  DevSidetrack* sbuf = sbuf_all[warp_in_block];
   const int gwarp = blockIdx.x * (blockDim.x >> 5) + warp_in_block;
   const int nwarps = gridDim.x * (blockDim.x >> 5);
   const bool full = p.start_level == 0;
 
   int beg, end, lvl;
+  if (blockIdx.x == 0 && threadIdx.x == 0)
+    p.ctr->sort_beg = full ? 0 : p.lvlp[p.start_level];
   if (full) {
     // phase 0: reset per-vertex state, seed level 0 with the sinks
     for (int base = blockIdx.x * blockDim.x; base < p.n;
@@ -242,9 +248,8 @@ sfxt_persistent_kernel(SfxtParams p) {
       p.pool_mark[lvl] = *reinterpret_cast<volatile unsigned long long*>(&p.ctr->hnode_used);
     }
     for (int i = beg + gwarp; i < end; i += nwarps) {
-      build_vertex(p, __ldcg(p.order + i), lvl, sbuf, full);
+      build_vertex(p, __ldcg(p.order + i), lvl, full);
     }
-    (void)lane;
     // the tail keeps growing as soon as the next level starts appending, so
     // the level bound is the snapshot the last arriving block took
     if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit, &p.ctr->tail,
@@ -261,13 +266,145 @@ sfxt_persistent_kernel(SfxtParams p) {
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     p.ctr->levels = lvl;
     p.lvlp[lvl] = beg;
+    p.ctr->sort_end = beg;
   }
+}
+
+// ------------------------------------------------------------ row sorting
+// Orders each rebuilt vertex's deviation list by (key, edge position): one
+// warp per vertex, a register bitonic network for rows up to 32 and a shared
+// memory one up to kSmemRow.  Longer rows go to sort_big_rows_kernel.
+constexpr int kSortWarps = 8;
+
+__device__ __forceinline__ unsigned long long sort_word(float key, int idx) {
+  return (static_cast<unsigned long long>(float_key(key)) << 32) |
+         static_cast<unsigned>(idx);
+}
+
+__global__ void __launch_bounds__(kSortWarps * 32)
+sort_rows_kernel(const int32_t* order, const int* range, const int32_t* adjp,
+                 const int32_t* dev_cnt, DevSidetrack* dev) {
+  __shared__ unsigned long long skey[kSortWarps][kSmemRow];
+  __shared__ DevSidetrack srec[kSortWarps][kSmemRow];
+  const int lane = threadIdx.x & 31;
+  const int w = threadIdx.x >> 5;
+  const int beg = range[0], end = range[1];
+  for (int i = beg + blockIdx.x * kSortWarps + w; i < end; i += gridDim.x * kSortWarps) {
+    const int v = order[i];
+    const int cnt = dev_cnt[v];
+    if (cnt <= 1 || cnt > kSmemRow) continue;
+    DevSidetrack* row = dev + adjp[v];
+    if (cnt <= 32) {
+      DevSidetrack r;
+      unsigned long long x = ~0ull;
+      if (lane < cnt) {
+        r = row[lane];
+        x = sort_word(r.key, lane);
+      }
+      for (int k = 2; k <= 32; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+          const unsigned long long y = __shfl_xor_sync(0xffffffffu, x, j);
+          const bool up = (lane & k) == 0;
+          const bool lower = (lane & j) == 0;
+          x = (lower == up) ? (x < y ? x : y) : (x > y ? x : y);
+        }
+      }
+      // lane i now holds the i-th smallest; fetch that record from its lane
+      const int src = static_cast<int>(x & 0xffffffffu);
+      DevSidetrack o;
+      o.head = __shfl_sync(0xffffffffu, r.head, src & 31);
+      o.w = __shfl_sync(0xffffffffu, r.w, src & 31);
+      o.dist_head = __shfl_sync(0xffffffffu, r.dist_head, src & 31);
+      o.key = __shfl_sync(0xffffffffu, r.key, src & 31);
+      if (lane < cnt) row[lane] = o;
+    } else {
+      int n2 = 64;
+      while (n2 < cnt) n2 <<= 1;
+      for (int t = lane; t < n2; t += 32) {
+        if (t < cnt) {
+          const DevSidetrack r = row[t];
+          srec[w][t] = r;
+          skey[w][t] = sort_word(r.key, t);
+        } else {
+          skey[w][t] = ~0ull;
+        }
+      }
+      __syncwarp();
+      for (int k = 2; k <= n2; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+          for (int t = lane; t < n2; t += 32) {
+            const int u = t ^ j;
+            if (u > t) {
+              const unsigned long long a = skey[w][t], b = skey[w][u];
+              const bool asc = (t & k) == 0;
+              if ((a > b) == asc) {
+                skey[w][t] = b;
+                skey[w][u] = a;
+              }
+            }
+          }
+          __syncwarp();
+        }
+      }
+      for (int t = lane; t < cnt; t += 32)
+        row[t] = srec[w][static_cast<int>(skey[w][t] & 0xffffffffu)];
+      __syncwarp();
+    }
+  }
+}
+
+// Rows longer than kSmemRow (a super-source, say): one block per row, a
+// bitonic sort of the (key, position) words in dynamic shared memory, then a
+// gather through the staging copy kept in big_tmp.
+__global__ void sort_big_rows_kernel(const int32_t* rows, const int32_t* adjp,
+                                     const int32_t* dev_cnt, DevSidetrack* dev,
+                                     const int32_t* big_off, DevSidetrack* big_tmp,
+                                     int cap) {
+  extern __shared__ unsigned long long wbuf[];
+  const int v = rows[blockIdx.x];
+  const int cnt = dev_cnt[v];
+  if (cnt <= kSmemRow) return;
+  DevSidetrack* row = dev + adjp[v];
+  DevSidetrack* tmp = big_tmp + big_off[v];
+  int n2 = 1;
+  while (n2 < cnt) n2 <<= 1;
+  if (n2 > cap) n2 = cap;  // host guarantees cnt <= cap
+  for (int t = threadIdx.x; t < n2; t += blockDim.x) {
+    if (t < cnt) {
+      const DevSidetrack r = row[t];
+      tmp[t] = r;
+      wbuf[t] = sort_word(r.key, t);
+    } else {
+      wbuf[t] = ~0ull;
+    }
+  }
+  __syncthreads();
+  for (int k = 2; k <= n2; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int t = threadIdx.x; t < n2; t += blockDim.x) {
+        const int u = t ^ j;
+        if (u > t) {
+          const unsigned long long a = wbuf[t], b = wbuf[u];
+          const bool asc = (t & k) == 0;
+          if ((a > b) == asc) {
+            wbuf[t] = b;
+            wbuf[u] = a;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  for (int t = threadIdx.x; t < cnt; t += blockDim.x)
+    row[t] = tmp[static_cast<int>(wbuf[t] & 0xffffffffu)];
 }
 
 }  // namespace
 
-int launch_sfxt(const SfxtParams& p, int device, void* stream, int* grid_out) {
+int launch_sfxt(const SfxtParams& p, int device, void* stream, int* grid_out,
+                int* launches) {
   int sms = 0, per_sm = 0;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
   cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   if (e != cudaSuccess) return e;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sfxt_persistent_kernel,
@@ -278,9 +415,26 @@ int launch_sfxt(const SfxtParams& p, int device, void* stream, int* grid_out) {
   if (grid_out) *grid_out = grid;
   SfxtParams pp = p;
   void* args[] = {&pp};
-  return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(sfxt_persistent_kernel),
-                                     dim3(grid), dim3(kSfxtThreads), args, 0,
-                                     static_cast<cudaStream_t>(stream));
+  e = cudaLaunchCooperativeKernel(reinterpret_cast<void*>(sfxt_persistent_kernel),
+                                  dim3(grid), dim3(kSfxtThreads), args, 0, st);
+  if (e != cudaSuccess) return e;
+  sort_rows_kernel<<<sms * 8, kSortWarps * 32, 0, st>>>(
+      p.order, &p.ctr->sort_beg, p.adjp, p.dev_cnt, p.dev);
+  int n = 2;
+  if (p.n_big_rows > 0) {
+    const size_t smem = static_cast<size_t>(p.big_row_cap) * sizeof(unsigned long long);
+    if (smem > 48 * 1024) {
+      e = cudaFuncSetAttribute(sort_big_rows_kernel,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(smem));
+      if (e != cudaSuccess) return e;
+    }
+    sort_big_rows_kernel<<<p.n_big_rows, 1024, smem, st>>>(
+        p.big_rows, p.adjp, p.dev_cnt, p.dev, p.big_off, p.big_tmp, p.big_row_cap);
+    ++n;
+  }
+  if (launches) *launches += n;
+  return cudaGetLastError();
 }
 
 }  // namespace cpg

@@ -198,7 +198,7 @@ class CpGen:
     def __init__(self, device: int = 0, stream: int | None = None,
                  division: int = DIV_REFERENCE, frontier: int = FRONTIER_AUTO,
                  hbm_budget_bytes: int = 0, spin_limit: int = 0,
-                 root_seeding: int = ROOTS_REFERENCE):
+                 root_seeding: int = ROOTS_REFERENCE, host_stepped: bool = False):
         o = Options()
         lib.cpg_options_init(C.byref(o))
         o.device = device
@@ -208,6 +208,7 @@ class CpGen:
         o.hbm_budget_bytes = hbm_budget_bytes
         o.spin_limit = spin_limit
         o.root_seeding = root_seeding
+        o.reserved[0] = 1 if host_stepped else 0
         self._h = C.c_void_p()
         st = lib.cpg_create(C.byref(self._h), C.byref(o))
         if st != CPG_OK:

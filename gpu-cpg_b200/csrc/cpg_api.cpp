@@ -63,7 +63,9 @@ struct cpg_handle {
   unsigned long long cap_paths = 0, cap_front = 0, cap_pend = 0;
   DevMem d_pcost, d_pparent, d_pfrom, d_pto, d_plevel, d_front0, d_front1,
       d_pend0, d_pend1, d_pctr, d_selstate, d_selhist, d_counts, d_keys,
-      d_vals, d_sorthist, d_cnt, d_rank, d_out_cost, d_out_nodes;
+      d_vals, d_sorthist, d_cnt, d_rank, d_out_cost, d_out_nodes, d_pq, d_qids,
+      d_ehist, d_esort, d_equery, d_ectr;
+  size_t sorted_vals_off = 0;  // where the sorted path indices start in d_vals
   int64_t n_result = 0;
   unsigned long long n_paths = 0;
   bool result_valid = false;
@@ -487,7 +489,7 @@ int try_query(cpg_handle* h, unsigned long long k) {
     if (st != CPG_OK) return st;
     float lim, tie = std::nanf("");
     bool final_phase = false;
-    if (cp.nz + cq.nz >= k) {
+    if (cp.nz >= k) {
       // enough known candidates: the k-th smallest of paths and pending is
       // >= the answer's k-th cost, so one more closure finishes the query.
       // Paths costing exactly t are reported but not expanded.
@@ -503,7 +505,7 @@ int try_query(cpg_handle* h, unsigned long long k) {
       // accepting only costs strictly below the j-th keeps a tie group at
       // that cost for a later phase.
       const unsigned long long j =
-          std::min<unsigned long long>(n_pend, std::max<unsigned long long>(64, 2 * (n_paths + 1)));
+          std::min<unsigned long long>(n_pend, std::max<unsigned long long>(64, 4 * (n_paths + 1)));
       st = select_kth(h, pend_cost_in, n_pend, 4, nullptr, 0, 1, j, 0, t);
       if (st != CPG_OK) return st;
       const float below = std::nextafter(t, -INFINITY);
@@ -587,6 +589,98 @@ int try_query(cpg_handle* h, unsigned long long k) {
   h->stats.split = t;
   h->n_paths = n_paths;
   h->n_result = static_cast<int64_t>(k_out);
+  h->result_valid = true;
+  return CPG_OK;
+}
+
+// The whole query on the device: one cooperative launch of the engine.
+// Returns kRetry when a bounded buffer overflowed.
+int engine_query(cpg_handle* h, unsigned long long k) {
+  Status st = alloc_query(h, k);
+  if (st != CPG_OK) return st;
+  cudaStream_t s = h->stream;
+  int grid = 0;
+  CK(engine_grid(h->device, &grid), "engine occupancy");
+  const size_t cp = h->cap_paths;
+  CK(ensure(h->d_pq, cp * 4), "alloc paths");
+  CK(ensure(h->d_qids, 2 * k * 4), "alloc sort");
+  CK(ensure(h->d_ehist, static_cast<size_t>(kSelBins) * 4), "alloc select");
+  CK(ensure(h->d_esort, (256 * static_cast<size_t>(grid) + 256) * 4), "alloc sort");
+  CK(ensure(h->d_equery, sizeof(EngineQuery)), "alloc query");
+  CK(ensure(h->d_ectr, sizeof(EngineCounters)), "alloc counters");
+  EngineQuery q{};
+  q.k = static_cast<long long>(k);
+  q.src_beg = 0;
+  q.src_end = h->n_srcs;
+  CK(cudaMemcpyAsync(h->d_equery.p, &q, sizeof(q), cudaMemcpyHostToDevice, s), "H2D query");
+  CK(cudaMemsetAsync(h->d_ectr.p, 0, sizeof(EngineCounters), s), "memset");
+  CK(cudaMemsetAsync(h->d_ehist.p, 0, static_cast<size_t>(kSelBins) * 4, s), "memset");
+  // every output slot is written by the compaction; zero-filling keeps a path
+  // index in range even if selection and compaction ever disagreed
+  CK(cudaMemsetAsync(h->d_vals.p, 0, 2 * k * 4, s), "memset");
+  EngineParams p{};
+  p.g.adjp = P<int32_t>(h->d_adjp);
+  p.g.dist = P<int32_t>(h->d_dist);
+  p.g.dev_cnt = P<int32_t>(h->d_dev_cnt);
+  p.g.dev = P<DevSidetrack>(h->d_dev);
+  p.g.ht_root = P<int32_t>(h->d_ht_root);
+  p.g.hnodes = P<HeapNode>(h->d_hnodes);
+  p.g.division = h->opts.division;
+  p.srcs = P<int32_t>(h->d_srcs);
+  p.q = P<EngineQuery>(h->d_equery);
+  p.nq = 1;
+  p.root_ref = h->opts.root_seeding == CPG_ROOTS_REFERENCE;
+  p.ps = path_store(h);
+  p.pq = P<int32_t>(h->d_pq);
+  p.pend[0] = P<Item>(h->d_pend0);
+  p.pend[1] = P<Item>(h->d_pend1);
+  p.pend_cap = h->cap_pend;
+  p.front[0] = P<Item>(h->d_front0);
+  p.front[1] = P<Item>(h->d_front1);
+  p.front_cap = h->cap_front;
+  p.hist = P<unsigned int>(h->d_ehist);
+  p.keys[0] = P<unsigned int>(h->d_keys);
+  p.keys[1] = P<unsigned int>(h->d_keys) + k;
+  p.qids[0] = P<unsigned int>(h->d_qids);
+  p.qids[1] = P<unsigned int>(h->d_qids) + k;
+  p.vals[0] = P<unsigned int>(h->d_vals);
+  p.vals[1] = P<unsigned int>(h->d_vals) + k;
+  p.out_cap = k;
+  p.sort_hist = P<unsigned int>(h->d_esort);
+  p.digit_tot = P<unsigned int>(h->d_esort) + 256 * static_cast<size_t>(grid);
+  p.rank_of = P<int32_t>(h->d_rank);
+  p.out_cost = P<float>(h->d_out_cost);
+  p.out_nodes = P<cpg_path_node>(h->d_out_nodes);
+  p.ctr = P<EngineCounters>(h->d_ectr);
+  p.spin_limit = h->opts.spin_limit ? h->opts.spin_limit : kDefaultSpinLimit;
+  CK(cudaEventRecord(h->ev[2], s), "event");
+  CK(launch_engine(p, h->device, s), "engine launch");
+  CK(cudaEventRecord(h->ev[3], s), "event");
+  h->stats.kernel_launches += 1;
+  char* hb = static_cast<char*>(h->pinned);
+  CK(cudaMemcpyAsync(hb, h->d_ectr.p, sizeof(EngineCounters), cudaMemcpyDeviceToHost, s), "D2H counters");
+  CK(cudaMemcpyAsync(hb + 512, h->d_equery.p, sizeof(EngineQuery), cudaMemcpyDeviceToHost, s), "D2H query");
+  CK(cudaStreamSynchronize(s), "engine");
+  EngineCounters c;
+  EngineQuery qo;
+  std::memcpy(&c, hb, sizeof(c));
+  std::memcpy(&qo, hb + 512, sizeof(qo));
+  if (c.err == kDevTimeout)
+    return fail(h, CPG_ERR_TIMEOUT, "query engine: grid barrier wait ran out");
+  if (c.err == kDevCapacity) return kRetry;
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, h->ev[2], h->ev[3]);
+  h->stats.pfxt_ms = ms;
+  h->stats.select_ms = 0.0;
+  h->stats.paths_accepted = static_cast<int64_t>(c.paths);
+  h->stats.items_generated = static_cast<int64_t>(c.paths + c.pend_out);
+  h->stats.pending_peak = static_cast<int64_t>(c.pend_out);
+  h->stats.phases = c.phases;
+  h->stats.rounds = c.rounds;
+  h->stats.split = qo.t;
+  h->n_paths = c.paths;
+  h->n_result = static_cast<int64_t>(qo.k_out);
+  h->sorted_vals_off = c.sorted_buf ? k : 0;
   h->result_valid = true;
   return CPG_OK;
 }
@@ -691,7 +785,8 @@ cpg_status cpg_destroy(cpg_handle* h) {
                    &h->d_front0, &h->d_front1, &h->d_pend0, &h->d_pend1,
                    &h->d_pctr, &h->d_selstate, &h->d_selhist, &h->d_counts,
                    &h->d_keys, &h->d_vals, &h->d_sorthist, &h->d_cnt,
-                   &h->d_rank, &h->d_out_cost, &h->d_out_nodes};
+                   &h->d_rank, &h->d_out_cost, &h->d_out_nodes, &h->d_pq,
+                   &h->d_qids, &h->d_ehist, &h->d_esort, &h->d_equery, &h->d_ectr};
   for (DevMem* b : all) release(*b);
   for (auto& e : h->ev)
     if (e) cudaEventDestroy(e);
@@ -847,13 +942,21 @@ cpg_status cpg_report_paths(cpg_handle* h, int64_t k) {
   h->cap_paths = std::max(h->cap_paths, std::max<unsigned long long>(4 * uk, 1 << 16) + nsrc);
   h->cap_front = std::max(h->cap_front, std::max<unsigned long long>(2 * uk, 1 << 16));
   h->cap_pend = std::max(h->cap_pend, std::max<unsigned long long>(8 * uk, 1 << 17) + nsrc);
-  for (int attempt = 0; attempt < 6; ++attempt) {
-    const int r = try_query(h, uk);
+  const bool host_stepped = h->opts.reserved[0] == 1;
+  for (int attempt = 0; attempt < 10; ++attempt) {
+    const int r = host_stepped ? try_query(h, uk) : engine_query(h, uk);
     if (r == kRetry) {
+      // a bounded pile overflowed: grow 4x while device memory allows (a tie
+      // wall of equal-cost paths can need far more than K of them)
       h->stats.retries += 1;
-      h->cap_paths *= 2;
-      h->cap_front *= 2;
-      h->cap_pend *= 2;
+      size_t free_b = 0, total_b = 0;
+      cudaMemGetInfo(&free_b, &total_b);
+      const size_t held = static_cast<size_t>(h->stats.bytes_reserved);
+      const size_t next = 4 * held;
+      if (next > held + free_b * 9 / 10) break;
+      h->cap_paths *= 4;
+      h->cap_front *= 4;
+      h->cap_pend *= 4;
       continue;
     }
     return static_cast<cpg_status>(r);
@@ -905,7 +1008,8 @@ cpg_status cpg_get_path_vertices(cpg_handle* h, int64_t i, int32_t* verts,
   Status st = cache_sfxt_host(h);
   if (st != CPG_OK) return st;
   unsigned int idx = 0;
-  CK(cudaMemcpy(&idx, P<unsigned int>(h->d_vals) + i, 4, cudaMemcpyDeviceToHost), "D2H index");
+  CK(cudaMemcpy(&idx, P<unsigned int>(h->d_vals) + h->sorted_vals_off + i, 4,
+                cudaMemcpyDeviceToHost), "D2H index");
   // deviations from the leaf back to the root
   std::vector<std::pair<int32_t, int32_t>> devs;
   int32_t cur = static_cast<int32_t>(idx), src = -1;

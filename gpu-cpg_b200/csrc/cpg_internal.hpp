@@ -201,6 +201,77 @@ int launch_promote(const Item* pend_in, unsigned long long n_in, float lim,
                    unsigned long long pend_cap, PfxtCounters* ctr,
                    void* stream);
 
+// ---------------------------------------------------------------- engine
+// The persistent query engine (engine.cu) runs whole queries on the device:
+// root seeding, every split raise, the closures, the final top-K select and
+// the segmented sort, for any number of queries over one device graph, in
+// one cooperative launch with no host round trip.
+constexpr int kMaxQueries = 4096;   // Item.j carries the query id in 12 bits
+constexpr int kJBits = 20;          // ... and the deviation index in 20 bits
+constexpr unsigned kJMask = (1u << kJBits) - 1u;
+constexpr int kSelBins = 2048;
+
+struct EngineQuery {
+  long long k;
+  int src_beg, src_end;       // this query's sources in EngineParams::srcs
+  int mode;                   // 0 idle, 1 grow, 2 final, 3 output select
+  int done;
+  float t, lim, tie, root_abs;
+  unsigned int prefix;        // radix select state
+  unsigned int pad0;
+  unsigned long long krem;    // rank still wanted inside the prefix
+  unsigned long long ksel;    // rank the select started from
+  unsigned long long paths_nz, pend_nz, pend_n;
+  unsigned long long k_out, out_off, out_lt, out_eq;
+  int phases;
+  int pad;
+};
+
+struct EngineCounters {
+  int err;
+  int active;
+  unsigned long long paths;
+  unsigned long long frontier[3];
+  unsigned long long pend_out;
+  unsigned long long out_total;
+  int rounds;
+  int phases;
+  int sorted_buf;             // which vals[] holds the sorted path indices
+  int pad;
+  GridBarrier bar;
+};
+
+struct EngineParams {
+  PfxtGraph g;
+  const int32_t* srcs;
+  EngineQuery* q;
+  int nq;
+  int root_ref;               // reference G-PathGen root seeding
+  PathStore ps;
+  int32_t* pq;                // query of each accepted path
+  Item* pend[2];
+  unsigned long long pend_cap;
+  Item* front[2];
+  unsigned long long front_cap;
+  unsigned int* hist;         // nq * kSelBins
+  unsigned int* keys[2];
+  unsigned int* qids[2];
+  unsigned int* vals[2];
+  unsigned long long out_cap;
+  unsigned int* sort_hist;    // 256 * gridDim.x
+  unsigned int* digit_tot;    // 256
+  int32_t* rank_of;           // per accepted path, -1 if not reported
+  float* out_cost;
+  cpg_path_node* out_nodes;
+  EngineCounters* ctr;
+  unsigned int spin_limit;
+};
+
+// Cooperative launch of the engine; *grid_out receives the grid size (the
+// host sizes sort_hist as 256 * grid).
+int engine_grid(int device, int* grid_out);
+int launch_engine(const EngineParams& p, int device, void* stream);
+
 // ---------------------------------------------------------------- select/sort
 size_t select_state_bytes();
 // k-th smallest (1-based) value among the union of a (stride sa floats) and b

@@ -1,0 +1,783 @@
+// Persistent query engine for sm_100a: whole critical-path queries on the
+// device, for one query or a batch of them, in one cooperative launch.
+//
+// Per query it reproduces the reference's report_paths after the suffix tree
+// (gpucpg/gpucpg.cu:18502-21366) for SHORT_LONG:
+//   roots       one PfxtNode per reachable source, cost (float)dist/SCALE_UP
+//               (18502-18520), optionally trimmed by G-PathGen's initial split
+//               (19136-19179)
+//   split       raised until at least K non-zero paths cost <= split, the
+//               stopping rule of the SHORT_LONG driver (19134-20850)
+//   output      the K cheapest non-zero paths, ascending (21323-21360)
+// The split raises, the closures between them, the top-K select and the
+// segmented sort run back to back between bounded grid barriers; the host
+// launches once and reads the results.
+//
+// Work layout: pending path-graph items of all queries share one pile (the
+// query id rides in the top bits of Item::j), accepted paths share one store
+// (pq[] holds their query); per-query state lives in EngineQuery.  Selection
+// is a three-pass radix select per query over kSelBins-bin histograms;
+// output is a stable LSD radix sort over (query, cost) words.
+//
+// This file is compiled with --use_fast_math like the reference (see
+// pfxt_device.cuh for the child-cost expression).
+#include <climits>
+
+#include "pfxt_device.cuh"
+
+namespace cpg {
+
+namespace {
+
+constexpr int kEngThreads = 256;
+constexpr int kEngWarps = kEngThreads / 32;
+
+#define ENG_SYNC()                                                   \
+  do {                                                               \
+    if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit)) return;  \
+  } while (0)
+
+__device__ __forceinline__ unsigned q_of(const Item& it) {
+  return static_cast<unsigned>(it.j) >> kJBits;
+}
+__device__ __forceinline__ int j_of(const Item& it) {
+  return static_cast<int>(static_cast<unsigned>(it.j) & kJMask);
+}
+__device__ __forceinline__ int pack_j(unsigned q, int j) {
+  return static_cast<int>((q << kJBits) | static_cast<unsigned>(j));
+}
+
+__device__ __forceinline__ Item load_item(const Item* a, unsigned long long i) {
+  const int4 r = __ldcg(reinterpret_cast<const int4*>(a + i));
+  Item it;
+  it.cost = __int_as_float(r.x);
+  it.parent = r.y;
+  it.node = r.z;
+  it.j = r.w;
+  return it;
+}
+
+__device__ __forceinline__ float float_below(float t) {
+  // largest float < t
+  if (t == 0.0f) return -__int_as_float(1);
+  const int b = __float_as_int(t);
+  return __int_as_float(t > 0.0f ? b - 1 : b + 1);
+}
+
+__device__ __forceinline__ void agg_add_u32(unsigned int* base, bool on, unsigned key) {
+  const unsigned m = __match_any_sync(0xffffffffu, on ? key : 0xffffffffu);
+  const int lane = threadIdx.x & 31;
+  if (on && (__ffs(m) - 1) == lane) atomicAdd(base + key, static_cast<unsigned>(__popc(m)));
+}
+
+// ------------------------------------------------------------------ seeding
+// One warp per query: reachable sources become root items; with the
+// reference rule, roots at or below the initial split beyond the first
+// (int)(0.005f*R + 1) (in source-id order) are dropped.
+__device__ void seed_query(const EngineParams& p, int qi) {
+  const int lane = threadIdx.x & 31;
+  EngineQuery& Q = p.q[qi];
+  const int b = Q.src_beg, e = Q.src_end;
+  // number of reachable sources
+  int r = 0;
+  for (int i = b + lane; i < e; i += 32) r += __ldg(p.g.dist + p.srcs[i]) != INT_MAX;
+  r = __reduce_add_sync(0xffffffffu, r);
+  float split = __int_as_float(0x7f800000);
+  int n_short = INT_MAX;
+  if (p.root_ref && r > 0) {
+    const float perc = 0.005f;
+    const int idx = static_cast<int>(perc * r);
+    n_short = static_cast<int>(perc * r + 1);
+    // split = the idx-th smallest reachable root cost (rank by value, then id)
+    float found = 0.f;
+    int hit = 0;
+    for (int i = b + lane; i < e; i += 32) {
+      const int di = __ldg(p.g.dist + p.srcs[i]);
+      if (di == INT_MAX) continue;
+      const float ci = __fdiv_rn(static_cast<float>(di), 10000.0f);
+      int rank = 0;
+      for (int jj = b; jj < e; ++jj) {
+        const int dj = __ldg(p.g.dist + p.srcs[jj]);
+        if (dj == INT_MAX) continue;
+        const float cj = __fdiv_rn(static_cast<float>(dj), 10000.0f);
+        rank += (cj < ci) || (cj == ci && jj < i);
+      }
+      if (rank == idx) {
+        found = ci;
+        hit = 1;
+      }
+    }
+    const unsigned hb = __ballot_sync(0xffffffffu, hit);
+    split = __shfl_sync(0xffffffffu, found, __ffs(hb) - 1);
+  }
+  int short_seen = 0;
+  float rabs = 0.f;
+  for (int base = b; base < e; base += 32) {
+    const int i = base + lane;
+    float c = 0.f;
+    bool reach = false;
+    int src = -1;
+    if (i < e) {
+      src = p.srcs[i];
+      const int d = __ldg(p.g.dist + src);
+      reach = d != INT_MAX;
+      c = __fdiv_rn(static_cast<float>(d), 10000.0f);
+    }
+    const bool low = reach && !(c > split);
+    const unsigned lb = __ballot_sync(0xffffffffu, low);
+    const int before = short_seen + __popc(lb & lanemask_lt());
+    const bool keep = reach && (!low || before < n_short);
+    short_seen += __popc(lb);
+    if (keep) rabs = fmaxf(rabs, fabsf(c));
+    const unsigned long long slot = warp_append(&p.ctr->pend_out, keep);
+    if (keep) {
+      if (slot < p.pend_cap) {
+        Item it;
+        it.cost = c;
+        it.parent = -1;
+        it.node = -2 - src;
+        it.j = pack_j(static_cast<unsigned>(qi), 0);
+        p.pend[0][slot] = it;
+      } else {
+        atomicCAS(&p.ctr->err, kDevOk, kDevCapacity);
+      }
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) rabs = fmaxf(rabs, __shfl_xor_sync(0xffffffffu, rabs, o));
+  if (lane == 0) {
+    Q.root_abs = rabs;
+    Q.done = 0;
+    Q.mode = 0;
+    Q.phases = 0;
+    Q.paths_nz = Q.pend_nz = Q.pend_n = 0;
+    Q.out_lt = Q.out_eq = 0;
+  }
+}
+
+// ------------------------------------------------------------------ select
+// One histogram pass of the per-query radix select.  Elements: accepted
+// paths (when the query's mode selects over them) and pending items.
+__device__ void select_hist(const EngineParams& p, unsigned long long n_paths,
+                            const Item* pend, unsigned long long n_pend, int shift,
+                            int bits) {
+  const unsigned long long tid =
+      static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const unsigned long long nth = static_cast<unsigned long long>(gridDim.x) * blockDim.x;
+  const int hi = shift + bits;
+  const unsigned hmask = hi >= 32 ? 0u : ~((1u << hi) - 1u);
+  const unsigned long long tot = n_paths + n_pend;
+  const unsigned long long pad = (tot + 31) & ~31ull;
+  for (unsigned long long i = tid; i < pad; i += nth) {
+    bool on = false;
+    unsigned key = 0, q = 0;
+    if (i < tot) {
+      float c;
+      int mode;
+      if (i < n_paths) {
+        q = static_cast<unsigned>(__ldcg(p.pq + i));
+        c = __ldcg(p.ps.cost + i);
+        mode = __ldcg(&p.q[q].mode);
+        on = (mode == 2 || mode == 3) && c != 0.0f;
+      } else {
+        const Item it = load_item(pend, i - n_paths);
+        q = q_of(it);
+        c = it.cost;
+        mode = __ldcg(&p.q[q].mode);
+        on = (mode == 2 && c != 0.0f) || mode == 1;
+      }
+      if (on) {
+        key = float_key(c);
+        on = (key & hmask) == (__ldcg(&p.q[q].prefix) & hmask);
+      }
+    }
+    const unsigned bin = (key >> shift) & ((1u << bits) - 1u);
+    agg_add_u32(p.hist, on, q * kSelBins + bin);
+  }
+}
+
+// One warp per selecting query: find the bin holding the krem-th key.
+__device__ void select_pick(const EngineParams& p, int shift, int bits) {
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  const int bins = 1 << bits;
+  const int per = bins / 32;
+  for (int qi = gw; qi < p.nq; qi += nw) {
+    EngineQuery& Q = p.q[qi];
+    if (Q.mode == 0) continue;
+    unsigned int* h = p.hist + static_cast<size_t>(qi) * kSelBins;
+    unsigned long long sum = 0;
+    for (int t = 0; t < per; ++t) sum += h[lane * per + t];
+    unsigned long long incl = sum;
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned long long t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    const unsigned long long k = Q.krem;
+    const unsigned long long excl = incl - sum;
+    const bool mine = excl < k && k <= incl;
+    const unsigned mb = __ballot_sync(0xffffffffu, mine);
+    // k beyond the total (cannot happen when the host-side counts hold):
+    // clamp to the last non-empty chunk
+    const int owner = mb ? __ffs(mb) - 1 : 31;
+    if (lane == owner) {
+      unsigned long long acc = excl;
+      int bin = lane * per;
+      for (int t = 0; t < per - 1; ++t, ++bin) {
+        if (acc + h[bin] >= k) break;
+        acc += h[bin];
+      }
+      Q.prefix |= static_cast<unsigned>(bin) << shift;
+      Q.krem = k - acc;
+    }
+    __syncwarp();
+    for (int t = lane; t < bins; t += 32) h[t] = 0;
+  }
+}
+
+__device__ bool run_select(const EngineParams& p, unsigned long long n_paths,
+                           const Item* pend, unsigned long long n_pend) {
+  const int shifts[3] = {21, 10, 0};
+  const int bits[3] = {11, 11, 10};
+  for (int pass = 0; pass < 3; ++pass) {
+    select_hist(p, n_paths, pend, n_pend, shifts[pass], bits[pass]);
+    if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit)) return false;
+    select_pick(p, shifts[pass], bits[pass]);
+    if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit)) return false;
+  }
+  return true;
+}
+
+// ------------------------------------------------------------------ closure
+__device__ __forceinline__ void route(const EngineParams& p, Item* out,
+                                      unsigned long long* out_cnt, Item* pend_out,
+                                      bool exists, const Item& it, float lim) {
+  const bool take = exists && it.cost <= lim;
+  const bool defer = exists && !take;
+  const unsigned long long a = warp_append(out_cnt, take);
+  if (take) {
+    if (a < p.front_cap) out[a] = it;
+    else atomicCAS(&p.ctr->err, kDevOk, kDevCapacity);
+  }
+  const unsigned long long b = warp_append(&p.ctr->pend_out, defer);
+  if (defer) {
+    if (b < p.pend_cap) pend_out[b] = it;
+    else atomicCAS(&p.ctr->err, kDevOk, kDevCapacity);
+  }
+}
+
+// Rounds over the frontier until it is empty.  Returns false on error.
+__device__ bool run_closure(const EngineParams& p, Item* pend_out) {
+  const unsigned long long tid =
+      static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const unsigned long long nth = static_cast<unsigned long long>(gridDim.x) * blockDim.x;
+  int r = 0;
+  for (;;) {
+    volatile unsigned long long* fc = p.ctr->frontier;
+    const unsigned long long n_cur = fc[r % 3];
+    if (n_cur == 0) break;
+    if (n_cur > p.front_cap) {
+      atomicCAS(&p.ctr->err, kDevOk, kDevCapacity);
+      return false;
+    }
+    const Item* in = p.front[r & 1];
+    Item* out = p.front[(r + 1) & 1];
+    unsigned long long* out_cnt = &p.ctr->frontier[(r + 1) % 3];
+    if (blockIdx.x == 0 && threadIdx.x == 0) p.ctr->frontier[(r + 2) % 3] = 0;
+    const unsigned long long n_pad = (n_cur + 31) & ~31ull;
+    for (unsigned long long i = tid; i < n_pad; i += nth) {
+      const bool valid = i < n_cur;
+      Item it;
+      it.cost = 0.f;
+      it.parent = -1;
+      it.node = -1;
+      it.j = 0;
+      if (valid) it = load_item(in, i);
+      const unsigned q = q_of(it);
+      const int jj = j_of(it);
+      const unsigned long long qp = warp_append(&p.ctr->paths, valid);
+      bool stored = false;
+      int to = -1;
+      HeapNode hn;
+      hn.vtx = -1;
+      hn.left = -1;
+      hn.right = -1;
+      float lim = 0.f, tie = 0.f;
+      if (valid) {
+        lim = __ldcg(&p.q[q].lim);
+        tie = __ldcg(&p.q[q].tie);
+        int from = -1, level = 0;
+        if (it.node <= -2) {
+          to = -(it.node + 2);
+        } else {
+          hn = load_node(p.g.hnodes, it.node);
+          from = hn.vtx;
+          const DevSidetrack d = load_dev(p.g.dev, __ldg(p.g.adjp + from) + jj);
+          to = d.head;
+          level = __ldcg(p.ps.level + it.parent) + 1;
+        }
+        if (qp < p.ps.cap) {
+          p.ps.cost[qp] = it.cost;
+          p.ps.parent[qp] = it.parent;
+          p.ps.from[qp] = from;
+          p.ps.to[qp] = to;
+          p.ps.level[qp] = level;
+          p.pq[qp] = static_cast<int>(q);
+          stored = true;
+        } else {
+          atomicCAS(&p.ctr->err, kDevOk, kDevCapacity);
+        }
+      }
+      // a path costing exactly the final split is reported, not expanded
+      const bool expand = stored && !(it.cost == tie);
+      const bool sib = expand && it.node >= 0;
+      const float pcost = sib ? __ldcg(p.ps.cost + it.parent) : 0.f;
+      {
+        Item c;
+        c.parent = it.parent;
+        int cn, cj;
+        bool ex;
+        cn = jj == 0 ? hn.left : it.node;
+        cj = jj == 0 ? 0 : 2 * jj + 1;
+        ex = sib && make_candidate(p.g, cn, cj, pcost, c.cost);
+        c.node = cn;
+        c.j = pack_j(q, cj);
+        route(p, out, out_cnt, pend_out, ex, c, lim);
+        cn = jj == 0 ? hn.right : it.node;
+        cj = jj == 0 ? 0 : 2 * jj + 2;
+        ex = sib && make_candidate(p.g, cn, cj, pcost, c.cost);
+        c.node = cn;
+        c.j = pack_j(q, cj);
+        route(p, out, out_cnt, pend_out, ex, c, lim);
+        ex = sib && jj == 0 && make_candidate(p.g, it.node, 1, pcost, c.cost);
+        c.node = it.node;
+        c.j = pack_j(q, 1);
+        route(p, out, out_cnt, pend_out, ex, c, lim);
+        ex = sib && jj == 0 && make_candidate(p.g, it.node, 2, pcost, c.cost);
+        c.j = pack_j(q, 2);
+        route(p, out, out_cnt, pend_out, ex, c, lim);
+      }
+      {
+        Item c;
+        c.parent = static_cast<int>(qp);
+        c.node = expand ? __ldg(p.g.ht_root + to) : -1;
+        c.j = pack_j(q, 0);
+        const bool ex = expand && make_candidate(p.g, c.node, 0, it.cost, c.cost);
+        route(p, out, out_cnt, pend_out, ex, c, lim);
+      }
+    }
+    if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit)) return false;
+    ++r;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) p.ctr->rounds += r;
+  return true;
+}
+
+// ------------------------------------------------------------------ sort
+// Stable LSD pass over n (query, cost key, path) triples, 8-bit digit taken
+// from the cost key (on_q == 0) or the query id.  Each block owns one
+// contiguous tile.
+__device__ bool lsd_pass(const EngineParams& p, unsigned long long n, int src,
+                         int shift, bool on_q) {
+  __shared__ unsigned int running[256];
+  __shared__ unsigned int wcount[kEngWarps][256];
+  __shared__ unsigned int dbase[256];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const unsigned G = gridDim.x;
+  const unsigned long long tile = (n + G - 1) / G;
+  const unsigned long long t0 = blockIdx.x * tile;
+  const unsigned long long t1 = t0 + tile < n ? t0 + tile : n;
+  const unsigned int* kin = p.keys[src];
+  const unsigned int* qin = p.qids[src];
+  const unsigned int* vin = p.vals[src];
+  auto digit_of = [&](unsigned long long i) -> unsigned {
+    return ((on_q ? __ldcg(qin + i) : __ldcg(kin + i)) >> shift) & 255u;
+  };
+  // 1. tile histogram
+  running[threadIdx.x] = 0;
+  __syncthreads();
+  for (unsigned long long i = t0 + threadIdx.x; i < t1; i += blockDim.x)
+    atomicAdd(&running[digit_of(i)], 1u);
+  __syncthreads();
+  p.sort_hist[threadIdx.x * G + blockIdx.x] = running[threadIdx.x];
+  if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit)) return false;
+  // 2. one warp per digit: exclusive scan across tiles
+  {
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int d = gw; d < 256; d += nw) {
+      unsigned int carry = 0;
+      for (unsigned b0 = 0; b0 < G; b0 += 32) {
+        const unsigned b = b0 + lane;
+        const unsigned x = b < G ? p.sort_hist[d * G + b] : 0u;
+        unsigned incl = x;
+        for (int o = 1; o < 32; o <<= 1) {
+          const unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += t;
+        }
+        if (b < G) p.sort_hist[d * G + b] = carry + incl - x;
+        carry += __shfl_sync(0xffffffffu, incl, 31);
+      }
+      if (lane == 0) p.digit_tot[d] = carry;
+    }
+  }
+  if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit)) return false;
+  // 3. digit bases, then a stable scatter of the tile
+  if (threadIdx.x == 0) {
+    unsigned acc = 0;
+    for (int d = 0; d < 256; ++d) {
+      dbase[d] = acc;
+      acc += __ldcg(p.digit_tot + d);
+    }
+  }
+  __syncthreads();
+  running[threadIdx.x] = dbase[threadIdx.x] + __ldcg(p.sort_hist + threadIdx.x * G + blockIdx.x);
+  for (int w = 0; w < kEngWarps; ++w) wcount[w][threadIdx.x] = 0;
+  __syncthreads();
+  unsigned int* kout = p.keys[src ^ 1];
+  unsigned int* qout = p.qids[src ^ 1];
+  unsigned int* vout = p.vals[src ^ 1];
+  for (unsigned long long c0 = t0; c0 < t1; c0 += blockDim.x) {
+    const unsigned long long i = c0 + threadIdx.x;
+    const bool valid = i < t1;
+    unsigned d = 256u, kk = 0, qq = 0, vv = 0;
+    if (valid) {
+      kk = __ldcg(kin + i);
+      qq = __ldcg(qin + i);
+      vv = __ldcg(vin + i);
+      d = ((on_q ? qq : kk) >> shift) & 255u;
+    }
+    const unsigned peers = __match_any_sync(0xffffffffu, d);
+    const unsigned lrank = __popc(peers & lanemask_lt());
+    if (valid && lrank == 0) wcount[wid][d] = __popc(peers);
+    __syncthreads();
+    if (valid) {
+      unsigned pos = running[d] + lrank;
+      for (int w = 0; w < wid; ++w) pos += wcount[w][d];
+      kout[pos] = kk;
+      qout[pos] = qq;
+      vout[pos] = vv;
+    }
+    __syncthreads();
+    {
+      unsigned s = 0;
+      for (int w = 0; w < kEngWarps; ++w) {
+        s += wcount[w][threadIdx.x];
+        wcount[w][threadIdx.x] = 0;
+      }
+      running[threadIdx.x] += s;
+    }
+    __syncthreads();
+  }
+  return grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit);
+}
+
+// ------------------------------------------------------------------ kernel
+__global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
+  const unsigned long long tid =
+      static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const unsigned long long nth = static_cast<unsigned long long>(gridDim.x) * blockDim.x;
+  const int gw = static_cast<int>(tid >> 5);
+  const int nw = static_cast<int>(nth >> 5);
+
+  // seed roots (pending pile 0)
+  for (int qi = gw; qi < p.nq; qi += nw) seed_query(p, qi);
+  ENG_SYNC();
+  int pin = 0;
+  unsigned long long n_pend = *reinterpret_cast<volatile unsigned long long*>(&p.ctr->pend_out);
+  unsigned long long n_paths = 0;
+
+  for (int phase = 0;; ++phase) {
+    const Item* pend = p.pend[pin];
+    Item* pend_next = p.pend[pin ^ 1];
+    // A. per-query counts
+    {
+      const unsigned long long tot = n_paths + n_pend;
+      const unsigned long long pad = (tot + 31) & ~31ull;
+      for (unsigned long long i = tid; i < pad; i += nth) {
+        bool path_nz = false, pend_any = false, pend_nz = false;
+        unsigned q = 0, key = 0xffffffffu;
+        if (i < n_paths) {
+          q = static_cast<unsigned>(__ldcg(p.pq + i));
+          path_nz = __ldcg(p.ps.cost + i) != 0.0f;
+        } else if (i < tot) {
+          const Item it = load_item(pend, i - n_paths);
+          q = q_of(it);
+          pend_any = true;
+          pend_nz = it.cost != 0.0f;
+          key = float_key(it.cost);
+        }
+        {
+          const unsigned m = __match_any_sync(0xffffffffu, path_nz ? q : 0xffffffffu);
+          if (path_nz && (__ffs(m) - 1) == static_cast<int>(threadIdx.x & 31))
+            atomicAdd(&p.q[q].paths_nz, static_cast<unsigned long long>(__popc(m)));
+        }
+        {
+          const unsigned m = __match_any_sync(0xffffffffu, pend_any ? q : 0xffffffffu);
+          const unsigned mz = __match_any_sync(0xffffffffu, pend_nz ? q : 0xffffffffu);
+          const int lane = threadIdx.x & 31;
+          if (pend_any && (__ffs(m) - 1) == lane)
+            atomicAdd(&p.q[q].pend_n, static_cast<unsigned long long>(__popc(m)));
+          if (pend_nz && (__ffs(mz) - 1) == lane)
+            atomicAdd(&p.q[q].pend_nz, static_cast<unsigned long long>(__popc(mz)));
+        }
+        (void)key;
+      }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) p.ctr->active = 0;
+    ENG_SYNC();
+    // B. per-query decision
+    for (unsigned long long qi = tid; qi < static_cast<unsigned long long>(p.nq); qi += nth) {
+      EngineQuery& Q = p.q[qi];
+      Q.mode = 0;
+      if (Q.done) continue;
+      Q.prefix = 0;
+      // Every path costing <= the last phase's limit is accepted, so once
+      // K non-zero paths are, the K-th of them is the answer's K-th cost and
+      // the final phase only sweeps items within the rounding margin.
+      if (Q.paths_nz >= static_cast<unsigned long long>(Q.k)) {
+        Q.mode = 2;                       // final: the k-th of paths+pending
+        Q.krem = static_cast<unsigned long long>(Q.k);
+        Q.ksel = Q.krem;
+      } else if (Q.pend_n > 0) {
+        Q.mode = 1;                       // grow by count
+        unsigned long long j = 4 * (Q.paths_nz + 1);
+        if (j < 64) j = 64;
+        if (j > Q.pend_n) j = Q.pend_n;
+        Q.krem = j;
+        Q.ksel = j;
+      } else {
+        Q.done = 1;                       // every path enumerated
+        continue;
+      }
+      ++Q.phases;
+      atomicAdd(&p.ctr->active, 1);
+    }
+    ENG_SYNC();
+    if (*reinterpret_cast<volatile int*>(&p.ctr->active) == 0) break;
+    // C. per-query radix select
+    if (!run_select(p, n_paths, pend, n_pend)) return;
+    // D. split and acceptance limit
+    for (unsigned long long qi = tid; qi < static_cast<unsigned long long>(p.nq); qi += nth) {
+      EngineQuery& Q = p.q[qi];
+      if (Q.mode == 0) continue;
+      const float t = key_float(Q.prefix);
+      Q.t = t;
+      if (Q.mode == 2) {
+        const float a = fmaxf(fmaxf(fabsf(t), Q.root_abs), 1.0f);
+        Q.lim = t + a * 0x1p-16f;
+        Q.tie = t;
+      } else {
+        // accept strictly below the split when anything pending is cheaper
+        // than it (ksel - krem items are), so a tie group at the split waits
+        Q.lim = Q.ksel > Q.krem ? float_below(t) : t;
+        Q.tie = __int_as_float(0x7fc00000);  // NaN: expand every path
+      }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      p.ctr->frontier[0] = 0;
+      p.ctr->frontier[1] = 0;
+      p.ctr->frontier[2] = 0;
+      p.ctr->pend_out = 0;
+    }
+    ENG_SYNC();
+    // E. promote pending items under their query's limit
+    {
+      const unsigned long long pad = (n_pend + 31) & ~31ull;
+      for (unsigned long long i = tid; i < pad; i += nth) {
+        bool take = false, keep = false;
+        Item it;
+        it.cost = 0.f;
+        if (i < n_pend) {
+          it = load_item(pend, i);
+          const EngineQuery& Q = p.q[q_of(it)];
+          const int mode = __ldcg(&Q.mode);
+          const int done = __ldcg(&Q.done);
+          take = mode != 0 && it.cost <= __ldcg(&Q.lim);
+          keep = !take && !done;
+        }
+        const unsigned long long a = warp_append(&p.ctr->frontier[0], take);
+        if (take) {
+          if (a < p.front_cap) p.front[0][a] = it;
+          else atomicCAS(&p.ctr->err, kDevOk, kDevCapacity);
+        }
+        const unsigned long long b = warp_append(&p.ctr->pend_out, keep);
+        if (keep) {
+          if (b < p.pend_cap) pend_next[b] = it;
+          else atomicCAS(&p.ctr->err, kDevOk, kDevCapacity);
+        }
+      }
+    }
+    ENG_SYNC();
+    // F. closure
+    if (!run_closure(p, pend_next)) return;
+    // G. final-mode queries are answered; counts restart
+    for (unsigned long long qi = tid; qi < static_cast<unsigned long long>(p.nq); qi += nth) {
+      EngineQuery& Q = p.q[qi];
+      if (Q.mode == 2) Q.done = 1;
+      Q.paths_nz = Q.pend_nz = Q.pend_n = 0;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) p.ctr->phases = phase + 1;
+    ENG_SYNC();
+    n_paths = *reinterpret_cast<volatile unsigned long long*>(&p.ctr->paths);
+    n_pend = *reinterpret_cast<volatile unsigned long long*>(&p.ctr->pend_out);
+    pin ^= 1;
+  }
+
+  // ---------------------------------------------------------------- output
+  if (n_paths > p.ps.cap) {
+    atomicCAS(&p.ctr->err, kDevOk, kDevCapacity);
+    return;
+  }
+  // H. non-zero paths per query
+  {
+    const unsigned long long pad = (n_paths + 31) & ~31ull;
+    for (unsigned long long i = tid; i < pad; i += nth) {
+      bool nz = false;
+      unsigned q = 0;
+      if (i < n_paths) {
+        q = static_cast<unsigned>(__ldcg(p.pq + i));
+        nz = __ldcg(p.ps.cost + i) != 0.0f;
+      }
+      const unsigned m = __match_any_sync(0xffffffffu, nz ? q : 0xffffffffu);
+      if (nz && (__ffs(m) - 1) == static_cast<int>(threadIdx.x & 31))
+        atomicAdd(&p.q[q].paths_nz, static_cast<unsigned long long>(__popc(m)));
+      if (i < n_paths) p.rank_of[i] = -1;
+    }
+  }
+  ENG_SYNC();
+  for (unsigned long long qi = tid; qi < static_cast<unsigned long long>(p.nq); qi += nth) {
+    EngineQuery& Q = p.q[qi];
+    const unsigned long long k = static_cast<unsigned long long>(Q.k);
+    Q.k_out = Q.paths_nz < k ? Q.paths_nz : k;
+    Q.mode = Q.k_out > 0 ? 3 : 0;
+    Q.prefix = 0;
+    Q.krem = Q.k_out;
+    Q.out_lt = Q.out_eq = 0;
+  }
+  ENG_SYNC();
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    unsigned long long acc = 0;
+    for (int qi = 0; qi < p.nq; ++qi) {
+      p.q[qi].out_off = acc;
+      acc += p.q[qi].k_out;
+    }
+    p.ctr->out_total = acc;
+  }
+  if (!run_select(p, n_paths, nullptr, 0)) return;
+  const unsigned long long n_out = *reinterpret_cast<volatile unsigned long long*>(&p.ctr->out_total);
+  if (n_out > p.out_cap) {
+    atomicCAS(&p.ctr->err, kDevOk, kDevCapacity);
+    return;
+  }
+  // J. compaction into per-query segments: keys below the k-th, then the
+  // first ones equal to it
+  {
+    const unsigned long long pad = (n_paths + 31) & ~31ull;
+    for (unsigned long long i = tid; i < pad; i += nth) {
+      bool lt = false, eq = false;
+      unsigned q = 0, key = 0;
+      if (i < n_paths) {
+        q = static_cast<unsigned>(__ldcg(p.pq + i));
+        const float c = __ldcg(p.ps.cost + i);
+        const EngineQuery& Q = p.q[q];
+        if (c != 0.0f && __ldcg(&Q.mode) == 3) {
+          key = float_key(c);
+          const unsigned kth = __ldcg(&Q.prefix);
+          lt = key < kth;
+          eq = key == kth;
+        }
+      }
+      const int lane = threadIdx.x & 31;
+      const unsigned ml = __match_any_sync(0xffffffffu, lt ? q : 0xffffffffu);
+      unsigned long long bl = 0;
+      if (lt && (__ffs(ml) - 1) == lane) bl = atomicAdd(&p.q[q].out_lt, static_cast<unsigned long long>(__popc(ml)));
+      bl = __shfl_sync(0xffffffffu, bl, lt ? __ffs(ml) - 1 : lane);
+      const unsigned me = __match_any_sync(0xffffffffu, eq ? q : 0xffffffffu);
+      unsigned long long be = 0;
+      if (eq && (__ffs(me) - 1) == lane) be = atomicAdd(&p.q[q].out_eq, static_cast<unsigned long long>(__popc(me)));
+      be = __shfl_sync(0xffffffffu, be, eq ? __ffs(me) - 1 : lane);
+      if (lt || eq) {
+        const EngineQuery& Q = p.q[q];
+        const unsigned long long need_eq = __ldcg(&Q.krem);
+        const unsigned long long n_lt = __ldcg(&Q.k_out) - need_eq;
+        const unsigned long long off = __ldcg(&Q.out_off);
+        unsigned long long slot = ~0ull;
+        if (lt) {
+          const unsigned long long r = bl + __popc(ml & lanemask_lt());
+          if (r < n_lt) slot = off + r;
+        } else {
+          const unsigned long long r = be + __popc(me & lanemask_lt());
+          if (r < need_eq) slot = off + n_lt + r;
+        }
+        if (slot != ~0ull) {
+          p.keys[0][slot] = key;
+          p.qids[0][slot] = q;
+          p.vals[0][slot] = static_cast<unsigned>(i);
+        }
+      }
+    }
+  }
+  ENG_SYNC();
+  // K. stable LSD sort over (query, cost)
+  int src = 0;
+  for (int pass = 0; pass < 4; ++pass) {
+    if (!lsd_pass(p, n_out, src, pass * 8, false)) return;
+    src ^= 1;
+  }
+  for (int shift = 0; (p.nq - 1) >> shift; shift += 8) {
+    if (!lsd_pass(p, n_out, src, shift, true)) return;
+    src ^= 1;
+  }
+  // L. ranks within each query's list, then M. emission
+  for (unsigned long long i = tid; i < n_out; i += nth) {
+    const unsigned q = __ldcg(p.qids[src] + i);
+    p.rank_of[__ldcg(p.vals[src] + i)] =
+        static_cast<int>(i - __ldcg(&p.q[q].out_off));
+  }
+  ENG_SYNC();
+  for (unsigned long long i = tid; i < n_out; i += nth) {
+    const unsigned idx = __ldcg(p.vals[src] + i);
+    const float c = __ldcg(p.ps.cost + idx);
+    p.out_cost[i] = c;
+    if (p.out_nodes) {
+      cpg_path_node nd;
+      nd.level = __ldcg(p.ps.level + idx);
+      nd.from = __ldcg(p.ps.from + idx);
+      nd.to = __ldcg(p.ps.to + idx);
+      const int par = __ldcg(p.ps.parent + idx);
+      nd.parent = par >= 0 ? __ldcg(p.rank_of + par) : -1;
+      nd.num_children = 0;
+      nd.slack = c;
+      p.out_nodes[i] = nd;
+    }
+  }
+  // the sorted path indices stay in vals[src]; the host learns which buffer
+  if (blockIdx.x == 0 && threadIdx.x == 0) p.ctr->sorted_buf = src;
+}
+
+}  // namespace
+
+int engine_grid(int device, int* grid_out) {
+  int sms = 0, per_sm = 0;
+  cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  if (e != cudaSuccess) return e;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, engine_kernel, kEngThreads, 0);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) per_sm = 1;
+  *grid_out = sms * per_sm;
+  return cudaSuccess;
+}
+
+int launch_engine(const EngineParams& p, int device, void* stream) {
+  int grid = 0;
+  cudaError_t e = static_cast<cudaError_t>(engine_grid(device, &grid));
+  if (e != cudaSuccess) return e;
+  EngineParams pp = p;
+  void* args[] = {&pp};
+  return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(engine_kernel), dim3(grid),
+                                     dim3(kEngThreads), args, 0,
+                                     static_cast<cudaStream_t>(stream));
+}
+
+}  // namespace cpg

@@ -72,7 +72,9 @@ typedef struct {
   int64_t hbm_budget_bytes; /* cap on per-query device memory; 0 = none */
   uint32_t spin_limit;      /* grid-barrier poll limit; 0 = default */
   int32_t root_seeding;     /* cpg_root_seeding */
-  int32_t reserved[7];
+  int32_t reserved[7];      /* [0] = 1: step the split raises from the host
+                               (one kernel sequence per raise) instead of the
+                               persistent device engine; for A/B checks */
 } cpg_options;
 
 typedef struct cpg_handle cpg_handle;

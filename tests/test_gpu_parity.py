@@ -245,3 +245,18 @@ def test_cpp_shim_runs(tmp_path):
     got = np.array([float(x) for x in out.stdout.split()], np.float32)
     want = oracle.OracleGraph.from_edges(n, src, dst, w).closure_topk(500)[0]["slack"]
     np.testing.assert_allclose(got, want, rtol=RTOL)
+
+
+@pytest.mark.parametrize("name", ["small_f32_s11", "single20k_int", "tv80_unit_wgts"])
+def test_host_stepped_and_engine_agree(name):
+    """The persistent device engine and the host-stepped phase loop return
+    the same costs."""
+    k = 3000
+    n, src, dst, w = _load(name)
+    out = []
+    for hs in (False, True):
+        with cpg_b200.CpGen(division=cpg_b200.DIV_IEEE, host_stepped=hs) as g:
+            g.load_edges(n, src, dst, w)
+            g.report_paths(k)
+            out.append(g.get_slacks(k))
+    assert np.array_equal(out[0].view(np.uint32), out[1].view(np.uint32))

@@ -500,12 +500,13 @@ int try_query(cpg_handle* h, unsigned long long k) {
       final_phase = true;
     } else {
       // too few known: grow geometrically by count.  Promoting the j cheapest
-      // pending items (j ~ twice the accepted paths) keeps the split away
+      // pending items (j ~ four times the accepted paths, at most half the
+      // pile) keeps the split away
       // from expensive outliers, whose closure could be exponentially large;
       // accepting only costs strictly below the j-th keeps a tie group at
       // that cost for a later phase.
-      const unsigned long long j =
-          std::min<unsigned long long>(n_pend, std::max<unsigned long long>(64, 4 * (n_paths + 1)));
+      const unsigned long long j = std::min<unsigned long long>(
+          (n_pend + 1) / 2, std::max<unsigned long long>(64, 4 * (n_paths + 1)));
       st = select_kth(h, pend_cost_in, n_pend, 4, nullptr, 0, 1, j, 0, t);
       if (st != CPG_OK) return st;
       const float below = std::nextafter(t, -INFINITY);

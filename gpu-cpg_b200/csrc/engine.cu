@@ -541,9 +541,13 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
         Q.ksel = Q.krem;
       } else if (Q.pend_n > 0) {
         Q.mode = 1;                       // grow by count
+        // promote ~4x the accepted count, but never more than half the
+        // pile: the top of the pile holds the expensive outliers whose
+        // closure can be exponentially large
         unsigned long long j = 4 * (Q.paths_nz + 1);
         if (j < 64) j = 64;
-        if (j > Q.pend_n) j = Q.pend_n;
+        const unsigned long long half = (Q.pend_n + 1) / 2;
+        if (j > half) j = half;
         Q.krem = j;
         Q.ksel = j;
       } else {
@@ -629,22 +633,9 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
     atomicCAS(&p.ctr->err, kDevOk, kDevCapacity);
     return;
   }
-  // H. non-zero paths per query
-  {
-    const unsigned long long pad = (n_paths + 31) & ~31ull;
-    for (unsigned long long i = tid; i < pad; i += nth) {
-      bool nz = false;
-      unsigned q = 0;
-      if (i < n_paths) {
-        q = static_cast<unsigned>(__ldcg(p.pq + i));
-        nz = __ldcg(p.ps.cost + i) != 0.0f;
-      }
-      const unsigned m = __match_any_sync(0xffffffffu, nz ? q : 0xffffffffu);
-      if (nz && (__ffs(m) - 1) == static_cast<int>(threadIdx.x & 31))
-        atomicAdd(&p.q[q].paths_nz, static_cast<unsigned long long>(__popc(m)));
-      if (i < n_paths) p.rank_of[i] = -1;
-    }
-  }
+  // H. the last phase's counts (step A of the pass that found every query
+  // done) are current: no path was accepted after them
+  for (unsigned long long i = tid; i < n_paths; i += nth) p.rank_of[i] = -1;
   ENG_SYNC();
   for (unsigned long long qi = tid; qi < static_cast<unsigned long long>(p.nq); qi += nth) {
     EngineQuery& Q = p.q[qi];

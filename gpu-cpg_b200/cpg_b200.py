@@ -115,6 +115,7 @@ def _load():
         "cpg_reset": (C.c_int, [H]),
         "cpg_get_stats": (C.c_int, [H, P(Stats)]),
         "cpg_sync": (C.c_int, [H]),
+        "cpg_select_topk": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, P(C.c_int64), C.c_void_p]),
         "cpg_gen_params_init": (None, [P(GenParams)]),
         "cpg_dag_generate": (C.c_int, [P(GenParams), P(C.c_void_p)]),
         "cpg_dag_sizes": (C.c_int, [C.c_void_p, P(C.c_int32), P(C.c_int32)]),
@@ -333,6 +334,15 @@ class CpGen:
 
     def sync(self):
         self._check(lib.cpg_sync(self._h), "sync")
+
+
+def select_topk(d_costs: int, n: int, k: int, d_out: int, stream: int | None = None) -> int:
+    """cpg_select_topk on device pointers (e.g. torch tensors' data_ptr())."""
+    got = C.c_int64()
+    st = lib.cpg_select_topk(d_costs, int(n), int(k), d_out, C.byref(got), stream)
+    if st != CPG_OK:
+        raise CpgError(st, "cpg_select_topk failed")
+    return got.value
 
 
 def header_symbols(path: str = HEADER_PATH) -> list[str]:

@@ -1072,6 +1072,46 @@ cpg_status cpg_sync(cpg_handle* h) {
   return CPG_OK;
 }
 
+// ---------------------------------------------------------------- top-K
+
+cpg_status cpg_select_topk(const float* d_costs, int64_t n, int64_t k, float* d_out,
+                           int64_t* n_out, void* stream) {
+  if (n < 0 || k < 0 || !n_out || (n > 0 && !d_costs) || (k > 0 && !d_out))
+    return CPG_ERR_INVALID;
+  *n_out = 0;
+  if (n == 0 || k == 0) return CPG_OK;
+  if (n > (int64_t{1} << 32) - 1 || k > (int64_t{1} << 31))
+    return CPG_ERR_INVALID;
+  const unsigned long long kk = static_cast<unsigned long long>(std::min(k, n));
+  const size_t words = 2048 + 4 + 2 + 1 + 4 * kk + topk_sort_hist_words(kk) + 4;
+  void* buf = nullptr;
+  if (cudaMalloc(&buf, words * 4 + 64) != cudaSuccess) {
+    cudaGetLastError();
+    return CPG_ERR_OOM;
+  }
+  char* b = static_cast<char*>(buf);
+  TopkScratch sc;
+  sc.hist = reinterpret_cast<unsigned int*>(b);
+  sc.state = b + 2048 * 4;
+  sc.counts = reinterpret_cast<unsigned long long*>(b + 2048 * 4 + 16);
+  sc.cnt = sc.counts + 2;
+  sc.tkey = reinterpret_cast<unsigned int*>(sc.cnt + 2);
+  sc.keys = sc.tkey + 4;
+  sc.vals = sc.keys + 2 * kk;
+  sc.sort_hist = sc.vals + 2 * kk;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cudaError_t e = cudaMemsetAsync(sc.hist, 0, 2048 * 4, s);
+  unsigned long long got = 0;
+  if (e == cudaSuccess)
+    e = static_cast<cudaError_t>(launch_topk_costs(d_costs, static_cast<unsigned long long>(n),
+                                                   kk, sc, d_out, &got, s));
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaFree(buf);
+  if (e != cudaSuccess) return e == cudaErrorMemoryAllocation ? CPG_ERR_OOM : CPG_ERR_CUDA;
+  *n_out = static_cast<int64_t>(got);
+  return CPG_OK;
+}
+
 // ---------------------------------------------------------------- generator
 
 struct cpg_dag {

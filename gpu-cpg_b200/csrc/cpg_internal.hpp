@@ -307,6 +307,22 @@ int launch_build_graph(const int32_t* adjp, const int32_t* adj, const float* w,
                        int32_t* iadj, int32_t* srcs, int32_t* n_srcs,
                        int32_t* scratch, void* stream);
 
+// Standalone top-K of a device cost array (select_sort.cu).
+struct TopkScratch {
+  unsigned int* hist;             // 2048 words, zero on entry and on exit
+  void* state;                    // select state, 16 bytes
+  unsigned long long* counts;     // 2 words
+  unsigned int* tkey;             // 1 word
+  unsigned int* keys;             // 2*k words
+  unsigned int* vals;             // 2*k words
+  unsigned int* sort_hist;        // topk_sort_hist_words(k) words
+  unsigned long long* cnt;        // 2 words
+};
+size_t topk_sort_hist_words(unsigned long long k);
+int launch_topk_costs(const float* costs, unsigned long long n, unsigned long long k,
+                      const TopkScratch& s, float* out, unsigned long long* n_out,
+                      void* stream);
+
 // Scatter new delays into the device fan-out edges.
 int launch_scatter_delays(DevEdge* edges, const int32_t* eids, const float* w,
                           int64_t count, void* stream);

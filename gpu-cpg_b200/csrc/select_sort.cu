@@ -367,3 +367,77 @@ int launch_emit_topk(const PathStore& ps, unsigned long long n_paths,
 }
 
 }  // namespace cpg
+
+namespace cpg {
+
+namespace {
+
+__global__ void keys_to_costs_kernel(const unsigned int* keys, unsigned long long n,
+                                     float* out) {
+  for (unsigned long long i = static_cast<unsigned long long>(blockIdx.x) * blockDim.x +
+                              threadIdx.x;
+       i < n; i += static_cast<unsigned long long>(gridDim.x) * blockDim.x)
+    out[i] = key_float(keys[i]);
+}
+
+}  // namespace
+
+size_t topk_sort_hist_words(unsigned long long k) {
+  return 256 * ((k + kSortTile - 1) / kSortTile);
+}
+
+// The k smallest non-zero values of costs[0..n), ascending, into out.  Two
+// stages separated by a host read of the non-zero count: count, then select
+// + compact + sort + gather.  s.hist must hold 2048 zero words (the select
+// leaves them zero again); s.keys/s.vals 2*k words each.
+int launch_topk_costs(const float* costs, unsigned long long n, unsigned long long k,
+                      const TopkScratch& s, float* out, unsigned long long* n_out,
+                      void* stream) {
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  *n_out = 0;
+  if (n == 0 || k == 0) return cudaSuccess;
+  cudaError_t e = cudaMemsetAsync(s.counts, 0, 2 * sizeof(unsigned long long), st);
+  if (e != cudaSuccess) return e;
+  const unsigned int all = 0xffffffffu;
+  e = cudaMemcpyAsync(s.tkey, &all, 4, cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return e;
+  count_le_kernel<<<grid_for(n, 256, 148 * 8), 256, 0, st>>>(costs, n, 1, s.tkey, s.counts);
+  unsigned long long host_counts[2] = {0, 0};
+  e = cudaMemcpyAsync(host_counts, s.counts, sizeof(host_counts), cudaMemcpyDeviceToHost, st);
+  if (e != cudaSuccess) return e;
+  e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return e;
+  const unsigned long long kk = host_counts[1] < k ? host_counts[1] : k;
+  *n_out = kk;
+  if (kk == 0) return cudaSuccess;
+  int launches = 0;
+  e = static_cast<cudaError_t>(launch_select_kth(costs, n, 1, nullptr, 0, 1, kk, 1, s.state,
+                                                 s.hist, st, &launches));
+  if (e != cudaSuccess) return e;
+  cudaMemsetAsync(s.cnt, 0, 2 * sizeof(unsigned long long), st);
+  cudaMemsetAsync(s.vals, 0, kk * sizeof(unsigned int), st);
+  compact_kernel<<<grid_for(n, 256, 148 * 16), 256, 0, st>>>(
+      costs, n, static_cast<const SelectState*>(s.state), kk, s.keys, s.vals, s.cnt);
+  const int nblocks = static_cast<int>((kk + kSortTile - 1) / kSortTile);
+  unsigned int* kin = s.keys;
+  unsigned int* vin = s.vals;
+  unsigned int* kout = s.keys + kk;
+  unsigned int* vout = s.vals + kk;
+  for (int pass = 0; pass < 4; ++pass) {
+    const int shift = pass * 8;
+    sort_hist_kernel<<<nblocks, kSortThreads, 0, st>>>(kin, kk, shift, s.sort_hist, nblocks);
+    sort_scan_kernel<<<1, 1024, 0, st>>>(s.sort_hist, 256 * nblocks);
+    sort_scatter_kernel<<<nblocks, kSortThreads, 0, st>>>(kin, vin, kout, vout, kk, shift,
+                                                          s.sort_hist, nblocks);
+    unsigned int* t = kin;
+    kin = kout;
+    kout = t;
+    t = vin;
+    vin = vout;
+    vout = t;
+  }
+  keys_to_costs_kernel<<<grid_for(kk, 256, 148 * 8), 256, 0, st>>>(kin, kk, out);
+  return cudaGetLastError();
+}
+
+}  // namespace cpg

@@ -179,6 +179,18 @@ cpg_status cpg_get_stats(const cpg_handle* h, cpg_stats* out);
 /* Synchronise the handle's stream. */
 cpg_status cpg_sync(cpg_handle* h);
 
+/* ------------------------------------------------------------ top-K */
+/* The k smallest non-zero values of a device array of path costs, ascending,
+ * written to the device buffer d_out (room for k floats); *n_out receives
+ * min(k, number of non-zero values).  This is the final step of report_paths
+ * on its own: the reference sorts the whole short pile and drops zero-cost
+ * nodes (gpucpg.cu:21323-21360); here a radix select finds the k-th value and
+ * only the k survivors are radix-sorted.  Runs on `stream` (a cudaStream_t,
+ * NULL for the default stream) and returns after the result is written.
+ * Allocates and frees its own device scratch. */
+cpg_status cpg_select_topk(const float* d_costs, int64_t n, int64_t k,
+                           float* d_out, int64_t* n_out, void* stream);
+
 /* ------------------------------------------------------------ generator */
 /* Seeded levelised timing DAG in the reference's text format conventions:
  * explicit virtual super-source (id n_pins) and super-sink (id n_pins+1) with

@@ -292,6 +292,22 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_profile_case(args):
+    """A short fixed sequence for ncu: one warm-up query, then one query
+    (suffix tree + engine) on the same workload at --k."""
+    import cpg_b200
+    import cases
+    c = cases.CASES[WORKLOAD]
+    dag = cpg_b200.generate(cpg_b200.gen_params(**c["gen"]))
+    with cpg_b200.CpGen() as g:
+        g.load_dag(dag)
+        for _ in range(2):
+            g.levelize()
+            g.report_paths(args.k)
+        g.sync()
+        print(json.dumps({"profile_case": WORKLOAD, "k": args.k, **g.stats()}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -301,8 +317,12 @@ def main():
     ap.add_argument("--k", type=int, default=1_000_000)
     ap.add_argument("--cpu-k", type=int, default=100_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-case", action="store_true",
+                    help="one warm-up and one measured query only (for ncu)")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.profile_case:
+        run_profile_case(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

@@ -214,6 +214,14 @@ Status upload_graph(cpg_handle* h, int32_t n, int32_t m, const int32_t* adjp,
   CK(cudaMemcpyAsync(hn, nsrc_dev, 4, cudaMemcpyDeviceToHost, s), "D2H sources");
   CK(cudaStreamSynchronize(s), "upload");
   h->n_srcs = *hn;
+  // sources in vertex-id order, as the reference's _srcs list (gpucpg.cu:
+  // 531-533): G-PathGen's root seeding keeps the first roots in that order
+  if (h->n_srcs > 1) {
+    std::vector<int32_t> srcs(h->n_srcs);
+    CK(cudaMemcpy(srcs.data(), h->d_srcs.p, srcs.size() * 4, cudaMemcpyDeviceToHost), "D2H sources");
+    std::sort(srcs.begin(), srcs.end());
+    CK(cudaMemcpy(h->d_srcs.p, srcs.data(), srcs.size() * 4, cudaMemcpyHostToDevice), "H2D sources");
+  }
   h->has_graph = true;
   h->sfxt_valid = false;
   h->h_sfxt_cached = false;

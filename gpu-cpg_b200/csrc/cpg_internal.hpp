@@ -221,7 +221,8 @@ struct EngineQuery {
   unsigned int pad0;
   unsigned long long krem;    // rank still wanted inside the prefix
   unsigned long long ksel;    // rank the select started from
-  unsigned long long paths_nz, pend_nz, pend_n;
+  unsigned long long paths_nz, pend_nz, pend_n;     // maintained incrementally
+  unsigned long long pend_next_n, pend_next_nz;      // the pile being written
   unsigned long long k_out, out_off, out_lt, out_eq;
   int phases;
   int pad;
@@ -230,6 +231,8 @@ struct EngineQuery {
 struct EngineCounters {
   int err;
   int active;
+  int sel_paths;              // some query selects over accepted paths
+  int pad0;
   unsigned long long paths;
   unsigned long long frontier[3];
   unsigned long long pend_out;

@@ -22,6 +22,7 @@
 // This file is compiled with --use_fast_math like the reference (see
 // pfxt_device.cuh for the child-cost expression).
 #include <climits>
+#include <cstddef>
 
 #include "pfxt_device.cuh"
 
@@ -70,6 +71,27 @@ __device__ __forceinline__ void agg_add_u32(unsigned int* base, bool on, unsigne
   if (on && (__ffs(m) - 1) == lane) atomicAdd(base + key, static_cast<unsigned>(__popc(m)));
 }
 
+// Warp-aggregated per-query add: lanes with `on` add v to the 64-bit field at
+// byte offset `off` of their query's EngineQuery; one atomic per distinct
+// query in the warp.  All lanes call.
+__device__ __forceinline__ void qadd(EngineQuery* qs, size_t off, bool on, unsigned q,
+                                     unsigned v) {
+  unsigned act = __ballot_sync(0xffffffffu, on && v != 0);
+  const int lane = threadIdx.x & 31;
+  while (act) {
+    const int leader = __ffs(act) - 1;
+    const unsigned ql = __shfl_sync(0xffffffffu, q, leader);
+    const bool mine = on && v != 0 && q == ql;
+    const unsigned m = __ballot_sync(0xffffffffu, mine);
+    const unsigned sum = __reduce_add_sync(0xffffffffu, mine ? v : 0u);
+    if (lane == leader)
+      atomicAdd(reinterpret_cast<unsigned long long*>(reinterpret_cast<char*>(qs + ql) + off),
+                static_cast<unsigned long long>(sum));
+    act &= ~m;
+  }
+}
+#define QOFF(field) offsetof(EngineQuery, field)
+
 // ------------------------------------------------------------------ seeding
 // One warp per query: reachable sources become root items; with the
 // reference rule, roots at or below the initial split beyond the first
@@ -110,7 +132,7 @@ __device__ void seed_query(const EngineParams& p, int qi) {
     const unsigned hb = __ballot_sync(0xffffffffu, hit);
     split = __shfl_sync(0xffffffffu, found, __ffs(hb) - 1);
   }
-  int short_seen = 0;
+  int short_seen = 0, kept_n = 0, kept_nz = 0;
   float rabs = 0.f;
   for (int base = b; base < e; base += 32) {
     const int i = base + lane;
@@ -128,6 +150,8 @@ __device__ void seed_query(const EngineParams& p, int qi) {
     const int before = short_seen + __popc(lb & lanemask_lt());
     const bool keep = reach && (!low || before < n_short);
     short_seen += __popc(lb);
+    kept_n += __popc(__ballot_sync(0xffffffffu, keep));
+    kept_nz += __popc(__ballot_sync(0xffffffffu, keep && c != 0.0f));
     if (keep) rabs = fmaxf(rabs, fabsf(c));
     const unsigned long long slot = warp_append(&p.ctr->pend_out, keep);
     if (keep) {
@@ -149,7 +173,10 @@ __device__ void seed_query(const EngineParams& p, int qi) {
     Q.done = 0;
     Q.mode = 0;
     Q.phases = 0;
-    Q.paths_nz = Q.pend_nz = Q.pend_n = 0;
+    Q.paths_nz = 0;
+    Q.pend_n = static_cast<unsigned long long>(kept_n);
+    Q.pend_nz = static_cast<unsigned long long>(kept_nz);
+    Q.pend_next_n = Q.pend_next_nz = 0;
     Q.out_lt = Q.out_eq = 0;
   }
 }
@@ -160,26 +187,35 @@ __device__ void seed_query(const EngineParams& p, int qi) {
 __device__ void select_hist(const EngineParams& p, unsigned long long n_paths,
                             const Item* pend, unsigned long long n_pend, int shift,
                             int bits) {
+  __shared__ unsigned int sh[kSelBins];
   const unsigned long long tid =
       static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   const unsigned long long nth = static_cast<unsigned long long>(gridDim.x) * blockDim.x;
   const int hi = shift + bits;
   const unsigned hmask = hi >= 32 ? 0u : ~((1u << hi) - 1u);
-  const unsigned long long tot = n_paths + n_pend;
+  // accepted paths take part only when some query selects over them
+  const unsigned long long np =
+      *reinterpret_cast<const volatile int*>(&p.ctr->sel_paths) ? n_paths : 0;
+  const unsigned long long tot = np + n_pend;
   const unsigned long long pad = (tot + 31) & ~31ull;
+  const bool single = p.nq == 1;
+  if (single) {
+    for (int i = threadIdx.x; i < kSelBins; i += blockDim.x) sh[i] = 0;
+    __syncthreads();
+  }
   for (unsigned long long i = tid; i < pad; i += nth) {
     bool on = false;
     unsigned key = 0, q = 0;
     if (i < tot) {
       float c;
       int mode;
-      if (i < n_paths) {
+      if (i < np) {
         q = static_cast<unsigned>(__ldcg(p.pq + i));
         c = __ldcg(p.ps.cost + i);
         mode = __ldcg(&p.q[q].mode);
         on = (mode == 2 || mode == 3) && c != 0.0f;
       } else {
-        const Item it = load_item(pend, i - n_paths);
+        const Item it = load_item(pend, i - np);
         q = q_of(it);
         c = it.cost;
         mode = __ldcg(&p.q[q].mode);
@@ -191,7 +227,16 @@ __device__ void select_hist(const EngineParams& p, unsigned long long n_paths,
       }
     }
     const unsigned bin = (key >> shift) & ((1u << bits) - 1u);
-    agg_add_u32(p.hist, on, q * kSelBins + bin);
+    if (single) {
+      if (on) atomicAdd(&sh[bin], 1u);
+    } else {
+      agg_add_u32(p.hist, on, q * kSelBins + bin);
+    }
+  }
+  if (single) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < (1 << bits); i += blockDim.x)
+      if (sh[i]) atomicAdd(&p.hist[i], sh[i]);
   }
 }
 
@@ -249,9 +294,11 @@ __device__ bool run_select(const EngineParams& p, unsigned long long n_paths,
 }
 
 // ------------------------------------------------------------------ closure
-__device__ __forceinline__ void route(const EngineParams& p, Item* out,
-                                      unsigned long long* out_cnt, Item* pend_out,
-                                      bool exists, const Item& it, float lim) {
+// Route one candidate (all lanes call): cost <= lim joins the next round's
+// frontier, the rest the next phase's pending pile.  Returns 1 if deferred.
+__device__ __forceinline__ int route(const EngineParams& p, Item* out,
+                                     unsigned long long* out_cnt, Item* pend_out,
+                                     bool exists, const Item& it, float lim) {
   const bool take = exists && it.cost <= lim;
   const bool defer = exists && !take;
   const unsigned long long a = warp_append(out_cnt, take);
@@ -264,6 +311,7 @@ __device__ __forceinline__ void route(const EngineParams& p, Item* out,
     if (b < p.pend_cap) pend_out[b] = it;
     else atomicCAS(&p.ctr->err, kDevOk, kDevCapacity);
   }
+  return defer ? 1 : 0;
 }
 
 // Rounds over the frontier until it is empty.  Returns false on error.
@@ -328,8 +376,10 @@ __device__ bool run_closure(const EngineParams& p, Item* pend_out) {
           atomicCAS(&p.ctr->err, kDevOk, kDevCapacity);
         }
       }
+      qadd(p.q, QOFF(paths_nz), stored && it.cost != 0.0f, q, 1u);
       // a path costing exactly the final split is reported, not expanded
       const bool expand = stored && !(it.cost == tie);
+      unsigned ndef = 0, ndef_nz = 0;
       const bool sib = expand && it.node >= 0;
       const float pcost = sib ? __ldcg(p.ps.cost + it.parent) : 0.f;
       {
@@ -342,20 +392,32 @@ __device__ bool run_closure(const EngineParams& p, Item* pend_out) {
         ex = sib && make_candidate(p.g, cn, cj, pcost, c.cost);
         c.node = cn;
         c.j = pack_j(q, cj);
-        route(p, out, out_cnt, pend_out, ex, c, lim);
+        if (route(p, out, out_cnt, pend_out, ex, c, lim)) {
+          ++ndef;
+          ndef_nz += c.cost != 0.0f;
+        }
         cn = jj == 0 ? hn.right : it.node;
         cj = jj == 0 ? 0 : 2 * jj + 2;
         ex = sib && make_candidate(p.g, cn, cj, pcost, c.cost);
         c.node = cn;
         c.j = pack_j(q, cj);
-        route(p, out, out_cnt, pend_out, ex, c, lim);
+        if (route(p, out, out_cnt, pend_out, ex, c, lim)) {
+          ++ndef;
+          ndef_nz += c.cost != 0.0f;
+        }
         ex = sib && jj == 0 && make_candidate(p.g, it.node, 1, pcost, c.cost);
         c.node = it.node;
         c.j = pack_j(q, 1);
-        route(p, out, out_cnt, pend_out, ex, c, lim);
+        if (route(p, out, out_cnt, pend_out, ex, c, lim)) {
+          ++ndef;
+          ndef_nz += c.cost != 0.0f;
+        }
         ex = sib && jj == 0 && make_candidate(p.g, it.node, 2, pcost, c.cost);
         c.j = pack_j(q, 2);
-        route(p, out, out_cnt, pend_out, ex, c, lim);
+        if (route(p, out, out_cnt, pend_out, ex, c, lim)) {
+          ++ndef;
+          ndef_nz += c.cost != 0.0f;
+        }
       }
       {
         Item c;
@@ -363,8 +425,13 @@ __device__ bool run_closure(const EngineParams& p, Item* pend_out) {
         c.node = expand ? __ldg(p.g.ht_root + to) : -1;
         c.j = pack_j(q, 0);
         const bool ex = expand && make_candidate(p.g, c.node, 0, it.cost, c.cost);
-        route(p, out, out_cnt, pend_out, ex, c, lim);
+        if (route(p, out, out_cnt, pend_out, ex, c, lim)) {
+          ++ndef;
+          ndef_nz += c.cost != 0.0f;
+        }
       }
+      qadd(p.q, QOFF(pend_next_n), valid, q, ndef);
+      qadd(p.q, QOFF(pend_next_nz), valid, q, ndef_nz);
     }
     if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit)) return false;
     ++r;
@@ -490,42 +557,7 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
   for (int phase = 0;; ++phase) {
     const Item* pend = p.pend[pin];
     Item* pend_next = p.pend[pin ^ 1];
-    // A. per-query counts
-    {
-      const unsigned long long tot = n_paths + n_pend;
-      const unsigned long long pad = (tot + 31) & ~31ull;
-      for (unsigned long long i = tid; i < pad; i += nth) {
-        bool path_nz = false, pend_any = false, pend_nz = false;
-        unsigned q = 0, key = 0xffffffffu;
-        if (i < n_paths) {
-          q = static_cast<unsigned>(__ldcg(p.pq + i));
-          path_nz = __ldcg(p.ps.cost + i) != 0.0f;
-        } else if (i < tot) {
-          const Item it = load_item(pend, i - n_paths);
-          q = q_of(it);
-          pend_any = true;
-          pend_nz = it.cost != 0.0f;
-          key = float_key(it.cost);
-        }
-        {
-          const unsigned m = __match_any_sync(0xffffffffu, path_nz ? q : 0xffffffffu);
-          if (path_nz && (__ffs(m) - 1) == static_cast<int>(threadIdx.x & 31))
-            atomicAdd(&p.q[q].paths_nz, static_cast<unsigned long long>(__popc(m)));
-        }
-        {
-          const unsigned m = __match_any_sync(0xffffffffu, pend_any ? q : 0xffffffffu);
-          const unsigned mz = __match_any_sync(0xffffffffu, pend_nz ? q : 0xffffffffu);
-          const int lane = threadIdx.x & 31;
-          if (pend_any && (__ffs(m) - 1) == lane)
-            atomicAdd(&p.q[q].pend_n, static_cast<unsigned long long>(__popc(m)));
-          if (pend_nz && (__ffs(mz) - 1) == lane)
-            atomicAdd(&p.q[q].pend_nz, static_cast<unsigned long long>(__popc(mz)));
-        }
-        (void)key;
-      }
-    }
-    if (blockIdx.x == 0 && threadIdx.x == 0) p.ctr->active = 0;
-    ENG_SYNC();
+    // (per-query counts are kept current by seeding, promotion and closure)
     // B. per-query decision
     for (unsigned long long qi = tid; qi < static_cast<unsigned long long>(p.nq); qi += nth) {
       EngineQuery& Q = p.q[qi];
@@ -539,15 +571,17 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
         Q.mode = 2;                       // final: the k-th of paths+pending
         Q.krem = static_cast<unsigned long long>(Q.k);
         Q.ksel = Q.krem;
+        atomicOr(&p.ctr->sel_paths, 1);
       } else if (Q.pend_n > 0) {
         Q.mode = 1;                       // grow by count
-        // promote ~4x the accepted count, but never more than half the
-        // pile: the top of the pile holds the expensive outliers whose
-        // closure can be exponentially large
+        // promote ~4x the accepted count, but never the top quarter of the
+        // pile: it holds the expensive outliers whose closure can be
+        // exponentially large
         unsigned long long j = 4 * (Q.paths_nz + 1);
         if (j < 64) j = 64;
-        const unsigned long long half = (Q.pend_n + 1) / 2;
-        if (j > half) j = half;
+        unsigned long long cap = (3 * Q.pend_n) / 4;
+        if (cap < 1) cap = 1;
+        if (j > cap) j = cap;
         Q.krem = j;
         Q.ksel = j;
       } else {
@@ -592,6 +626,7 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
         bool take = false, keep = false;
         Item it;
         it.cost = 0.f;
+        it.j = 0;
         if (i < n_pend) {
           it = load_item(pend, i);
           const EngineQuery& Q = p.q[q_of(it)];
@@ -610,6 +645,8 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
           if (b < p.pend_cap) pend_next[b] = it;
           else atomicCAS(&p.ctr->err, kDevOk, kDevCapacity);
         }
+        qadd(p.q, QOFF(pend_next_n), keep, q_of(it), 1u);
+        qadd(p.q, QOFF(pend_next_nz), keep && it.cost != 0.0f, q_of(it), 1u);
       }
     }
     ENG_SYNC();
@@ -619,9 +656,15 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
     for (unsigned long long qi = tid; qi < static_cast<unsigned long long>(p.nq); qi += nth) {
       EngineQuery& Q = p.q[qi];
       if (Q.mode == 2) Q.done = 1;
-      Q.paths_nz = Q.pend_nz = Q.pend_n = 0;
+      Q.pend_n = Q.pend_next_n;
+      Q.pend_nz = Q.pend_next_nz;
+      Q.pend_next_n = Q.pend_next_nz = 0;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) p.ctr->phases = phase + 1;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      p.ctr->phases = phase + 1;
+      p.ctr->active = 0;
+      p.ctr->sel_paths = 0;
+    }
     ENG_SYNC();
     n_paths = *reinterpret_cast<volatile unsigned long long*>(&p.ctr->paths);
     n_pend = *reinterpret_cast<volatile unsigned long long*>(&p.ctr->pend_out);
@@ -633,8 +676,7 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
     atomicCAS(&p.ctr->err, kDevOk, kDevCapacity);
     return;
   }
-  // H. the last phase's counts (step A of the pass that found every query
-  // done) are current: no path was accepted after them
+  // H. per-query counts are current (kept up to date by the closures)
   for (unsigned long long i = tid; i < n_paths; i += nth) p.rank_of[i] = -1;
   ENG_SYNC();
   for (unsigned long long qi = tid; qi < static_cast<unsigned long long>(p.nq); qi += nth) {
@@ -648,6 +690,7 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
   }
   ENG_SYNC();
   if (blockIdx.x == 0 && threadIdx.x == 0) {
+    p.ctr->sel_paths = 1;
     unsigned long long acc = 0;
     for (int qi = 0; qi < p.nq; ++qi) {
       p.q[qi].out_off = acc;

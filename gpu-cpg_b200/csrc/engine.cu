@@ -574,14 +574,15 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
         atomicOr(&p.ctr->sel_paths, 1);
       } else if (Q.pend_n > 0) {
         Q.mode = 1;                       // grow by count
-        // promote ~4x the accepted count, but never the top quarter of the
-        // pile: it holds the expensive outliers whose closure can be
-        // exponentially large
+        // promote ~4x the accepted count, but never more than half the
+        // pile: every path below the split is accepted with its whole
+        // closure, and the upper half of the pile reaches costs whose
+        // closure is exponentially large (measured: a 3/4 cap accepted 77x
+        // the paths needed)
         unsigned long long j = 4 * (Q.paths_nz + 1);
         if (j < 64) j = 64;
-        unsigned long long cap = (3 * Q.pend_n) / 4;
-        if (cap < 1) cap = 1;
-        if (j > cap) j = cap;
+        const unsigned long long half = (Q.pend_n + 1) / 2;
+        if (j > half) j = half;
         Q.krem = j;
         Q.ksel = j;
       } else {
@@ -688,9 +689,9 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
     Q.krem = Q.k_out;
     Q.out_lt = Q.out_eq = 0;
   }
+  if (blockIdx.x == 0 && threadIdx.x == 0) p.ctr->sel_paths = 1;
   ENG_SYNC();
   if (blockIdx.x == 0 && threadIdx.x == 0) {
-    p.ctr->sel_paths = 1;
     unsigned long long acc = 0;
     for (int qi = 0; qi < p.nq; ++qi) {
       p.q[qi].out_off = acc;

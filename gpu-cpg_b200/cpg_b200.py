@@ -116,6 +116,7 @@ def _load():
         "cpg_get_stats": (C.c_int, [H, P(Stats)]),
         "cpg_sync": (C.c_int, [H]),
         "cpg_select_topk": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, P(C.c_int64), C.c_void_p]),
+        "cpg_select_topk_noalloc": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, P(C.c_int64), C.c_void_p]),
         "cpg_gen_params_init": (None, [P(GenParams)]),
         "cpg_dag_generate": (C.c_int, [P(GenParams), P(C.c_void_p)]),
         "cpg_dag_sizes": (C.c_int, [C.c_void_p, P(C.c_int32), P(C.c_int32)]),

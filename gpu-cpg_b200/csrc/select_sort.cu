@@ -6,6 +6,8 @@
 // Replaces the reference's final comparator merge sort of the whole short
 // pile and its zero-cost filter (gpucpg/gpucpg.cu:21323-21360): only the k
 // survivors are sorted, and zero-cost paths are excluded before selection.
+#include <mutex>
+
 #include "device_common.cuh"
 
 namespace cpg {
@@ -441,3 +443,84 @@ int launch_topk_costs(const float* costs, unsigned long long n, unsigned long lo
 }
 
 }  // namespace cpg
+
+// ---------------------------------------------------------------- no-alloc
+// cpg_select_topk_noalloc: the same top-K as cpg_select_topk, for callers
+// that must not allocate device memory.  Its scratch is this file-scope
+// array, reserved when the library is loaded (4.3 MiB on every GPU that
+// loads it, held until the process exits).  In host code the name
+// g_topk_scratch is only a host-side stand-in: the kernels get the device
+// address that cudaGetSymbolAddress returns, looked up once per device with
+// that device current.
+namespace cpg {
+namespace {
+
+constexpr unsigned long long kNoAllocMaxK = CPG_SELECT_TOPK_NOALLOC_MAX_K;
+// hist 2048 + state 4 + counts 4 + cnt 4 + tkey 4, keys/vals 2*K each,
+// sort histogram 256 * ceil(K / 2048)
+constexpr size_t kNoAllocWords =
+    2048 + 16 + 4 * kNoAllocMaxK + 256 * ((kNoAllocMaxK + kSortTile - 1) / kSortTile);
+
+__device__ __align__(256) unsigned int g_topk_scratch[kNoAllocWords];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[kMaxDevices] = {};
+
+}  // namespace
+}  // namespace cpg
+
+extern "C" cpg_status cpg_select_topk_noalloc(const float* d_costs, int64_t n,
+                                              int64_t k, float* d_out,
+                                              int64_t* n_out, void* stream) {
+  using namespace cpg;
+  if (n < 0 || k < 0 || !n_out || (n > 0 && !d_costs) || (k > 0 && !d_out))
+    return CPG_ERR_INVALID;
+  *n_out = 0;
+  if (n > (int64_t{1} << 32) - 1) return CPG_ERR_INVALID;
+  if (static_cast<unsigned long long>(k) > kNoAllocMaxK) return CPG_ERR_CAPACITY;
+  if (n == 0 || k == 0) return CPG_OK;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    cudaGetLastError();
+    return CPG_ERR_CUDA;
+  }
+  void* base = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+      // one-time set-up on this device (the current one): the device address
+      // of the static scratch; do the first call before any stream capture
+      void* ptr = nullptr;
+      if (cudaGetSymbolAddress(&ptr, g_topk_scratch) != cudaSuccess || !ptr) {
+        cudaGetLastError();
+        return CPG_ERR_CUDA;
+      }
+      g_noalloc_ptr[dev] = ptr;
+    }
+    base = g_noalloc_ptr[dev];
+  }
+  const unsigned long long kk = static_cast<unsigned long long>(k < n ? k : n);
+  unsigned int* w = static_cast<unsigned int*>(base);
+  TopkScratch sc;
+  sc.hist = w;
+  sc.state = w + 2048;
+  sc.counts = reinterpret_cast<unsigned long long*>(w + 2048 + 4);
+  sc.cnt = reinterpret_cast<unsigned long long*>(w + 2048 + 8);
+  sc.tkey = w + 2048 + 12;
+  sc.keys = w + 2048 + 16;
+  sc.vals = sc.keys + 2 * kNoAllocMaxK;
+  sc.sort_hist = sc.vals + 2 * kNoAllocMaxK;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // the array keeps the previous call's contents: the select histogram must
+  // start at zero
+  cudaError_t e = cudaMemsetAsync(sc.hist, 0, 2048 * sizeof(unsigned int), s);
+  unsigned long long got = 0;
+  if (e == cudaSuccess)
+    e = static_cast<cudaError_t>(
+        launch_topk_costs(d_costs, static_cast<unsigned long long>(n), kk, sc, d_out, &got, s));
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return CPG_ERR_CUDA;
+  *n_out = static_cast<int64_t>(got);
+  return CPG_OK;
+}

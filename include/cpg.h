@@ -191,6 +191,32 @@ cpg_status cpg_sync(cpg_handle* h);
 cpg_status cpg_select_topk(const float* d_costs, int64_t n, int64_t k,
                            float* d_out, int64_t* n_out, void* stream);
 
+/* Largest k cpg_select_topk_noalloc accepts. */
+#define CPG_SELECT_TOPK_NOALLOC_MAX_K 262144
+
+/* cpg_select_topk for callers that cannot allocate device memory: the same
+ * k smallest non-zero costs, ascending, but its scratch is a fixed array
+ * inside the library instead of cudaMalloc/cudaFree.  Meant for code that
+ * runs where an allocation is not allowed or not affordable: between the
+ * kernels of a pipeline whose other streams must keep running (cudaFree
+ * synchronises the whole device), under a memory pool or budget that owns
+ * every device byte, or in a process that has reserved all device memory up
+ * front.  No counterpart in the reference, which allocates thrust vectors in
+ * every report_paths call.
+ *
+ * Limits and rules:
+ *  - k <= CPG_SELECT_TOPK_NOALLOC_MAX_K, else CPG_ERR_CAPACITY (nothing runs);
+ *    n < 2^32.
+ *  - The scratch (about 4.3 MiB) is reserved on every GPU that loads the
+ *    library and kept until the process exits.
+ *  - The first call on a device looks up the scratch's device address (with
+ *    that device current); make it before any stream capture.
+ *  - All calls share the one array: calls that overlap on the GPU (from two
+ *    streams or threads at once) race and must be serialised by the caller.
+ *  - Calls no cudaMalloc/cudaFree; returns after the result is written. */
+cpg_status cpg_select_topk_noalloc(const float* d_costs, int64_t n, int64_t k,
+                                   float* d_out, int64_t* n_out, void* stream);
+
 /* ------------------------------------------------------------ generator */
 /* Seeded levelised timing DAG in the reference's text format conventions:
  * explicit virtual super-source (id n_pins) and super-sink (id n_pins+1) with

@@ -132,7 +132,7 @@ struct SfxtParams {
   unsigned int spin_limit;
 };
 
-constexpr int kSfxtThreads = 256;
+constexpr int kSfxtThreads = 1024;  // one block per SM: fewer grid-barrier arrivals
 constexpr int kSmemRow = 256;  // deviation rows up to this length sort in smem
 
 // Launch the persistent SFXT kernel (cooperative) and the row sorts that

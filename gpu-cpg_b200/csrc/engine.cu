@@ -30,7 +30,7 @@ namespace cpg {
 
 namespace {
 
-constexpr int kEngThreads = 256;
+constexpr int kEngThreads = 1024;  // one block per SM: fewer grid-barrier arrivals
 constexpr int kEngWarps = kEngThreads / 32;
 
 #define ENG_SYNC()                                                   \
@@ -461,12 +461,12 @@ __device__ bool lsd_pass(const EngineParams& p, unsigned long long n, int src,
     return ((on_q ? __ldcg(qin + i) : __ldcg(kin + i)) >> shift) & 255u;
   };
   // 1. tile histogram
-  running[threadIdx.x] = 0;
+  for (int d = threadIdx.x; d < 256; d += blockDim.x) running[d] = 0;
   __syncthreads();
   for (unsigned long long i = t0 + threadIdx.x; i < t1; i += blockDim.x)
     atomicAdd(&running[digit_of(i)], 1u);
   __syncthreads();
-  p.sort_hist[threadIdx.x * G + blockIdx.x] = running[threadIdx.x];
+  for (int d = threadIdx.x; d < 256; d += blockDim.x) p.sort_hist[d * G + blockIdx.x] = running[d];
   if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit)) return false;
   // 2. one warp per digit: exclusive scan across tiles
   {
@@ -498,8 +498,9 @@ __device__ bool lsd_pass(const EngineParams& p, unsigned long long n, int src,
     }
   }
   __syncthreads();
-  running[threadIdx.x] = dbase[threadIdx.x] + __ldcg(p.sort_hist + threadIdx.x * G + blockIdx.x);
-  for (int w = 0; w < kEngWarps; ++w) wcount[w][threadIdx.x] = 0;
+  for (int d = threadIdx.x; d < 256; d += blockDim.x)
+    running[d] = dbase[d] + __ldcg(p.sort_hist + d * G + blockIdx.x);
+  for (int x = threadIdx.x; x < kEngWarps * 256; x += blockDim.x) wcount[x >> 8][x & 255] = 0;
   __syncthreads();
   unsigned int* kout = p.keys[src ^ 1];
   unsigned int* qout = p.qids[src ^ 1];
@@ -526,13 +527,13 @@ __device__ bool lsd_pass(const EngineParams& p, unsigned long long n, int src,
       vout[pos] = vv;
     }
     __syncthreads();
-    {
+    for (int d = threadIdx.x; d < 256; d += blockDim.x) {
       unsigned s = 0;
       for (int w = 0; w < kEngWarps; ++w) {
-        s += wcount[w][threadIdx.x];
-        wcount[w][threadIdx.x] = 0;
+        s += wcount[w][d];
+        wcount[w][d] = 0;
       }
-      running[threadIdx.x] += s;
+      running[d] += s;
     }
     __syncthreads();
   }

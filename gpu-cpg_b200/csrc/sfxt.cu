@@ -119,62 +119,10 @@ __device__ void build_vertex(const SfxtParams& p, int v, int lvl, bool do_kahn) 
     p.dist[v] = best;
     p.succ[v] = s;
     p.dev_cnt[v] = cnt;
-    const int base_root = s >= 0 ? __ldcg(p.ht_root + s) : -1;
-    const int base_size = s >= 0 ? __ldcg(p.ht_size + s) : 0;
-    if (cnt == 0) {
-      p.ht_root[v] = base_root;
-      p.ht_size[v] = base_size;
-    } else {
-      // persistent insert at position base_size+1 of a complete binary heap:
-      // copy the root-to-position path, carrying the larger element down
-      const unsigned pos = static_cast<unsigned>(base_size) + 1u;
-      const int depth = 31 - __clz(pos);
-      const unsigned long long a =
-          atomicAdd(&p.ctr->hnode_used, static_cast<unsigned long long>(depth + 1));
-      if (a + depth + 1 > p.hnode_cap) {
-        atomicCAS(&p.ctr->err, kDevOk, kDevCapacity);
-        p.ht_root[v] = -1;
-        p.ht_size[v] = 0;
-      } else {
-        int cv = v;
-        float ck = kmin;
-        int cur = base_root;
-        for (int d = depth - 1; d >= 0; --d) {
-          HeapNode old;
-          {
-            const int4 raw = __ldcg(reinterpret_cast<const int4*>(p.hnodes + cur));
-            old.vtx = raw.x;
-            old.left = raw.y;
-            old.right = raw.z;
-            old.key = __int_as_float(raw.w);
-          }
-          const int bit = (pos >> d) & 1u;
-          HeapNode nn;
-          if (heap_less(cv, ck, old.vtx, old.key)) {
-            nn.vtx = cv;
-            nn.key = ck;
-            cv = old.vtx;
-            ck = old.key;
-          } else {
-            nn.vtx = old.vtx;
-            nn.key = old.key;
-          }
-          const int next = static_cast<int>(a) + (depth - d);
-          nn.left = bit ? old.left : next;
-          nn.right = bit ? next : old.right;
-          p.hnodes[a + (depth - 1 - d)] = nn;
-          cur = bit ? old.right : old.left;
-        }
-        HeapNode leaf;
-        leaf.vtx = cv;
-        leaf.key = ck;
-        leaf.left = -1;
-        leaf.right = -1;
-        p.hnodes[a + depth] = leaf;
-        p.ht_root[v] = static_cast<int>(a);
-        p.ht_size[v] = static_cast<int>(pos);
-      }
-    }
+    // v's fan-outs are all processed, so its dependency counter is free: it
+    // carries the cheapest deviation key to the chain-heap insert, which runs
+    // one level later, off this level's critical path
+    p.deps[v] = __float_as_int(kmin);
   }
 
   if (do_kahn) {
@@ -197,6 +145,70 @@ __device__ void build_vertex(const SfxtParams& p, int v, int lvl, bool do_kahn) 
       }
     }
   }
+}
+
+// Chain heap of v: the heap of succ[v] with v's cheapest deviation inserted
+// at position size+1 of a complete binary heap, copying the root-to-position
+// path and carrying the larger element down.  One thread per vertex; runs one
+// level after v was relaxed, when succ[v]'s heap is complete.
+__device__ void heap_insert(const SfxtParams& p, int v) {
+  const int s = __ldcg(p.succ + v);
+  const int cnt = __ldcg(p.dev_cnt + v);
+  const int base_root = s >= 0 ? __ldcg(p.ht_root + s) : -1;
+  const int base_size = s >= 0 ? __ldcg(p.ht_size + s) : 0;
+  if (cnt == 0) {
+    p.ht_root[v] = base_root;
+    p.ht_size[v] = base_size;
+    return;
+  }
+  const float kmin = __int_as_float(__ldcg(p.deps + v));
+  const unsigned pos = static_cast<unsigned>(base_size) + 1u;
+  const int depth = 31 - __clz(pos);
+  const unsigned long long a =
+      atomicAdd(&p.ctr->hnode_used, static_cast<unsigned long long>(depth + 1));
+  if (a + depth + 1 > p.hnode_cap) {
+    atomicCAS(&p.ctr->err, kDevOk, kDevCapacity);
+    p.ht_root[v] = -1;
+    p.ht_size[v] = 0;
+    return;
+  }
+  int cv = v;
+  float ck = kmin;
+  int cur = base_root;
+  for (int d = depth - 1; d >= 0; --d) {
+    HeapNode old;
+    {
+      const int4 raw = __ldcg(reinterpret_cast<const int4*>(p.hnodes + cur));
+      old.vtx = raw.x;
+      old.left = raw.y;
+      old.right = raw.z;
+      old.key = __int_as_float(raw.w);
+    }
+    const int bit = (pos >> d) & 1u;
+    HeapNode nn;
+    if (heap_less(cv, ck, old.vtx, old.key)) {
+      nn.vtx = cv;
+      nn.key = ck;
+      cv = old.vtx;
+      ck = old.key;
+    } else {
+      nn.vtx = old.vtx;
+      nn.key = old.key;
+    }
+    const int next = static_cast<int>(a) + (depth - d);
+    nn.left = bit ? old.left : next;
+    nn.right = bit ? next : old.right;
+    p.hnodes[a + (depth - 1 - d)] = nn;
+    cur = bit ? old.right : old.left;
+  }
+  HeapNode leaf;
+  leaf.vtx = cv;
+  leaf.key = ck;
+  leaf.left = -1;
+  leaf.right = -1;
+  p.hnodes[a + depth] = leaf;
+  p.ht_root[v] = static_cast<int>(a);
+  p.ht_size[v] = static_cast<int>(pos);
 }
 
 __global__ void __launch_bounds__(kSfxtThreads)
@@ -241,21 +253,32 @@ sfxt_persistent_kernel(SfxtParams p) {
     end = p.lvlp[lvl + 1];
   }
 
+  const int first = lvl;   // first level rebuilt by this launch
+  int pbeg = beg;          // previous level's range, whose heaps are pending
+  int pend = beg;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nth = gridDim.x * blockDim.x;
   while (beg < end) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       p.lvlp[lvl] = beg;
       p.lvlp[lvl + 1] = end;
-      p.pool_mark[lvl] = *reinterpret_cast<volatile unsigned long long*>(&p.ctr->hnode_used);
+      // heap nodes in use before the previous level's inserts (which start
+      // in this pass)
+      if (lvl > first)
+        p.pool_mark[lvl - 1] = *reinterpret_cast<volatile unsigned long long*>(&p.ctr->hnode_used);
     }
     for (int i = beg + gwarp; i < end; i += nwarps) {
       build_vertex(p, __ldcg(p.order + i), lvl, full);
     }
+    for (int i = pbeg + tid; i < pend; i += nth) heap_insert(p, __ldcg(p.order + i));
     // the tail keeps growing as soon as the next level starts appending, so
     // the level bound is the snapshot the last arriving block took
     if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit, &p.ctr->tail,
                    &p.ctr->level_end))
       return;
     ++lvl;
+    pbeg = beg;
+    pend = end;
     beg = end;
     if (full) {
       end = *reinterpret_cast<volatile int*>(&p.ctr->level_end);
@@ -263,6 +286,10 @@ sfxt_persistent_kernel(SfxtParams p) {
       end = lvl < p.known_levels ? p.lvlp[lvl + 1] : beg;
     }
   }
+  // heaps of the last level
+  if (blockIdx.x == 0 && threadIdx.x == 0 && lvl > first)
+    p.pool_mark[lvl - 1] = *reinterpret_cast<volatile unsigned long long*>(&p.ctr->hnode_used);
+  for (int i = pbeg + tid; i < pend; i += nth) heap_insert(p, __ldcg(p.order + i));
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     p.ctr->levels = lvl;
     p.lvlp[lvl] = beg;

@@ -68,6 +68,7 @@ class Stats(C.Structure):
         ("phases", C.c_int32), ("rounds", C.c_int32), ("levels", C.c_int32),
         ("kernel_launches", C.c_int32), ("split", C.c_float),
         ("frontier_used", C.c_int32), ("retries", C.c_int32),
+        ("engine_stage_ms", C.c_float * 8),
     ]
 
 
@@ -331,7 +332,9 @@ class CpGen:
     def stats(self) -> dict:
         s = Stats()
         self._check(lib.cpg_get_stats(self._h, C.byref(s)), "stats")
-        return {f: getattr(s, f) for f, _ in Stats._fields_}
+        d = {f: getattr(s, f) for f, _ in Stats._fields_}
+        d["engine_stage_ms"] = [round(float(x), 4) for x in s.engine_stage_ms]
+        return d
 
     def sync(self):
         self._check(lib.cpg_sync(self._h), "sync")

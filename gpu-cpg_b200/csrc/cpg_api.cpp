@@ -28,6 +28,7 @@ struct DevMem {
 };
 
 constexpr unsigned int kDefaultSpinLimit = 1u << 24;
+enum { kRetry = 1000 };  // internal: a bounded buffer overflowed, grow and rerun
 constexpr int32_t kMaxRow = 16384;  // longest deviation row the row sort takes
 
 }  // namespace
@@ -238,74 +239,95 @@ Status load_edgelist(cpg_handle* h, const EdgeList& el) {
   return upload_graph(h, g.n, g.m, g.adjp.data(), g.adj.data(), g.w.data());
 }
 
+SfxtParams sfxt_params(cpg_handle* h, int32_t start_level) {
+  SfxtParams p{};
+  p.n = h->g.n;
+  p.adjp = P<int32_t>(h->d_adjp);
+  p.edges = P<DevEdge>(h->d_edges);
+  p.iadjp = P<int32_t>(h->d_iadjp);
+  p.iadj = P<int32_t>(h->d_iadj);
+  p.order = P<int32_t>(h->d_order);
+  p.lvlp = P<int32_t>(h->d_lvlp);
+  p.level_of = P<int32_t>(h->d_level_of);
+  p.dist = P<int32_t>(h->d_dist);
+  p.succ = P<int32_t>(h->d_succ);
+  p.dev_cnt = P<int32_t>(h->d_dev_cnt);
+  p.dev = P<DevSidetrack>(h->d_dev);
+  p.ht_root = P<int32_t>(h->d_ht_root);
+  p.ht_size = P<int32_t>(h->d_ht_size);
+  p.hnodes = P<HeapNode>(h->d_hnodes);
+  p.hnode_cap = h->hnode_cap;
+  p.pool_mark = P<unsigned long long>(h->d_pool_mark);
+  p.deps = P<int32_t>(h->d_deps);
+  p.big_off = P<int32_t>(h->d_big_off);
+  p.big_tmp = P<DevSidetrack>(h->d_big_tmp);
+  p.big_rows = P<int32_t>(h->d_big_rows);
+  p.n_big_rows = h->big_rows;
+  p.big_row_cap = h->big_cap;
+  p.ctr = P<SfxtCounters>(h->d_sctr);
+  p.start_level = start_level;
+  p.known_levels = h->levels;
+  p.spin_limit = h->opts.spin_limit ? h->opts.spin_limit : kDefaultSpinLimit;
+  return p;
+}
+
+// Device work of one suffix-tree build, asynchronous and capturable.
+Status enqueue_sfxt(cpg_handle* h, int32_t start_level, int* launches) {
+  cudaStream_t s = h->stream;
+  CK(launch_init_sfxt_counters(P<SfxtCounters>(h->d_sctr), P<unsigned long long>(h->d_pool_mark),
+                               start_level, s), "sfxt counters");
+  int grid = 0;
+  CK(launch_sfxt(sfxt_params(h, start_level), h->device, s, &grid, launches), "sfxt launch");
+  *launches += 1;
+  return CPG_OK;
+}
+
+// Reads the build's counters back; kRetry when the heap pool overflowed.
+int finish_sfxt(cpg_handle* h, int32_t start_level) {
+  SfxtCounters* out = static_cast<SfxtCounters*>(h->pinned);
+  CK(cudaMemcpyAsync(out, h->d_sctr.p, sizeof(SfxtCounters), cudaMemcpyDeviceToHost, h->stream),
+     "D2H sfxt counters");
+  CK(cudaStreamSynchronize(h->stream), "sfxt");
+  if (out->err == kDevTimeout)
+    return fail(h, CPG_ERR_TIMEOUT, "suffix tree: grid barrier wait ran out");
+  if (out->err == kDevCapacity) return kRetry;
+  if (start_level == 0) h->levels = out->levels;
+  h->stats.levels = h->levels;
+  h->stats.frontier_used = CPG_FRONTIER_CSR;
+  h->sfxt_valid = true;
+  h->h_sfxt_cached = false;
+  h->dirty_level = -1;
+  return CPG_OK;
+}
+
+Status grow_heap_pool(cpg_handle* h) {
+  release(h->d_hnodes);
+  h->hnode_cap *= 2;
+  CK(ensure(h->d_hnodes, h->hnode_cap * sizeof(HeapNode)), "alloc chain heaps");
+  return CPG_OK;
+}
+
 Status run_sfxt(cpg_handle* h, int32_t start_level) {
-  const int n = h->g.n;
   cudaStream_t s = h->stream;
   for (int attempt = 0; attempt < 8; ++attempt) {
-    SfxtCounters c{};
-    if (start_level > 0) {
-      unsigned long long mark = 0;
-      CK(cudaMemcpy(&mark, P<unsigned long long>(h->d_pool_mark) + start_level, 8,
-                    cudaMemcpyDeviceToHost), "read pool mark");
-      c.hnode_used = mark;
-    }
-    CK(cudaMemcpyAsync(h->d_sctr.p, &c, sizeof(c), cudaMemcpyHostToDevice, s), "H2D sfxt counters");
-    SfxtParams p{};
-    p.n = n;
-    p.adjp = P<int32_t>(h->d_adjp);
-    p.edges = P<DevEdge>(h->d_edges);
-    p.iadjp = P<int32_t>(h->d_iadjp);
-    p.iadj = P<int32_t>(h->d_iadj);
-    p.order = P<int32_t>(h->d_order);
-    p.lvlp = P<int32_t>(h->d_lvlp);
-    p.level_of = P<int32_t>(h->d_level_of);
-    p.dist = P<int32_t>(h->d_dist);
-    p.succ = P<int32_t>(h->d_succ);
-    p.dev_cnt = P<int32_t>(h->d_dev_cnt);
-    p.dev = P<DevSidetrack>(h->d_dev);
-    p.ht_root = P<int32_t>(h->d_ht_root);
-    p.ht_size = P<int32_t>(h->d_ht_size);
-    p.hnodes = P<HeapNode>(h->d_hnodes);
-    p.hnode_cap = h->hnode_cap;
-    p.pool_mark = P<unsigned long long>(h->d_pool_mark);
-    p.deps = P<int32_t>(h->d_deps);
-    p.big_off = P<int32_t>(h->d_big_off);
-    p.big_tmp = P<DevSidetrack>(h->d_big_tmp);
-    p.big_rows = P<int32_t>(h->d_big_rows);
-    p.n_big_rows = h->big_rows;
-    p.big_row_cap = h->big_cap;
-    p.ctr = P<SfxtCounters>(h->d_sctr);
-    p.start_level = start_level;
-    p.known_levels = h->levels;
-    p.spin_limit = h->opts.spin_limit ? h->opts.spin_limit : kDefaultSpinLimit;
     CK(cudaEventRecord(h->ev[0], s), "event");
-    int grid = 0, launches = 0;
-    CK(launch_sfxt(p, h->device, s, &grid, &launches), "sfxt launch");
+    int launches = 0;
+    Status st = enqueue_sfxt(h, start_level, &launches);
+    if (st != CPG_OK) return st;
     CK(cudaEventRecord(h->ev[1], s), "event");
     h->stats.kernel_launches += launches;
-    SfxtCounters* out = static_cast<SfxtCounters*>(h->pinned);
-    CK(cudaMemcpyAsync(out, h->d_sctr.p, sizeof(SfxtCounters), cudaMemcpyDeviceToHost, s), "D2H sfxt counters");
-    CK(cudaStreamSynchronize(s), "sfxt");
+    const int r = finish_sfxt(h, start_level);
     float ms = 0.f;
     cudaEventElapsedTime(&ms, h->ev[0], h->ev[1]);
     h->stats.sfxt_ms = ms;
-    if (out->err == kDevTimeout)
-      return fail(h, CPG_ERR_TIMEOUT, "suffix tree: grid barrier wait ran out");
-    if (out->err == kDevCapacity) {
+    if (r == kRetry) {
       // chain heaps outgrew their pool: grow and rebuild from scratch
-      release(h->d_hnodes);
-      h->hnode_cap *= 2;
-      CK(ensure(h->d_hnodes, h->hnode_cap * sizeof(HeapNode)), "alloc chain heaps");
+      st = grow_heap_pool(h);
+      if (st != CPG_OK) return st;
       start_level = 0;
       continue;
     }
-    if (start_level == 0) h->levels = out->levels;
-    h->stats.levels = h->levels;
-    h->stats.frontier_used = CPG_FRONTIER_CSR;
-    h->sfxt_valid = true;
-    h->h_sfxt_cached = false;
-    h->dirty_level = -1;
-    return CPG_OK;
+    return static_cast<Status>(r);
   }
   return fail(h, CPG_ERR_CAPACITY, "suffix tree: chain heap pool cannot grow");
 }
@@ -374,7 +396,6 @@ float margin_of(float t, float root_abs) {
   return a * 0x1p-16f;
 }
 
-enum { kRetry = 1000 };
 
 Status alloc_query(cpg_handle* h, unsigned long long k) {
   const size_t cp = h->cap_paths, cf = h->cap_front, cpd = h->cap_pend;
@@ -687,6 +708,7 @@ int engine_query(cpg_handle* h, unsigned long long k) {
   h->stats.phases = c.phases;
   h->stats.rounds = c.rounds;
   h->stats.split = qo.t;
+  for (int i = 0; i < 8; ++i) h->stats.engine_stage_ms[i] = static_cast<float>(c.t_ns[i] * 1e-6);
   h->n_paths = c.paths;
   h->n_result = static_cast<int64_t>(qo.k_out);
   h->sorted_vals_off = c.sorted_buf ? k : 0;

@@ -135,6 +135,10 @@ struct SfxtParams {
 constexpr int kSfxtThreads = 1024;  // one block per SM: fewer grid-barrier arrivals
 constexpr int kSmemRow = 256;  // deviation rows up to this length sort in smem
 
+// Zero a build's counters on the device (capturable: no host copy).
+int launch_init_sfxt_counters(SfxtCounters* c, const unsigned long long* pool_mark,
+                              int start_level, void* stream);
+
 // Launch the persistent SFXT kernel (cooperative) and the row sorts that
 // follow it.  Returns a cudaError_t; *launches counts the kernels.
 int launch_sfxt(const SfxtParams& p, int device, void* stream, int* grid_out,
@@ -241,6 +245,9 @@ struct EngineCounters {
   int phases;
   int sorted_buf;             // which vals[] holds the sorted path indices
   int pad;
+  // device time per stage (ns): 0 seed, 1 decide/bookkeeping, 2 select,
+  // 3 promote, 4 closure, 5 output select, 6 output sort, 7 emit
+  unsigned long long t_ns[8];
   GridBarrier bar;
 };
 

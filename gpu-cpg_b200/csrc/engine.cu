@@ -33,6 +33,23 @@ namespace {
 constexpr int kEngThreads = 1024;  // one block per SM: fewer grid-barrier arrivals
 constexpr int kEngWarps = kEngThreads / 32;
 
+// Stage clock: block 0's thread 0 adds the globaltimer time since the last
+// stamp to ctr->t_ns[stage] (stage = where the time went).
+#define STAMP(stage)                                                   \
+  do {                                                                 \
+    if (blockIdx.x == 0 && threadIdx.x == 0) {                         \
+      const unsigned long long now_ = gtime();                          \
+      p.ctr->t_ns[stage] += now_ - t_last;                             \
+      t_last = now_;                                                   \
+    }                                                                  \
+  } while (0)
+
+__device__ __forceinline__ unsigned long long gtime() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
 #define ENG_SYNC()                                                   \
   do {                                                               \
     if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit)) return;  \
@@ -548,9 +565,12 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
   const int gw = static_cast<int>(tid >> 5);
   const int nw = static_cast<int>(nth >> 5);
 
+  unsigned long long t_last = 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) t_last = gtime();
   // seed roots (pending pile 0)
   for (int qi = gw; qi < p.nq; qi += nw) seed_query(p, qi);
   ENG_SYNC();
+  STAMP(0);
   int pin = 0;
   unsigned long long n_pend = *reinterpret_cast<volatile unsigned long long*>(&p.ctr->pend_out);
   unsigned long long n_paths = 0;
@@ -594,9 +614,11 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
       atomicAdd(&p.ctr->active, 1);
     }
     ENG_SYNC();
+    STAMP(1);
     if (*reinterpret_cast<volatile int*>(&p.ctr->active) == 0) break;
     // C. per-query radix select
     if (!run_select(p, n_paths, pend, n_pend)) return;
+    STAMP(2);
     // D. split and acceptance limit
     for (unsigned long long qi = tid; qi < static_cast<unsigned long long>(p.nq); qi += nth) {
       EngineQuery& Q = p.q[qi];
@@ -621,6 +643,7 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
       p.ctr->pend_out = 0;
     }
     ENG_SYNC();
+    STAMP(1);
     // E. promote pending items under their query's limit
     {
       const unsigned long long pad = (n_pend + 31) & ~31ull;
@@ -652,8 +675,10 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
       }
     }
     ENG_SYNC();
+    STAMP(3);
     // F. closure
     if (!run_closure(p, pend_next)) return;
+    STAMP(4);
     // G. final-mode queries are answered; counts restart
     for (unsigned long long qi = tid; qi < static_cast<unsigned long long>(p.nq); qi += nth) {
       EngineQuery& Q = p.q[qi];
@@ -668,6 +693,7 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
       p.ctr->sel_paths = 0;
     }
     ENG_SYNC();
+    STAMP(1);
     n_paths = *reinterpret_cast<volatile unsigned long long*>(&p.ctr->paths);
     n_pend = *reinterpret_cast<volatile unsigned long long*>(&p.ctr->pend_out);
     pin ^= 1;
@@ -701,6 +727,7 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
     p.ctr->out_total = acc;
   }
   if (!run_select(p, n_paths, nullptr, 0)) return;
+  STAMP(5);
   const unsigned long long n_out = *reinterpret_cast<volatile unsigned long long*>(&p.ctr->out_total);
   if (n_out > p.out_cap) {
     atomicCAS(&p.ctr->err, kDevOk, kDevCapacity);
@@ -755,6 +782,7 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
     }
   }
   ENG_SYNC();
+  STAMP(5);
   // K. stable LSD sort over (query, cost)
   int src = 0;
   for (int pass = 0; pass < 4; ++pass) {
@@ -765,6 +793,7 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
     if (!lsd_pass(p, n_out, src, shift, true)) return;
     src ^= 1;
   }
+  STAMP(6);
   // L. ranks within each query's list, then M. emission
   for (unsigned long long i = tid; i < n_out; i += nth) {
     const unsigned q = __ldcg(p.qids[src] + i);
@@ -788,6 +817,7 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
       p.out_nodes[i] = nd;
     }
   }
+  STAMP(7);
   // the sorted path indices stay in vals[src]; the host learns which buffer
   if (blockIdx.x == 0 && threadIdx.x == 0) p.ctr->sorted_buf = src;
 }

@@ -43,75 +43,102 @@ __device__ __forceinline__ int fixed_delay(float w) {
 // One warp builds vertex v at level lvl: fixed-point distance, successor,
 // its deviation list (unsorted here; sort_rows_kernel orders it), its chain
 // heap, and the Kahn step for its fan-in neighbours.
+constexpr int kRegChunks = kSmemRow / 32;  // rows up to this many 32-edge chunks
+                                          // stay in registers
+
+__device__ __forceinline__ int cand_dist(int dh, float w) {
+  return static_cast<int>(static_cast<unsigned>(dh) + static_cast<unsigned>(fixed_delay(w)));
+}
+
 __device__ void build_vertex(const SfxtParams& p, int v, int lvl, bool do_kahn) {
   const int lane = threadIdx.x & 31;
   const int rb = p.adjp[v];
   const int re = p.adjp[v + 1];
   int best = INT_MAX;
   int s = -1;
-  // the first 32 edges stay in registers; longer rows reload (L1/L2 hits)
-  DevEdge e0;
-  e0.head = -1;
-  e0.w = 0.f;
-  int dh0 = INT_MAX;
-  if (rb + lane < re) {
-    e0 = p.edges[rb + lane];
-    dh0 = __ldcg(p.dist + e0.head);
-  }
-  if (lvl == 0) {
-    best = 0;  // sinks (out-degree 0) start at distance 0 (gpucpg.cu:17034-17038)
-  } else {
-    if (rb + lane < re)
-      best = static_cast<int>(static_cast<unsigned>(dh0) + static_cast<unsigned>(fixed_delay(e0.w)));
-    for (int e = rb + 32 + lane; e < re; e += 32) {
-      const DevEdge ed = p.edges[e];
-      const int c = static_cast<int>(static_cast<unsigned>(__ldcg(p.dist + ed.head)) +
-                                     static_cast<unsigned>(fixed_delay(ed.w)));
-      best = min(best, c);
-    }
-    best = warp_min_i(best);
-    if (rb + lane < re &&
-        static_cast<int>(static_cast<unsigned>(dh0) + static_cast<unsigned>(fixed_delay(e0.w))) == best)
-      s = e0.head;
-    for (int e = rb + 32 + lane; e < re; e += 32) {
-      const DevEdge ed = p.edges[e];
-      const int c = static_cast<int>(static_cast<unsigned>(__ldcg(p.dist + ed.head)) +
-                                     static_cast<unsigned>(fixed_delay(ed.w)));
-      if (c == best) s = max(s, ed.head);
-    }
-    s = warp_max_i(s);
-  }
-
-  // deviations: every fan-out edge whose head is not the successor and has a
-  // finite distance, compacted in edge order into v's own fan-out slots
   int cnt = 0;
   float kmin = __int_as_float(0x7f800000);  // +inf
-  for (int base = rb; base < re; base += 32) {
-    const int e = base + lane;
-    bool valid = false;
-    DevSidetrack rec;
-    if (e < re) {
-      DevEdge ed;
-      int dh;
-      if (base == rb) {
-        ed = e0;
-        dh = dh0;
-      } else {
-        ed = p.edges[e];
-        dh = __ldcg(p.dist + ed.head);
+  if (re - rb <= kRegChunks * 32) {
+    // the whole row in registers: every edge word, then every head distance,
+    // is requested before any is used, so a long row costs about two memory
+    // round trips instead of one per 32-edge chunk
+    DevEdge ed[kRegChunks];
+    int dh[kRegChunks];
+#pragma unroll
+    for (int c = 0; c < kRegChunks; ++c) {
+      const int e = rb + c * 32 + lane;
+      ed[c].head = -1;
+      ed[c].w = 0.f;
+      if (e < re) ed[c] = p.edges[e];
+    }
+#pragma unroll
+    for (int c = 0; c < kRegChunks; ++c) dh[c] = ed[c].head >= 0 ? __ldcg(p.dist + ed[c].head) : INT_MAX;
+    if (lvl == 0) {
+      best = 0;  // sinks (out-degree 0) start at distance 0 (gpucpg.cu:17034-17038)
+    } else {
+#pragma unroll
+      for (int c = 0; c < kRegChunks; ++c)
+        if (ed[c].head >= 0) best = min(best, cand_dist(dh[c], ed[c].w));
+      best = warp_min_i(best);
+#pragma unroll
+      for (int c = 0; c < kRegChunks; ++c)
+        if (ed[c].head >= 0 && cand_dist(dh[c], ed[c].w) == best) s = max(s, ed[c].head);
+      s = warp_max_i(s);
+    }
+    // deviations: fan-out edges whose head is not the successor and has a
+    // finite distance, compacted in edge order into v's own fan-out slots
+#pragma unroll
+    for (int c = 0; c < kRegChunks; ++c) {
+      if (rb + c * 32 >= re) break;
+      const bool valid = ed[c].head >= 0 && ed[c].head != s && dh[c] != INT_MAX;
+      const unsigned bal = __ballot_sync(0xffffffffu, valid);
+      if (valid) {
+        DevSidetrack rec;
+        rec.head = ed[c].head;
+        rec.w = ed[c].w;
+        rec.dist_head = dh[c];
+        rec.key = deviation_key(dh[c], best, ed[c].w);
+        p.dev[rb + cnt + __popc(bal & lanemask_lt())] = rec;
+        kmin = fminf(kmin, rec.key);
       }
-      valid = ed.head != s && dh != INT_MAX;
-      rec.head = ed.head;
-      rec.w = ed.w;
-      rec.dist_head = dh;
-      rec.key = deviation_key(dh, best, ed.w);
+      cnt += __popc(bal);
     }
-    const unsigned bal = __ballot_sync(0xffffffffu, valid);
-    if (valid) {
-      p.dev[rb + cnt + __popc(bal & lanemask_lt())] = rec;
-      kmin = fminf(kmin, rec.key);
+  } else {
+    // long rows (a super-source, say): chunk by chunk
+    if (lvl == 0) {
+      best = 0;
+    } else {
+      for (int e = rb + lane; e < re; e += 32) {
+        const DevEdge ed = p.edges[e];
+        best = min(best, cand_dist(__ldcg(p.dist + ed.head), ed.w));
+      }
+      best = warp_min_i(best);
+      for (int e = rb + lane; e < re; e += 32) {
+        const DevEdge ed = p.edges[e];
+        if (cand_dist(__ldcg(p.dist + ed.head), ed.w) == best) s = max(s, ed.head);
+      }
+      s = warp_max_i(s);
     }
-    cnt += __popc(bal);
+    for (int base = rb; base < re; base += 32) {
+      const int e = base + lane;
+      bool valid = false;
+      DevSidetrack rec;
+      if (e < re) {
+        const DevEdge ed = p.edges[e];
+        const int dh = __ldcg(p.dist + ed.head);
+        valid = ed.head != s && dh != INT_MAX;
+        rec.head = ed.head;
+        rec.w = ed.w;
+        rec.dist_head = dh;
+        rec.key = deviation_key(dh, best, ed.w);
+      }
+      const unsigned bal = __ballot_sync(0xffffffffu, valid);
+      if (valid) {
+        p.dev[rb + cnt + __popc(bal & lanemask_lt())] = rec;
+        kmin = fminf(kmin, rec.key);
+      }
+      cnt += __popc(bal);
+    }
   }
   for (int o = 16; o > 0; o >>= 1) kmin = fminf(kmin, __shfl_xor_sync(0xffffffffu, kmin, o));
 
@@ -127,21 +154,27 @@ __device__ void build_vertex(const SfxtParams& p, int v, int lvl, bool do_kahn) 
 
   if (do_kahn) {
     // every fan-in neighbour loses one pending fan-out; the last one to
-    // reach zero joins the next level
+    // reach zero joins the next level.  Up to four chunks of fan-in are
+    // loaded and decremented before any result is used.
     const int ib = p.iadjp[v];
     const int ie = p.iadjp[v + 1];
-    for (int base = ib; base < ie; base += 32) {
-      const int e = base + lane;
-      int u = -1;
-      bool ready = false;
-      if (e < ie) {
-        u = p.iadj[e];
-        ready = atomicSub(&p.deps[u], 1) == 1;
+    for (int base = ib; base < ie; base += 4 * 32) {
+      int u[4];
+      bool ready[4];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const int e = base + c * 32 + lane;
+        u[c] = e < ie ? p.iadj[e] : -1;
       }
-      const int slot = warp_append(&p.ctr->tail, ready);
-      if (ready) {
-        p.order[slot] = u;
-        p.level_of[u] = lvl + 1;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) ready[c] = u[c] >= 0 && atomicSub(&p.deps[u[c]], 1) == 1;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const int slot = warp_append(&p.ctr->tail, ready[c]);
+        if (ready[c]) {
+          p.order[slot] = u[c];
+          p.level_of[u[c]] = lvl + 1;
+        }
       }
     }
   }
@@ -482,6 +515,27 @@ int launch_scatter_delays(DevEdge* edges, const int32_t* eids, const float* w,
   const int64_t blocks = (count + threads - 1) / threads;
   scatter_delays_kernel<<<static_cast<unsigned>(blocks), threads, 0,
                           static_cast<cudaStream_t>(stream)>>>(edges, eids, w, count);
+  return cudaGetLastError();
+}
+}  // namespace cpg
+
+namespace cpg {
+namespace {
+// Counters for a build: zero, except the heap-pool cursor of an incremental
+// rebuild, which restarts where the first rebuilt level's heaps began.
+__global__ void init_sfxt_counters_kernel(SfxtCounters* c,
+                                          const unsigned long long* pool_mark,
+                                          int start_level) {
+  SfxtCounters z{};
+  if (start_level > 0) z.hnode_used = pool_mark[start_level];
+  *c = z;
+}
+}  // namespace
+
+int launch_init_sfxt_counters(SfxtCounters* c, const unsigned long long* pool_mark,
+                              int start_level, void* stream) {
+  init_sfxt_counters_kernel<<<1, 1, 0, static_cast<cudaStream_t>(stream)>>>(c, pool_mark,
+                                                                            start_level);
   return cudaGetLastError();
 }
 }  // namespace cpg

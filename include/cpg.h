@@ -106,6 +106,9 @@ typedef struct {
   float split;             /* final split (cost threshold) */
   int32_t frontier_used;   /* cpg_frontier actually used by the levelisation */
   int32_t retries;         /* query restarts after a bounded buffer overflowed */
+  /* device time of the query engine by stage (ms): seed, decide, select,
+   * promote, closure, output select, output sort, emit */
+  float engine_stage_ms[8];
 } cpg_stats;
 
 /* ------------------------------------------------------------ lifecycle */

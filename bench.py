@@ -292,6 +292,93 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------- batched form
+BATCH_DESC = ("256 seeded DAGs, pins log-uniform 5,000-200,000, levels U{40..150}, geometric "
+              "out-degree mean U[2,8] (cap 64), fp32 delays U[0.1,10], K log-uniform 100-100,000")
+
+
+def batch_workload(seed=4, count=256):
+    """The batched-form workload: graph generator settings and K per query."""
+    import cpg_b200
+    rng = np.random.default_rng(seed)
+    dags, ks = [], []
+    for i in range(count):
+        n = int(np.exp(rng.uniform(np.log(5_000), np.log(200_000))))
+        levels = int(rng.integers(40, 151))
+        side = max(8, n // (2 * levels))
+        p = cpg_b200.gen_params(seed=seed * 100_000 + i, n_pins=n, n_levels=levels,
+                                n_first=side, n_last=side, level_span=3, degree_kind=1,
+                                deg_mean=float(rng.uniform(2.0, 8.0)), deg_cap=64,
+                                weight_kind=0, w_lo=0.1, w_hi=10.0)
+        dags.append(cpg_b200.generate(p))
+        ks.append(int(np.exp(rng.uniform(np.log(100), np.log(100_000)))))
+    return dags, ks
+
+
+def run_batched(args):
+    """K-paths/sec of the batched form (one captured step answers all 256
+    queries, suffix trees rebuilt each step) against the plain form answering
+    the same queries one at a time on resident graphs."""
+    import torch
+    import cpg_b200
+    dags, ks = batch_workload()
+    stream = torch.cuda.Stream()
+    with cpg_b200.Batch(stream=stream.cuda_stream) as b:
+        for d in dags:
+            b.add_dag(d)
+        b.commit()
+        b.set_queries(list(range(len(dags))), ks)
+        b.run(True)
+        if args.autotune:
+            b.autotune()
+        for _ in range(args.warmup):
+            b.run(True)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            b.run(True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        total = sum(int(b.costs(q).size) for q in range(len(ks)))
+        st = b.stats()
+    # plain form: the same queries one at a time (graphs resident, suffix
+    # tree rebuilt per query as in report_paths)
+    handles = []
+    for d in dags:
+        g = cpg_b200.CpGen(stream=stream.cuda_stream)
+        g.load_dag(d)
+        handles.append(g)
+    for g, k in zip(handles, ks):
+        g.levelize()
+        g.report_paths(k)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for g, k in zip(handles, ks):
+        g.levelize()
+        g.report_paths(k)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    plain_ms = e0.elapsed_time(e1)
+    for g in handles:
+        g.close()
+    line = {
+        "form": "batched", "metric": METRIC, "value": total / (ms / 1e3), "unit": "paths/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "batch256", "desc": BATCH_DESC, "queries": len(ks),
+                   "paths_returned": total, "pins": int(sum(d.n for d in dags)),
+                   "edges": int(sum(d.m for d in dags))},
+        "plain_sequential": {"value": total / (plain_ms / 1e3), "unit": "paths/s",
+                             "ms": plain_ms},
+        "speedup_vs_plain": plain_ms / ms,
+        "batch_stats": st,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_profile_case(args):
     """A short fixed sequence for ncu: one warm-up query, then one query
     (suffix tree + engine) on the same workload at --k."""
@@ -319,9 +406,13 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-case", action="store_true",
                     help="one warm-up and one measured query only (for ncu)")
+    ap.add_argument("--form", default="plain", choices=["plain", "batched", "served"])
+    ap.add_argument("--autotune", action="store_true")
     args = ap.parse_args()
     if args.profile_case:
         run_profile_case(args)
+    elif args.form == "batched":
+        run_batched(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

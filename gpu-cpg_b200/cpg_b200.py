@@ -72,6 +72,15 @@ class Stats(C.Structure):
     ]
 
 
+class BatchStats(C.Structure):
+    _fields_ = [
+        ("step_ms", C.c_double), ("sfxt_ms", C.c_double), ("paths_accepted", C.c_int64),
+        ("phases", C.c_int32), ("rounds", C.c_int32), ("graph_captured", C.c_int32),
+        ("retries", C.c_int32), ("bytes_reserved", C.c_int64),
+        ("sfxt_ctas_per_sm", C.c_int32), ("engine_ctas_per_sm", C.c_int32),
+    ]
+
+
 class GenParams(C.Structure):
     _fields_ = [
         ("seed", C.c_uint64), ("n_pins", C.c_int32), ("n_levels", C.c_int32),
@@ -118,6 +127,18 @@ def _load():
         "cpg_sync": (C.c_int, [H]),
         "cpg_select_topk": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, P(C.c_int64), C.c_void_p]),
         "cpg_select_topk_noalloc": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, P(C.c_int64), C.c_void_p]),
+        "cpg_batch_create": (C.c_int, [P(C.c_void_p), P(Options)]),
+        "cpg_batch_destroy": (C.c_int, [C.c_void_p]),
+        "cpg_batch_last_error": (C.c_char_p, [C.c_void_p]),
+        "cpg_batch_add_graph": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
+                                          C.c_void_p, P(C.c_int32)]),
+        "cpg_batch_add_dag": (C.c_int, [C.c_void_p, C.c_void_p, P(C.c_int32)]),
+        "cpg_batch_commit": (C.c_int, [C.c_void_p]),
+        "cpg_batch_set_queries": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
+        "cpg_batch_run": (C.c_int, [C.c_void_p, C.c_int32]),
+        "cpg_batch_get_costs": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int64, P(C.c_int64)]),
+        "cpg_batch_get_stats": (C.c_int, [C.c_void_p, P(BatchStats)]),
+        "cpg_batch_autotune": (C.c_int, [C.c_void_p]),
         "cpg_gen_params_init": (None, [P(GenParams)]),
         "cpg_dag_generate": (C.c_int, [P(GenParams), P(C.c_void_p)]),
         "cpg_dag_sizes": (C.c_int, [C.c_void_p, P(C.c_int32), P(C.c_int32)]),
@@ -338,6 +359,89 @@ class CpGen:
 
     def sync(self):
         self._check(lib.cpg_sync(self._h), "sync")
+
+
+class Batch:
+    """Batched form: many (graph, k) queries per step, one captured launch
+    sequence (see cpg_batch_* in include/cpg.h)."""
+
+    def __init__(self, device: int = 0, stream: int | None = None,
+                 division: int = DIV_REFERENCE, root_seeding: int = ROOTS_REFERENCE):
+        o = Options()
+        lib.cpg_options_init(C.byref(o))
+        o.device = device
+        o.stream = stream
+        o.division = division
+        o.root_seeding = root_seeding
+        self._b = C.c_void_p()
+        st = lib.cpg_batch_create(C.byref(self._b), C.byref(o))
+        if st != CPG_OK:
+            raise CpgError(st, "cpg_batch_create failed")
+        self.ks = []
+
+    def _check(self, st, what):
+        if st != CPG_OK:
+            m = lib.cpg_batch_last_error(self._b)
+            raise CpgError(st, f"{what}: {m.decode() if m else ''}")
+
+    def close(self):
+        if self._b:
+            lib.cpg_batch_destroy(self._b)
+            self._b = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def add_graph(self, n, adjp, adj, w) -> int:
+        adjp = np.ascontiguousarray(adjp, np.int32)
+        adj = np.ascontiguousarray(adj, np.int32)
+        w = np.ascontiguousarray(w, np.float32)
+        gid = C.c_int32()
+        self._check(lib.cpg_batch_add_graph(self._b, int(n), int(adj.size), _ptr(adjp), _ptr(adj),
+                                            _ptr(w), C.byref(gid)), "add_graph")
+        return gid.value
+
+    def add_dag(self, dag: "Dag") -> int:
+        order = np.argsort(dag.src, kind="stable")
+        adjp = np.zeros(dag.n + 1, np.int64)
+        np.add.at(adjp, dag.src + 1, 1)
+        return self.add_graph(dag.n, np.cumsum(adjp).astype(np.int32), dag.dst[order], dag.w[order])
+
+    def commit(self):
+        self._check(lib.cpg_batch_commit(self._b), "commit")
+
+    def set_queries(self, graph_ids, ks):
+        g = np.ascontiguousarray(graph_ids, np.int32)
+        k = np.ascontiguousarray(ks, np.int64)
+        self.ks = k.tolist()
+        self._check(lib.cpg_batch_set_queries(self._b, int(g.size), _ptr(g), _ptr(k)), "set_queries")
+
+    def run(self, rebuild_sfxt: bool = True):
+        self._check(lib.cpg_batch_run(self._b, int(rebuild_sfxt)), "run")
+
+    def autotune(self):
+        self._check(lib.cpg_batch_autotune(self._b), "autotune")
+
+    def costs(self, q: int) -> np.ndarray:
+        cap = int(self.ks[q])
+        out = np.empty(max(cap, 1), np.float32)
+        n = C.c_int64()
+        self._check(lib.cpg_batch_get_costs(self._b, int(q), _ptr(out), cap, C.byref(n)), "costs")
+        return out[: n.value]
+
+    def stats(self) -> dict:
+        s = BatchStats()
+        self._check(lib.cpg_batch_get_stats(self._b, C.byref(s)), "stats")
+        return {f: getattr(s, f) for f, _ in BatchStats._fields_}
 
 
 def select_topk(d_costs: int, n: int, k: int, d_out: int, stream: int | None = None) -> int:

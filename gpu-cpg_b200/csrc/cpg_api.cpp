@@ -71,6 +71,11 @@ struct cpg_handle {
   unsigned long long n_paths = 0;
   bool result_valid = false;
 
+  // launch shape (chosen by the batch autotuner; 0 = maximum co-resident)
+  int sfxt_grid_limit = 0;
+  int engine_grid_limit = 0;
+  int sel_schedule = 0;  // 0: 11/11/10-bit select digits, 1: 8/8/8/8
+
   // staging
   void* pinned = nullptr;
   cudaEvent_t ev[6] = {};
@@ -268,6 +273,7 @@ SfxtParams sfxt_params(cpg_handle* h, int32_t start_level) {
   p.start_level = start_level;
   p.known_levels = h->levels;
   p.spin_limit = h->opts.spin_limit ? h->opts.spin_limit : kDefaultSpinLimit;
+  p.grid_limit = h->sfxt_grid_limit;
   return p;
 }
 
@@ -623,31 +629,39 @@ int try_query(cpg_handle* h, unsigned long long k) {
   return CPG_OK;
 }
 
-// The whole query on the device: one cooperative launch of the engine.
-// Returns kRetry when a bounded buffer overflowed.
-int engine_query(cpg_handle* h, unsigned long long k) {
-  Status st = alloc_query(h, k);
+// ---- query engine: prepare (allocate, upload the query table), enqueue
+// (asynchronous and capturable: memsets and one cooperative launch) and
+// finish (read counters back, map errors).
+
+// Buffers for nq queries whose K sum to k_total.
+Status engine_prepare(cpg_handle* h, const std::vector<EngineQuery>& qs,
+                      unsigned long long k_total) {
+  Status st = alloc_query(h, k_total);
   if (st != CPG_OK) return st;
+  int grid = 0;
+  CK(engine_grid(h->device, h->engine_grid_limit, &grid), "engine occupancy");
+  const size_t nq = qs.size();
+  CK(ensure(h->d_pq, h->cap_paths * 4), "alloc paths");
+  CK(ensure(h->d_qids, 2 * k_total * 4), "alloc sort");
+  CK(ensure(h->d_ehist, nq * static_cast<size_t>(kSelBins) * 4), "alloc select");
+  CK(ensure(h->d_esort, (256 * static_cast<size_t>(grid) + 256) * 4), "alloc sort");
+  CK(ensure(h->d_equery, nq * sizeof(EngineQuery)), "alloc queries");
+  CK(ensure(h->d_ectr, sizeof(EngineCounters)), "alloc counters");
+  CK(cudaMemcpyAsync(h->d_equery.p, qs.data(), nq * sizeof(EngineQuery),
+                     cudaMemcpyHostToDevice, h->stream), "H2D queries");
+  CK(cudaStreamSynchronize(h->stream), "H2D queries");
+  return CPG_OK;
+}
+
+Status engine_enqueue(cpg_handle* h, int nq, unsigned long long k_total) {
   cudaStream_t s = h->stream;
   int grid = 0;
-  CK(engine_grid(h->device, &grid), "engine occupancy");
-  const size_t cp = h->cap_paths;
-  CK(ensure(h->d_pq, cp * 4), "alloc paths");
-  CK(ensure(h->d_qids, 2 * k * 4), "alloc sort");
-  CK(ensure(h->d_ehist, static_cast<size_t>(kSelBins) * 4), "alloc select");
-  CK(ensure(h->d_esort, (256 * static_cast<size_t>(grid) + 256) * 4), "alloc sort");
-  CK(ensure(h->d_equery, sizeof(EngineQuery)), "alloc query");
-  CK(ensure(h->d_ectr, sizeof(EngineCounters)), "alloc counters");
-  EngineQuery q{};
-  q.k = static_cast<long long>(k);
-  q.src_beg = 0;
-  q.src_end = h->n_srcs;
-  CK(cudaMemcpyAsync(h->d_equery.p, &q, sizeof(q), cudaMemcpyHostToDevice, s), "H2D query");
+  CK(engine_grid(h->device, h->engine_grid_limit, &grid), "engine occupancy");
   CK(cudaMemsetAsync(h->d_ectr.p, 0, sizeof(EngineCounters), s), "memset");
-  CK(cudaMemsetAsync(h->d_ehist.p, 0, static_cast<size_t>(kSelBins) * 4, s), "memset");
+  CK(cudaMemsetAsync(h->d_ehist.p, 0, static_cast<size_t>(nq) * kSelBins * 4, s), "memset");
   // every output slot is written by the compaction; zero-filling keeps a path
   // index in range even if selection and compaction ever disagreed
-  CK(cudaMemsetAsync(h->d_vals.p, 0, 2 * k * 4, s), "memset");
+  CK(cudaMemsetAsync(h->d_vals.p, 0, 2 * k_total * 4, s), "memset");
   EngineParams p{};
   p.g.adjp = P<int32_t>(h->d_adjp);
   p.g.dist = P<int32_t>(h->d_dist);
@@ -658,7 +672,7 @@ int engine_query(cpg_handle* h, unsigned long long k) {
   p.g.division = h->opts.division;
   p.srcs = P<int32_t>(h->d_srcs);
   p.q = P<EngineQuery>(h->d_equery);
-  p.nq = 1;
+  p.nq = nq;
   p.root_ref = h->opts.root_seeding == CPG_ROOTS_REFERENCE;
   p.ps = path_store(h);
   p.pq = P<int32_t>(h->d_pq);
@@ -670,12 +684,12 @@ int engine_query(cpg_handle* h, unsigned long long k) {
   p.front_cap = h->cap_front;
   p.hist = P<unsigned int>(h->d_ehist);
   p.keys[0] = P<unsigned int>(h->d_keys);
-  p.keys[1] = P<unsigned int>(h->d_keys) + k;
+  p.keys[1] = P<unsigned int>(h->d_keys) + k_total;
   p.qids[0] = P<unsigned int>(h->d_qids);
-  p.qids[1] = P<unsigned int>(h->d_qids) + k;
+  p.qids[1] = P<unsigned int>(h->d_qids) + k_total;
   p.vals[0] = P<unsigned int>(h->d_vals);
-  p.vals[1] = P<unsigned int>(h->d_vals) + k;
-  p.out_cap = k;
+  p.vals[1] = P<unsigned int>(h->d_vals) + k_total;
+  p.out_cap = k_total;
   p.sort_hist = P<unsigned int>(h->d_esort);
   p.digit_tot = P<unsigned int>(h->d_esort) + 256 * static_cast<size_t>(grid);
   p.rank_of = P<int32_t>(h->d_rank);
@@ -683,35 +697,72 @@ int engine_query(cpg_handle* h, unsigned long long k) {
   p.out_nodes = P<cpg_path_node>(h->d_out_nodes);
   p.ctr = P<EngineCounters>(h->d_ectr);
   p.spin_limit = h->opts.spin_limit ? h->opts.spin_limit : kDefaultSpinLimit;
-  CK(cudaEventRecord(h->ev[2], s), "event");
+  p.grid_limit = h->engine_grid_limit;
+  if (h->sel_schedule == 1) {  // four 8-bit digits
+    p.sel_passes = 4;
+    for (int i = 0; i < 4; ++i) {
+      p.sel_shift[i] = 24 - 8 * i;
+      p.sel_bits[i] = 8;
+    }
+  } else {                     // 11 + 11 + 10 bits
+    p.sel_passes = 3;
+    p.sel_shift[0] = 21; p.sel_bits[0] = 11;
+    p.sel_shift[1] = 10; p.sel_bits[1] = 11;
+    p.sel_shift[2] = 0;  p.sel_bits[2] = 10;
+  }
   CK(launch_engine(p, h->device, s), "engine launch");
-  CK(cudaEventRecord(h->ev[3], s), "event");
-  h->stats.kernel_launches += 1;
+  return CPG_OK;
+}
+
+// Counters and the per-query table back on the host.  kRetry on overflow.
+int engine_finish(cpg_handle* h, std::vector<EngineQuery>& qout, EngineCounters& c,
+                  unsigned long long k_total) {
+  const size_t nq = qout.size();
   char* hb = static_cast<char*>(h->pinned);
-  CK(cudaMemcpyAsync(hb, h->d_ectr.p, sizeof(EngineCounters), cudaMemcpyDeviceToHost, s), "D2H counters");
-  CK(cudaMemcpyAsync(hb + 512, h->d_equery.p, sizeof(EngineQuery), cudaMemcpyDeviceToHost, s), "D2H query");
-  CK(cudaStreamSynchronize(s), "engine");
-  EngineCounters c;
-  EngineQuery qo;
+  CK(cudaMemcpyAsync(hb, h->d_ectr.p, sizeof(EngineCounters), cudaMemcpyDeviceToHost,
+                     h->stream), "D2H counters");
+  CK(cudaStreamSynchronize(h->stream), "engine");
   std::memcpy(&c, hb, sizeof(c));
-  std::memcpy(&qo, hb + 512, sizeof(qo));
   if (c.err == kDevTimeout)
     return fail(h, CPG_ERR_TIMEOUT, "query engine: grid barrier wait ran out");
   if (c.err == kDevCapacity) return kRetry;
-  float ms = 0.f;
-  cudaEventElapsedTime(&ms, h->ev[2], h->ev[3]);
-  h->stats.pfxt_ms = ms;
-  h->stats.select_ms = 0.0;
+  CK(cudaMemcpy(qout.data(), h->d_equery.p, nq * sizeof(EngineQuery), cudaMemcpyDeviceToHost),
+     "D2H queries");
   h->stats.paths_accepted = static_cast<int64_t>(c.paths);
   h->stats.items_generated = static_cast<int64_t>(c.paths + c.pend_out);
   h->stats.pending_peak = static_cast<int64_t>(c.pend_out);
   h->stats.phases = c.phases;
   h->stats.rounds = c.rounds;
-  h->stats.split = qo.t;
   for (int i = 0; i < 8; ++i) h->stats.engine_stage_ms[i] = static_cast<float>(c.t_ns[i] * 1e-6);
   h->n_paths = c.paths;
-  h->n_result = static_cast<int64_t>(qo.k_out);
-  h->sorted_vals_off = c.sorted_buf ? k : 0;
+  h->sorted_vals_off = c.sorted_buf ? k_total : 0;
+  return CPG_OK;
+}
+
+// One query through the engine.  Returns kRetry when a bounded buffer
+// overflowed.
+int engine_query(cpg_handle* h, unsigned long long k) {
+  std::vector<EngineQuery> qs(1);
+  qs[0].k = static_cast<long long>(k);
+  qs[0].src_beg = 0;
+  qs[0].src_end = h->n_srcs;
+  Status st = engine_prepare(h, qs, k);
+  if (st != CPG_OK) return st;
+  cudaStream_t s = h->stream;
+  CK(cudaEventRecord(h->ev[2], s), "event");
+  st = engine_enqueue(h, 1, k);
+  if (st != CPG_OK) return st;
+  CK(cudaEventRecord(h->ev[3], s), "event");
+  h->stats.kernel_launches += 1;
+  EngineCounters c;
+  const int r = engine_finish(h, qs, c, k);
+  if (r != CPG_OK) return r;
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, h->ev[2], h->ev[3]);
+  h->stats.pfxt_ms = ms;
+  h->stats.select_ms = 0.0;
+  h->stats.split = qs[0].t;
+  h->n_result = static_cast<int64_t>(qs[0].k_out);
   h->result_valid = true;
   return CPG_OK;
 }
@@ -1142,11 +1193,353 @@ cpg_status cpg_select_topk(const float* d_costs, int64_t n, int64_t k, float* d_
   return CPG_OK;
 }
 
-// ---------------------------------------------------------------- generator
+// ---------------------------------------------------------------- batched form
 
 struct cpg_dag {
   EdgeList el;
 };
+
+struct cpg_batch {
+  cpg_handle* h = nullptr;          // owns the side-by-side device graph
+  std::string err;
+  // graphs added so far, as one fan-out CSR
+  std::vector<int32_t> adjp{0}, adj;
+  std::vector<float> w;
+  std::vector<int32_t> voff{0};     // first vertex of each graph
+  bool committed = false;
+  std::vector<int32_t> src_beg, src_end;  // per graph: its sources in d_srcs
+  // queries
+  std::vector<EngineQuery> qs;
+  unsigned long long k_total = 0;
+  std::vector<EngineQuery> qout;
+  bool have_result = false;
+  // the captured step
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int captured_rebuild = -1;        // rebuild flag of the captured graph
+  bool prepared = false;
+  cpg_batch_stats stats{};
+};
+
+namespace {
+
+void batch_drop_graph(cpg_batch* b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+  b->captured_rebuild = -1;
+}
+
+Status batch_fail(cpg_batch* b, Status s, const std::string& msg) {
+  b->err = msg;
+  return s;
+}
+
+// Enqueue one step on the handle's stream (capturable).
+Status batch_enqueue(cpg_batch* b, bool rebuild) {
+  cpg_handle* h = b->h;
+  int launches = 0;
+  if (rebuild) {
+    Status st = enqueue_sfxt(h, 0, &launches);
+    if (st != CPG_OK) return st;
+  }
+  return engine_enqueue(h, static_cast<int>(b->qs.size()), b->k_total);
+}
+
+// Capture the step into a CUDA graph; on any capture error the step runs as
+// plain launches instead (graph_captured = 0).
+void batch_capture(cpg_batch* b, bool rebuild) {
+  batch_drop_graph(b);
+  cudaStream_t s = b->h->stream;
+  if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  const Status st = batch_enqueue(b, rebuild);
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(s, &g);
+  if (st != CPG_OK || e != cudaSuccess || !g) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    return;
+  }
+  if (cudaGraphInstantiate(&b->exec, g, 0) != cudaSuccess) {
+    cudaGraphDestroy(g);
+    b->exec = nullptr;
+    cudaGetLastError();
+    return;
+  }
+  b->graph = g;
+  b->captured_rebuild = rebuild ? 1 : 0;
+}
+
+// One step with the current capacities.  kRetry on overflow.
+int batch_step(cpg_batch* b, bool rebuild) {
+  cpg_handle* h = b->h;
+  cudaStream_t s = h->stream;
+  if (!b->prepared) {
+    Status st = engine_prepare(h, b->qs, b->k_total);
+    if (st != CPG_OK) return st;
+    b->prepared = true;
+    batch_drop_graph(b);
+  }
+  if (b->captured_rebuild != (rebuild ? 1 : 0)) batch_capture(b, rebuild);
+  CK(cudaEventRecord(h->ev[4], s), "event");
+  if (b->exec) {
+    CK(cudaGraphLaunch(b->exec, s), "graph launch");
+  } else {
+    Status st = batch_enqueue(b, rebuild);
+    if (st != CPG_OK) return st;
+  }
+  CK(cudaEventRecord(h->ev[5], s), "event");
+  if (rebuild) {
+    const int r = finish_sfxt(h, 0);
+    if (r == kRetry) {
+      Status st = grow_heap_pool(h);
+      if (st != CPG_OK) return st;
+      batch_drop_graph(b);
+      return kRetry;
+    }
+    if (r != CPG_OK) return r;
+  }
+  b->qout = b->qs;
+  EngineCounters c;
+  const int r = engine_finish(h, b->qout, c, b->k_total);
+  if (r == kRetry) {
+    b->prepared = false;
+    return kRetry;
+  }
+  if (r != CPG_OK) return r;
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, h->ev[4], h->ev[5]);
+  b->stats.step_ms = ms;
+  b->stats.sfxt_ms = 0.0;
+  b->stats.paths_accepted = static_cast<int64_t>(c.paths);
+  b->stats.phases = c.phases;
+  b->stats.rounds = c.rounds;
+  b->stats.graph_captured = b->exec ? 1 : 0;
+  b->stats.bytes_reserved = h->stats.bytes_reserved;
+  b->have_result = true;
+  return CPG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+cpg_status cpg_batch_create(cpg_batch** out, const cpg_options* opts) {
+  if (!out) return CPG_ERR_INVALID;
+  *out = nullptr;
+  cpg_batch* b = new (std::nothrow) cpg_batch();
+  if (!b) return CPG_ERR_OOM;
+  const cpg_status st = cpg_create(&b->h, opts);
+  if (st != CPG_OK) {
+    delete b;
+    return st;
+  }
+  *out = b;
+  return CPG_OK;
+}
+
+cpg_status cpg_batch_destroy(cpg_batch* b) {
+  if (!b) return CPG_ERR_INVALID;
+  batch_drop_graph(b);
+  if (b->h) cpg_destroy(b->h);
+  delete b;
+  return CPG_OK;
+}
+
+const char* cpg_batch_last_error(const cpg_batch* b) {
+  if (!b) return "null batch";
+  return b->err.empty() ? cpg_last_error(b->h) : b->err.c_str();
+}
+
+cpg_status cpg_batch_add_graph(cpg_batch* b, int32_t n, int32_t m, const int32_t* adjp,
+                               const int32_t* adjncy, const float* w, int32_t* graph_id) {
+  if (!b || n < 0 || m < 0 || !adjp || (m > 0 && (!adjncy || !w))) return CPG_ERR_INVALID;
+  if (adjp[0] != 0 || adjp[n] != m)
+    return batch_fail(b, CPG_ERR_INVALID, "CSR offsets must start at 0 and end at m");
+  const int64_t base_v = b->voff.back();
+  const int64_t base_e = static_cast<int64_t>(b->adj.size());
+  if (base_v + n > INT32_MAX - 2 || base_e + m > INT32_MAX - 1)
+    return batch_fail(b, CPG_ERR_CAPACITY, "batch exceeds 32-bit vertex or edge ids");
+  for (int32_t v = 0; v < n; ++v) b->adjp.push_back(static_cast<int32_t>(base_e + adjp[v + 1]));
+  for (int32_t e = 0; e < m; ++e) {
+    if (adjncy[e] < 0 || adjncy[e] >= n)
+      return batch_fail(b, CPG_ERR_INVALID, "edge head out of range");
+    b->adj.push_back(static_cast<int32_t>(base_v + adjncy[e]));
+  }
+  b->w.insert(b->w.end(), w, w + m);
+  b->voff.push_back(static_cast<int32_t>(base_v + n));
+  if (graph_id) *graph_id = static_cast<int32_t>(b->voff.size() - 2);
+  b->committed = false;
+  return CPG_OK;
+}
+
+cpg_status cpg_batch_add_dag(cpg_batch* b, const cpg_dag* d, int32_t* graph_id) {
+  if (!b || !d) return CPG_ERR_INVALID;
+  HostGraph g;
+  std::string err;
+  Status st = edges_to_csr(d->el, g, err);
+  if (st != CPG_OK) return batch_fail(b, st, err);
+  return cpg_batch_add_graph(b, g.n, g.m, g.adjp.data(), g.adj.data(), g.w.data(), graph_id);
+}
+
+cpg_status cpg_batch_commit(cpg_batch* b) {
+  if (!b) return CPG_ERR_INVALID;
+  cpg_handle* h = b->h;
+  const int32_t n = b->voff.back();
+  Status st = upload_graph(h, n, static_cast<int32_t>(b->adj.size()), b->adjp.data(),
+                           b->adj.data(), b->w.data());
+  if (st != CPG_OK) return st;
+  // sources of each graph: a contiguous run of the id-sorted source list
+  std::vector<int32_t> srcs(h->n_srcs);
+  if (h->n_srcs)
+    CK(cudaMemcpy(srcs.data(), h->d_srcs.p, srcs.size() * 4, cudaMemcpyDeviceToHost), "D2H sources");
+  const size_t ng = b->voff.size() - 1;
+  b->src_beg.assign(ng, 0);
+  b->src_end.assign(ng, 0);
+  for (size_t g = 0; g < ng; ++g) {
+    b->src_beg[g] = static_cast<int32_t>(
+        std::lower_bound(srcs.begin(), srcs.end(), b->voff[g]) - srcs.begin());
+    b->src_end[g] = static_cast<int32_t>(
+        std::lower_bound(srcs.begin(), srcs.end(), b->voff[g + 1]) - srcs.begin());
+  }
+  b->committed = true;
+  b->prepared = false;
+  batch_drop_graph(b);
+  return CPG_OK;
+}
+
+cpg_status cpg_batch_set_queries(cpg_batch* b, int32_t nq, const int32_t* graph_ids,
+                                 const int64_t* ks) {
+  if (!b || nq <= 0 || !graph_ids || !ks) return CPG_ERR_INVALID;
+  if (!b->committed) return batch_fail(b, CPG_ERR_STATE, "commit the graphs first");
+  if (nq > kMaxQueries) return batch_fail(b, CPG_ERR_CAPACITY, "more than 4096 queries");
+  const int32_t ng = static_cast<int32_t>(b->voff.size() - 1);
+  std::vector<EngineQuery> qs(nq);
+  unsigned long long tot = 0;
+  for (int32_t i = 0; i < nq; ++i) {
+    if (graph_ids[i] < 0 || graph_ids[i] >= ng || ks[i] < 0 || ks[i] > (int64_t{1} << 30))
+      return batch_fail(b, CPG_ERR_INVALID, "bad query");
+    qs[i] = EngineQuery{};
+    qs[i].k = ks[i];
+    qs[i].src_beg = b->src_beg[graph_ids[i]];
+    qs[i].src_end = b->src_end[graph_ids[i]];
+    tot += static_cast<unsigned long long>(ks[i]);
+  }
+  if (tot > (1ull << 31)) return batch_fail(b, CPG_ERR_CAPACITY, "sum of k above 2^31");
+  b->qs.swap(qs);
+  b->k_total = tot ? tot : 1;
+  cpg_handle* h = b->h;
+  h->cap_paths = std::max<unsigned long long>(4 * b->k_total, 1 << 16) + h->n_srcs;
+  h->cap_front = std::max<unsigned long long>(2 * b->k_total, 1 << 16);
+  h->cap_pend = std::max<unsigned long long>(8 * b->k_total, 1 << 17) + h->n_srcs;
+  b->prepared = false;
+  b->have_result = false;
+  return CPG_OK;
+}
+
+cpg_status cpg_batch_run(cpg_batch* b, int32_t rebuild_sfxt) {
+  if (!b) return CPG_ERR_INVALID;
+  if (b->qs.empty()) return batch_fail(b, CPG_ERR_STATE, "no queries set");
+  cpg_handle* h = b->h;
+  CK(cudaSetDevice(h->device), "cudaSetDevice");
+  bool rebuild = rebuild_sfxt != 0 || !h->sfxt_valid;
+  b->stats.retries = 0;
+  for (int attempt = 0; attempt < 10; ++attempt) {
+    const int r = batch_step(b, rebuild);
+    if (r == kRetry) {
+      b->stats.retries += 1;
+      size_t free_b = 0, total_b = 0;
+      cudaMemGetInfo(&free_b, &total_b);
+      const size_t held = static_cast<size_t>(h->stats.bytes_reserved);
+      if (4 * held > held + free_b * 9 / 10) break;
+      h->cap_paths *= 4;
+      h->cap_front *= 4;
+      h->cap_pend *= 4;
+      b->prepared = false;
+      rebuild = true;
+      continue;
+    }
+    return static_cast<cpg_status>(r);
+  }
+  return batch_fail(b, CPG_ERR_CAPACITY, "batch buffers cannot grow further");
+}
+
+cpg_status cpg_batch_get_costs(const cpg_batch* bc, int32_t q, float* out, int64_t cap,
+                               int64_t* n_out) {
+  cpg_batch* b = const_cast<cpg_batch*>(bc);
+  if (!b || q < 0 || cap < 0) return CPG_ERR_INVALID;
+  if (!b->have_result || q >= static_cast<int32_t>(b->qout.size()))
+    return batch_fail(b, CPG_ERR_STATE, "no result for that query");
+  cpg_handle* h = b->h;
+  const EngineQuery& Q = b->qout[q];
+  const int64_t n = std::min<int64_t>(cap, static_cast<int64_t>(Q.k_out));
+  if (n_out) *n_out = static_cast<int64_t>(Q.k_out) < cap ? static_cast<int64_t>(Q.k_out) : cap;
+  if (n > 0) {
+    if (!out) return CPG_ERR_INVALID;
+    CK(cudaMemcpy(out, P<float>(h->d_out_cost) + Q.out_off, n * 4, cudaMemcpyDeviceToHost),
+       "D2H costs");
+  }
+  return CPG_OK;
+}
+
+cpg_status cpg_batch_get_stats(const cpg_batch* b, cpg_batch_stats* out) {
+  if (!b || !out) return CPG_ERR_INVALID;
+  *out = b->stats;
+  out->sfxt_ctas_per_sm = b->h->sfxt_grid_limit;
+  out->engine_ctas_per_sm = b->h->engine_grid_limit;
+  return CPG_OK;
+}
+
+cpg_status cpg_batch_autotune(cpg_batch* b) {
+  if (!b) return CPG_ERR_INVALID;
+  if (b->qs.empty()) return batch_fail(b, CPG_ERR_STATE, "no queries set");
+  cpg_handle* h = b->h;
+  int sms = 0;
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device), "attribute");
+  // candidates: persistent CTAs for each kernel (all SMs, half of them) and
+  // the select's digit schedule; each timed over two steps after a warm-up
+  struct Cand {
+    int sfxt, engine, sched;
+  };
+  const Cand cands[] = {{0, 0, 0}, {0, 0, 1}, {sms / 2, 0, 0}, {0, sms / 2, 0},
+                        {sms / 2, sms / 2, 0}};
+  double best = 1e30;
+  Cand pick = cands[0];
+  for (const Cand& c : cands) {
+    h->sfxt_grid_limit = c.sfxt;
+    h->engine_grid_limit = c.engine;
+    h->sel_schedule = c.sched;
+    b->prepared = false;  // sort scratch depends on the engine grid
+    batch_drop_graph(b);
+    cpg_status st = cpg_batch_run(b, 1);
+    if (st != CPG_OK) return st;
+    double t = 0;
+    for (int i = 0; i < 2; ++i) {
+      st = cpg_batch_run(b, 1);
+      if (st != CPG_OK) return st;
+      t += b->stats.step_ms;
+    }
+    if (t < best) {
+      best = t;
+      pick = c;
+    }
+  }
+  h->sfxt_grid_limit = pick.sfxt;
+  h->engine_grid_limit = pick.engine;
+  h->sel_schedule = pick.sched;
+  b->prepared = false;
+  batch_drop_graph(b);
+  return CPG_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- generator
+
 
 void cpg_gen_params_init(cpg_gen_params* p) {
   if (!p) return;

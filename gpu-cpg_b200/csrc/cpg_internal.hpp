@@ -130,6 +130,7 @@ struct SfxtParams {
   int32_t start_level;     // 0: full levelise + relax; > 0: relax from here
   int32_t known_levels;    // level count when start_level > 0
   unsigned int spin_limit;
+  int32_t grid_limit;      // persistent CTAs (0: one per co-resident slot)
 };
 
 constexpr int kSfxtThreads = 1024;  // one block per SM: fewer grid-barrier arrivals
@@ -275,11 +276,15 @@ struct EngineParams {
   cpg_path_node* out_nodes;
   EngineCounters* ctr;
   unsigned int spin_limit;
+  int grid_limit;             // persistent CTAs (0: one per co-resident slot)
+  int sel_passes;             // radix select digit schedule (sum of bits 32)
+  int sel_shift[4];
+  int sel_bits[4];
 };
 
 // Cooperative launch of the engine; *grid_out receives the grid size (the
-// host sizes sort_hist as 256 * grid).
-int engine_grid(int device, int* grid_out);
+// host sizes sort_hist as 256 * grid) for a given CTA limit (0: maximum).
+int engine_grid(int device, int limit, int* grid_out);
 int launch_engine(const EngineParams& p, int device, void* stream);
 
 // ---------------------------------------------------------------- select/sort

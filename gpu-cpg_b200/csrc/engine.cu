@@ -299,12 +299,10 @@ __device__ void select_pick(const EngineParams& p, int shift, int bits) {
 
 __device__ bool run_select(const EngineParams& p, unsigned long long n_paths,
                            const Item* pend, unsigned long long n_pend) {
-  const int shifts[3] = {21, 10, 0};
-  const int bits[3] = {11, 11, 10};
-  for (int pass = 0; pass < 3; ++pass) {
-    select_hist(p, n_paths, pend, n_pend, shifts[pass], bits[pass]);
+  for (int pass = 0; pass < p.sel_passes; ++pass) {
+    select_hist(p, n_paths, pend, n_pend, p.sel_shift[pass], p.sel_bits[pass]);
     if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit)) return false;
-    select_pick(p, shifts[pass], bits[pass]);
+    select_pick(p, p.sel_shift[pass], p.sel_bits[pass]);
     if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit)) return false;
   }
   return true;
@@ -824,20 +822,22 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
 
 }  // namespace
 
-int engine_grid(int device, int* grid_out) {
+int engine_grid(int device, int limit, int* grid_out) {
   int sms = 0, per_sm = 0;
   cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   if (e != cudaSuccess) return e;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, engine_kernel, kEngThreads, 0);
   if (e != cudaSuccess) return e;
   if (per_sm < 1) per_sm = 1;
-  *grid_out = sms * per_sm;
+  int grid = sms * per_sm;
+  if (limit > 0 && limit < grid) grid = limit;
+  *grid_out = grid;
   return cudaSuccess;
 }
 
 int launch_engine(const EngineParams& p, int device, void* stream) {
   int grid = 0;
-  cudaError_t e = static_cast<cudaError_t>(engine_grid(device, &grid));
+  cudaError_t e = static_cast<cudaError_t>(engine_grid(device, p.grid_limit, &grid));
   if (e != cudaSuccess) return e;
   EngineParams pp = p;
   void* args[] = {&pp};

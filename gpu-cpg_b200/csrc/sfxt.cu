@@ -472,6 +472,7 @@ int launch_sfxt(const SfxtParams& p, int device, void* stream, int* grid_out,
   if (e != cudaSuccess) return e;
   if (per_sm < 1) per_sm = 1;
   int grid = sms * per_sm;
+  if (p.grid_limit > 0 && p.grid_limit < grid) grid = p.grid_limit;
   if (grid_out) *grid_out = grid;
   SfxtParams pp = p;
   void* args[] = {&pp};

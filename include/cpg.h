@@ -78,6 +78,7 @@ typedef struct {
 } cpg_options;
 
 typedef struct cpg_handle cpg_handle;
+typedef struct cpg_dag cpg_dag;  /* a generated graph (see cpg_dag_generate) */
 
 /* PfxtNode (gpucpg.cuh:74-107), same field order and 24-byte layout.
  * parent indexes the list returned by cpg_get_paths (-1 for a root, or when
@@ -182,6 +183,52 @@ cpg_status cpg_get_stats(const cpg_handle* h, cpg_stats* out);
 /* Synchronise the handle's stream. */
 cpg_status cpg_sync(cpg_handle* h);
 
+/* ------------------------------------------------------------ batched form */
+/* Many independent queries (graph, k) answered together.  The graphs are
+ * loaded side by side into one device graph; a step rebuilds the suffix
+ * trees of all of them in one persistent launch and answers every query in
+ * one persistent engine launch.  The step is captured once into a CUDA graph
+ * and replayed.  Project-built form: the reference answers one query per
+ * report_paths call and has no batched counterpart. */
+typedef struct cpg_batch cpg_batch;
+
+typedef struct {
+  double step_ms;          /* device time of the last step (CUDA events) */
+  double sfxt_ms;          /* part of step_ms spent in the suffix trees */
+  int64_t paths_accepted;
+  int32_t phases, rounds;
+  int32_t graph_captured;  /* 1 when the step ran as a captured CUDA graph */
+  int32_t retries;
+  int64_t bytes_reserved;
+  int32_t sfxt_ctas_per_sm;   /* launch shape chosen by cpg_batch_autotune */
+  int32_t engine_ctas_per_sm;
+} cpg_batch_stats;
+
+cpg_status cpg_batch_create(cpg_batch** out, const cpg_options* opts);
+cpg_status cpg_batch_destroy(cpg_batch* b);
+const char* cpg_batch_last_error(const cpg_batch* b);
+/* Append one graph (fan-out CSR, copied); *graph_id receives its index. */
+cpg_status cpg_batch_add_graph(cpg_batch* b, int32_t n, int32_t m,
+                               const int32_t* adjp, const int32_t* adjncy,
+                               const float* w, int32_t* graph_id);
+cpg_status cpg_batch_add_dag(cpg_batch* b, const cpg_dag* d, int32_t* graph_id);
+/* Upload every graph added so far (one device graph). */
+cpg_status cpg_batch_commit(cpg_batch* b);
+/* Queries of the next steps: query i asks graph_ids[i] for ks[i] paths. */
+cpg_status cpg_batch_set_queries(cpg_batch* b, int32_t nq,
+                                 const int32_t* graph_ids, const int64_t* ks);
+/* One step: rebuild the suffix trees (if rebuild_sfxt) and answer every
+ * query.  The first step captures the CUDA graph; later steps replay it. */
+cpg_status cpg_batch_run(cpg_batch* b, int32_t rebuild_sfxt);
+/* Costs of query q from the last step (ascending, min(k, paths) of them). */
+cpg_status cpg_batch_get_costs(const cpg_batch* b, int32_t q, float* out,
+                               int64_t cap, int64_t* n_out);
+cpg_status cpg_batch_get_stats(const cpg_batch* b, cpg_batch_stats* out);
+/* Time the candidate launch shapes on the current queries and keep the
+ * fastest (persistent CTAs per SM for the suffix-tree and engine kernels).
+ * Results are unchanged by the choice. */
+cpg_status cpg_batch_autotune(cpg_batch* b);
+
 /* ------------------------------------------------------------ top-K */
 /* The k smallest non-zero values of a device array of path costs, ascending,
  * written to the device buffer d_out (room for k floats); *n_out receives
@@ -241,7 +288,6 @@ typedef struct {
   int32_t add_virtual;
 } cpg_gen_params;
 
-typedef struct cpg_dag cpg_dag;
 void cpg_gen_params_init(cpg_gen_params* p);
 cpg_status cpg_dag_generate(const cpg_gen_params* p, cpg_dag** out);
 cpg_status cpg_dag_sizes(const cpg_dag* d, int32_t* n, int32_t* m);

@@ -379,6 +379,69 @@ def run_batched(args):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- served form
+SERVED_DESC = ("open-loop Poisson stream of 5,000 queries at 500/s over 32 resident graphs from the "
+               "batched-form generator, K log-uniform 100-100,000, 20% re-ask with 1% of the "
+               "graph's delays re-sampled; HBM admission budget 150 GB")
+
+
+def served_stream(n_graphs, sizes, count=5000, rate=500.0, seed=9):
+    rng = np.random.default_rng(seed)
+    gaps = rng.exponential(1.0 / rate, size=count)
+    t = np.cumsum(gaps)
+    qs = []
+    for i in range(count):
+        g = int(rng.integers(n_graphs))
+        k = int(np.exp(rng.uniform(np.log(100), np.log(100_000))))
+        upd = None
+        if rng.random() < 0.2:
+            m = sizes[g]
+            e = rng.choice(m, size=max(1, m // 100), replace=False).astype(np.int32)
+            upd = (e, rng.uniform(0.1, 10.0, size=e.size).astype(np.float32))
+        qs.append((float(t[i]), g, k, upd))
+    return qs
+
+
+def _replay(dags, qs, max_batch):
+    """Submit at the stream's arrival times (open loop), then collect."""
+    import cpg_b200
+    with cpg_b200.Server(max_batch=max_batch, hbm_budget_bytes=150 << 30) as s:
+        for d in dags:
+            s.add_dag(d)
+        s.start()
+        t0 = time.perf_counter()
+        tickets = []
+        for at, g, k, upd in qs:
+            delay = at - (time.perf_counter() - t0)
+            if delay > 0:
+                time.sleep(delay)
+            tickets.append(s.submit(g, k, *(upd if upd else (None, None))))
+        for tk in tickets:
+            s.wait(tk, timeout_ms=600000)
+        st = s.stats()
+        s.stop()
+    return st
+
+
+def run_served(args):
+    dags, _ = batch_workload(seed=5, count=32)
+    qs = served_stream(len(dags), [d.m for d in dags], count=args.served_queries)
+    served = _replay(dags, qs, max_batch=256)
+    plain = _replay(dags, qs, max_batch=1)
+    line = {
+        "form": "served", "metric": METRIC, "value": served["paths_per_s"], "unit": "paths/s",
+        "n_gpus": 1, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "served5000", "desc": SERVED_DESC, "queries": len(qs),
+                   "graphs": len(dags)},
+        "p50_ms": served["p50_ms"], "p99_ms": served["p99_ms"],
+        "served": served,
+        "plain_sequential": {"value": plain["paths_per_s"], "p50_ms": plain["p50_ms"],
+                             "p99_ms": plain["p99_ms"], "stats": plain},
+        "speedup_vs_plain": served["paths_per_s"] / max(plain["paths_per_s"], 1e-9),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_profile_case(args):
     """A short fixed sequence for ncu: one warm-up query, then one query
     (suffix tree + engine) on the same workload at --k."""
@@ -408,11 +471,14 @@ def main():
                     help="one warm-up and one measured query only (for ncu)")
     ap.add_argument("--form", default="plain", choices=["plain", "batched", "served"])
     ap.add_argument("--autotune", action="store_true")
+    ap.add_argument("--served-queries", type=int, default=5000)
     args = ap.parse_args()
     if args.profile_case:
         run_profile_case(args)
     elif args.form == "batched":
         run_batched(args)
+    elif args.form == "served":
+        run_served(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

@@ -81,6 +81,21 @@ class BatchStats(C.Structure):
     ]
 
 
+class ServerOptions(C.Structure):
+    _fields_ = [("max_batch", C.c_int32), ("hbm_budget_bytes", C.c_int64),
+                ("reserved", C.c_int32 * 6)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [
+        ("completed", C.c_int64), ("paths", C.c_int64), ("p50_ms", C.c_double),
+        ("p99_ms", C.c_double), ("mean_ms", C.c_double), ("max_ms", C.c_double),
+        ("wall_s", C.c_double), ("paths_per_s", C.c_double), ("launches", C.c_int64),
+        ("sfxt_rebuilds", C.c_int64), ("busy_ms", C.c_double), ("max_batch_seen", C.c_int32),
+        ("reserved", C.c_int32),
+    ]
+
+
 class GenParams(C.Structure):
     _fields_ = [
         ("seed", C.c_uint64), ("n_pins", C.c_int32), ("n_levels", C.c_int32),
@@ -139,6 +154,20 @@ def _load():
         "cpg_batch_get_costs": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int64, P(C.c_int64)]),
         "cpg_batch_get_stats": (C.c_int, [C.c_void_p, P(BatchStats)]),
         "cpg_batch_autotune": (C.c_int, [C.c_void_p]),
+        "cpg_server_options_init": (None, [P(ServerOptions)]),
+        "cpg_server_create": (C.c_int, [P(C.c_void_p), P(Options), P(ServerOptions)]),
+        "cpg_server_destroy": (C.c_int, [C.c_void_p]),
+        "cpg_server_last_error": (C.c_char_p, [C.c_void_p]),
+        "cpg_server_add_graph": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
+                                           C.c_void_p, P(C.c_int32)]),
+        "cpg_server_add_dag": (C.c_int, [C.c_void_p, C.c_void_p, P(C.c_int32)]),
+        "cpg_server_start": (C.c_int, [C.c_void_p]),
+        "cpg_server_submit": (C.c_int, [C.c_void_p, C.c_int32, C.c_int64, C.c_int32, C.c_void_p,
+                                        C.c_void_p, P(C.c_int64)]),
+        "cpg_server_wait": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, P(C.c_int64),
+                                      P(C.c_double), C.c_int32]),
+        "cpg_server_stop": (C.c_int, [C.c_void_p]),
+        "cpg_server_get_stats": (C.c_int, [C.c_void_p, P(ServerStats)]),
         "cpg_gen_params_init": (None, [P(GenParams)]),
         "cpg_dag_generate": (C.c_int, [P(GenParams), P(C.c_void_p)]),
         "cpg_dag_sizes": (C.c_int, [C.c_void_p, P(C.c_int32), P(C.c_int32)]),
@@ -442,6 +471,95 @@ class Batch:
         s = BatchStats()
         self._check(lib.cpg_batch_get_stats(self._b, C.byref(s)), "stats")
         return {f: getattr(s, f) for f, _ in BatchStats._fields_}
+
+
+class Server:
+    """Served form: a C++ request loop over resident graphs with continuous
+    batching (see cpg_server_* in include/cpg.h)."""
+
+    def __init__(self, device: int = 0, max_batch: int = 256, hbm_budget_bytes: int = 150 << 30,
+                 division: int = DIV_REFERENCE, root_seeding: int = ROOTS_REFERENCE):
+        o = Options()
+        lib.cpg_options_init(C.byref(o))
+        o.device = device
+        o.division = division
+        o.root_seeding = root_seeding
+        so = ServerOptions()
+        lib.cpg_server_options_init(C.byref(so))
+        so.max_batch = max_batch
+        so.hbm_budget_bytes = hbm_budget_bytes
+        self._s = C.c_void_p()
+        st = lib.cpg_server_create(C.byref(self._s), C.byref(o), C.byref(so))
+        if st != CPG_OK:
+            raise CpgError(st, "cpg_server_create failed")
+        self.ks = {}
+
+    def _check(self, st, what):
+        if st != CPG_OK:
+            m = lib.cpg_server_last_error(self._s)
+            raise CpgError(st, f"{what}: {m.decode() if m else ''}")
+
+    def close(self):
+        if self._s:
+            lib.cpg_server_destroy(self._s)
+            self._s = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def add_dag(self, dag: "Dag") -> int:
+        order = np.argsort(dag.src, kind="stable")
+        adjp = np.zeros(dag.n + 1, np.int64)
+        np.add.at(adjp, dag.src + 1, 1)
+        adjp = np.cumsum(adjp).astype(np.int32)
+        adj = np.ascontiguousarray(dag.dst[order], np.int32)
+        w = np.ascontiguousarray(dag.w[order], np.float32)
+        gid = C.c_int32()
+        self._check(lib.cpg_server_add_graph(self._s, int(dag.n), int(adj.size), _ptr(adjp), _ptr(adj),
+                                             _ptr(w), C.byref(gid)), "add_graph")
+        return gid.value
+
+    def start(self):
+        self._check(lib.cpg_server_start(self._s), "start")
+
+    def submit(self, graph_id: int, k: int, eids=None, w=None) -> int:
+        t = C.c_int64()
+        if eids is None:
+            st = lib.cpg_server_submit(self._s, int(graph_id), int(k), 0, None, None, C.byref(t))
+        else:
+            e = np.ascontiguousarray(eids, np.int32)
+            x = np.ascontiguousarray(w, np.float32)
+            st = lib.cpg_server_submit(self._s, int(graph_id), int(k), int(e.size), _ptr(e), _ptr(x),
+                                       C.byref(t))
+        self._check(st, "submit")
+        self.ks[t.value] = int(k)
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = -1):
+        cap = self.ks.pop(ticket, 0)
+        out = np.empty(max(cap, 1), np.float32)
+        n = C.c_int64()
+        lat = C.c_double()
+        self._check(lib.cpg_server_wait(self._s, int(ticket), _ptr(out), cap, C.byref(n), C.byref(lat),
+                                        int(timeout_ms)), "wait")
+        return out[: n.value], lat.value
+
+    def stop(self):
+        self._check(lib.cpg_server_stop(self._s), "stop")
+
+    def stats(self) -> dict:
+        s = ServerStats()
+        self._check(lib.cpg_server_get_stats(self._s, C.byref(s)), "stats")
+        return {f: getattr(s, f) for f, _ in ServerStats._fields_ if f != "reserved"}
 
 
 def select_topk(d_costs: int, n: int, k: int, d_out: int, stream: int | None = None) -> int:

@@ -9,11 +9,17 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <climits>
 #include <cmath>
+#include <condition_variable>
 #include <cstring>
+#include <deque>
+#include <mutex>
 #include <new>
 #include <string>
+#include <thread>
+#include <unordered_map>
 #include <vector>
 
 #include "cpg_internal.hpp"
@@ -56,6 +62,7 @@ struct cpg_handle {
   int32_t dirty_level = -1;  // lowest level whose delays changed
   std::vector<int32_t> h_level_of, h_succ;
   bool h_sfxt_cached = false;
+  bool h_levels_cached = false;  // levels depend on the graph, not on delays
   DevMem d_order, d_lvlp, d_level_of, d_dist, d_succ, d_dev_cnt, d_dev,
       d_ht_root, d_ht_size, d_hnodes, d_pool_mark, d_deps, d_sctr;
   unsigned long long hnode_cap = 0;
@@ -231,6 +238,7 @@ Status upload_graph(cpg_handle* h, int32_t n, int32_t m, const int32_t* adjp,
   h->has_graph = true;
   h->sfxt_valid = false;
   h->h_sfxt_cached = false;
+  h->h_levels_cached = false;
   h->dirty_level = -1;
   h->result_valid = false;
   h->n_result = 0;
@@ -297,7 +305,10 @@ int finish_sfxt(cpg_handle* h, int32_t start_level) {
   if (out->err == kDevTimeout)
     return fail(h, CPG_ERR_TIMEOUT, "suffix tree: grid barrier wait ran out");
   if (out->err == kDevCapacity) return kRetry;
-  if (start_level == 0) h->levels = out->levels;
+  if (start_level == 0) {
+    h->levels = out->levels;
+    h->h_levels_cached = false;
+  }
   h->stats.levels = h->levels;
   h->stats.frontier_used = CPG_FRONTIER_CSR;
   h->sfxt_valid = true;
@@ -348,6 +359,17 @@ Status cache_sfxt_host(cpg_handle* h) {
     CK(cudaMemcpy(h->h_succ.data(), h->d_succ.p, n * 4, cudaMemcpyDeviceToHost), "D2H succ");
   }
   h->h_sfxt_cached = true;
+  return CPG_OK;
+}
+
+// Host copy of the reverse levels (kept across delay updates).
+Status ensure_levels_host(cpg_handle* h) {
+  if (h->h_levels_cached) return CPG_OK;
+  const size_t n = h->g.n;
+  h->h_level_of.resize(n);
+  if (n)
+    CK(cudaMemcpy(h->h_level_of.data(), h->d_level_of.p, n * 4, cudaMemcpyDeviceToHost), "D2H levels");
+  h->h_levels_cached = true;
   return CPG_OK;
 }
 
@@ -949,7 +971,7 @@ cpg_status cpg_update_delays(cpg_handle* h, int64_t count, const int32_t* eids,
   int32_t lowest = INT32_MAX;
   const bool have_levels = h->sfxt_valid || h->dirty_level > 0;
   if (have_levels) {
-    Status st = cache_sfxt_host(h);
+    Status st = ensure_levels_host(h);
     if (st != CPG_OK) return st;
   }
   // tail of each fan-out edge, by binary search over the CSR offsets
@@ -1533,6 +1555,334 @@ cpg_status cpg_batch_autotune(cpg_batch* b) {
   h->sel_schedule = pick.sched;
   b->prepared = false;
   batch_drop_graph(b);
+  return CPG_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- served form
+
+namespace {
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch())
+      .count();
+}
+
+// Predicted device bytes of one query of k paths: path store, frontier and
+// pending piles, sort buffers and outputs at the engine's initial sizing.
+int64_t predicted_bytes(int64_t k) {
+  const int64_t kk = std::max<int64_t>(k, 1);
+  return 4 * kk * 24 + 4 * kk * 16 + 16 * kk * 16 + 6 * kk * 4 + kk * 28 + (64 << 10);
+}
+
+struct ServerReq {
+  int64_t ticket;
+  int32_t graph;
+  int64_t k;
+  std::vector<int32_t> eids;  // union edge ids
+  std::vector<float> w;
+  double t_submit;
+};
+
+struct ServerResult {
+  std::vector<float> costs;
+  double latency_ms = 0;
+  Status status = CPG_OK;
+  bool done = false;
+};
+
+}  // namespace
+
+struct cpg_server {
+  cpg_batch* b = nullptr;
+  cpg_server_options so{};
+  std::string err;
+  std::thread th;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<ServerReq> queue;
+  std::unordered_map<int64_t, ServerResult> results;
+  int64_t next_ticket = 0;
+  bool running = false, stopping = false;
+  // statistics
+  std::vector<double> lat_ms;
+  int64_t paths = 0, launches = 0, rebuilds = 0;
+  double busy_ms = 0, first_submit = -1, last_done = 0;
+  int32_t max_batch_seen = 0;
+};
+
+namespace {
+
+// One engine launch over the admitted queries.  Returns kRetry on overflow.
+int server_launch(cpg_server* sv, const std::vector<ServerReq>& batch,
+                  std::vector<std::vector<float>>& out) {
+  cpg_batch* b = sv->b;
+  cpg_handle* h = b->h;
+  std::vector<EngineQuery> qs(batch.size());
+  unsigned long long k_total = 0;
+  for (size_t i = 0; i < batch.size(); ++i) {
+    qs[i] = EngineQuery{};
+    qs[i].k = batch[i].k;
+    qs[i].src_beg = b->src_beg[batch[i].graph];
+    qs[i].src_end = b->src_end[batch[i].graph];
+    k_total += static_cast<unsigned long long>(batch[i].k);
+  }
+  if (k_total == 0) k_total = 1;
+  h->cap_paths = std::max<unsigned long long>(h->cap_paths, std::max<unsigned long long>(4 * k_total, 1 << 16) + h->n_srcs);
+  h->cap_front = std::max<unsigned long long>(h->cap_front, std::max<unsigned long long>(2 * k_total, 1 << 16));
+  h->cap_pend = std::max<unsigned long long>(h->cap_pend, std::max<unsigned long long>(8 * k_total, 1 << 17) + h->n_srcs);
+  Status st = engine_prepare(h, qs, k_total);
+  if (st != CPG_OK) return st;
+  cudaStream_t s = h->stream;
+  CK(cudaEventRecord(h->ev[4], s), "event");
+  st = engine_enqueue(h, static_cast<int>(qs.size()), k_total);
+  if (st != CPG_OK) return st;
+  CK(cudaEventRecord(h->ev[5], s), "event");
+  EngineCounters c;
+  const int r = engine_finish(h, qs, c, k_total);
+  if (r != CPG_OK) return r;
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, h->ev[4], h->ev[5]);
+  sv->busy_ms += ms;
+  sv->launches += 1;
+  // all outputs in one copy, then split per query
+  unsigned long long total = 0;
+  for (const EngineQuery& q : qs) total = std::max(total, q.out_off + q.k_out);
+  std::vector<float> all(total);
+  if (total)
+    CK(cudaMemcpy(all.data(), h->d_out_cost.p, total * 4, cudaMemcpyDeviceToHost), "D2H costs");
+  out.resize(qs.size());
+  for (size_t i = 0; i < qs.size(); ++i)
+    out[i].assign(all.begin() + qs[i].out_off, all.begin() + qs[i].out_off + qs[i].k_out);
+  return CPG_OK;
+}
+
+void server_loop(cpg_server* sv) {
+  cpg_handle* h = sv->b->h;
+  cudaSetDevice(h->device);
+  for (;;) {
+    std::vector<ServerReq> batch;
+    {
+      std::unique_lock<std::mutex> lk(sv->mu);
+      sv->cv_work.wait(lk, [&] { return sv->stopping || !sv->queue.empty(); });
+      if (sv->queue.empty()) break;  // stopping and drained
+      // admit in arrival order: up to max_batch queries whose predicted
+      // footprint fits the budget; a query that updates delays starts a new
+      // launch so every query sees arrival-order graph state
+      int64_t used = 0;
+      while (!sv->queue.empty() &&
+             static_cast<int32_t>(batch.size()) < std::max(1, sv->so.max_batch)) {
+        ServerReq& r = sv->queue.front();
+        if (!batch.empty() && !r.eids.empty()) break;
+        const int64_t need = predicted_bytes(r.k);
+        if (!batch.empty() && sv->so.hbm_budget_bytes > 0 && used + need > sv->so.hbm_budget_bytes)
+          break;
+        used += need;
+        batch.push_back(std::move(r));
+        sv->queue.pop_front();
+      }
+    }
+    Status st = CPG_OK;
+    if (!batch[0].eids.empty()) {
+      st = cpg_update_delays(h, static_cast<int64_t>(batch[0].eids.size()), batch[0].eids.data(),
+                             batch[0].w.data());
+      if (st == CPG_OK) {
+        st = ensure_sfxt(h);  // incremental: levels at or above the change
+        sv->rebuilds += 1;
+      }
+    }
+    std::vector<std::vector<float>> out;
+    for (int attempt = 0; st == CPG_OK && attempt < 10; ++attempt) {
+      const int r = server_launch(sv, batch, out);
+      if (r == kRetry) {
+        h->cap_paths *= 4;
+        h->cap_front *= 4;
+        h->cap_pend *= 4;
+        continue;
+      }
+      st = static_cast<Status>(r);
+      break;
+    }
+    const double t = now_s();
+    {
+      std::lock_guard<std::mutex> lk(sv->mu);
+      sv->max_batch_seen = std::max<int32_t>(sv->max_batch_seen, static_cast<int32_t>(batch.size()));
+      for (size_t i = 0; i < batch.size(); ++i) {
+        ServerResult& res = sv->results[batch[i].ticket];
+        res.status = st;
+        if (st == CPG_OK && i < out.size()) {
+          res.costs = std::move(out[i]);
+          sv->paths += static_cast<int64_t>(res.costs.size());
+        }
+        res.latency_ms = (t - batch[i].t_submit) * 1e3;
+        res.done = true;
+        sv->lat_ms.push_back(res.latency_ms);
+      }
+      sv->last_done = t;
+      if (st != CPG_OK) sv->err = cpg_last_error(h);
+    }
+    sv->cv_done.notify_all();
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+void cpg_server_options_init(cpg_server_options* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->max_batch = 256;
+  o->hbm_budget_bytes = 150ll << 30;
+}
+
+cpg_status cpg_server_create(cpg_server** out, const cpg_options* opts,
+                             const cpg_server_options* sopts) {
+  if (!out) return CPG_ERR_INVALID;
+  *out = nullptr;
+  cpg_server* sv = new (std::nothrow) cpg_server();
+  if (!sv) return CPG_ERR_OOM;
+  if (sopts) sv->so = *sopts;
+  else cpg_server_options_init(&sv->so);
+  const cpg_status st = cpg_batch_create(&sv->b, opts);
+  if (st != CPG_OK) {
+    delete sv;
+    return st;
+  }
+  *out = sv;
+  return CPG_OK;
+}
+
+cpg_status cpg_server_stop(cpg_server* sv) {
+  if (!sv) return CPG_ERR_INVALID;
+  {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    sv->stopping = true;
+  }
+  sv->cv_work.notify_all();
+  if (sv->th.joinable()) sv->th.join();
+  sv->running = false;
+  return CPG_OK;
+}
+
+cpg_status cpg_server_destroy(cpg_server* sv) {
+  if (!sv) return CPG_ERR_INVALID;
+  cpg_server_stop(sv);
+  if (sv->b) cpg_batch_destroy(sv->b);
+  delete sv;
+  return CPG_OK;
+}
+
+const char* cpg_server_last_error(const cpg_server* sv) {
+  if (!sv) return "null server";
+  return sv->err.empty() ? cpg_batch_last_error(sv->b) : sv->err.c_str();
+}
+
+cpg_status cpg_server_add_graph(cpg_server* sv, int32_t n, int32_t m, const int32_t* adjp,
+                                const int32_t* adjncy, const float* w, int32_t* graph_id) {
+  if (!sv || sv->running) return CPG_ERR_INVALID;
+  return cpg_batch_add_graph(sv->b, n, m, adjp, adjncy, w, graph_id);
+}
+
+cpg_status cpg_server_add_dag(cpg_server* sv, const cpg_dag* d, int32_t* graph_id) {
+  if (!sv || sv->running) return CPG_ERR_INVALID;
+  return cpg_batch_add_dag(sv->b, d, graph_id);
+}
+
+cpg_status cpg_server_start(cpg_server* sv) {
+  if (!sv || sv->running) return CPG_ERR_INVALID;
+  cpg_status st = cpg_batch_commit(sv->b);
+  if (st != CPG_OK) return st;
+  st = cpg_levelize(sv->b->h);
+  if (st != CPG_OK) return st;
+  sv->stopping = false;
+  sv->running = true;
+  sv->th = std::thread(server_loop, sv);
+  return CPG_OK;
+}
+
+cpg_status cpg_server_submit(cpg_server* sv, int32_t graph_id, int64_t k, int32_t n_updates,
+                             const int32_t* eids, const float* w, int64_t* ticket) {
+  if (!sv || !ticket || k < 0 || n_updates < 0 || (n_updates > 0 && (!eids || !w)))
+    return CPG_ERR_INVALID;
+  if (!sv->running) return CPG_ERR_STATE;
+  cpg_batch* b = sv->b;
+  const int32_t ng = static_cast<int32_t>(b->voff.size() - 1);
+  if (graph_id < 0 || graph_id >= ng || k > (int64_t{1} << 30)) return CPG_ERR_INVALID;
+  ServerReq r;
+  r.graph = graph_id;
+  r.k = k;
+  const int32_t e0 = b->adjp[b->voff[graph_id]];
+  const int32_t e1 = b->adjp[b->voff[graph_id + 1]];
+  r.eids.reserve(n_updates);
+  for (int32_t i = 0; i < n_updates; ++i) {
+    if (eids[i] < 0 || e0 + eids[i] >= e1) return CPG_ERR_INVALID;
+    r.eids.push_back(e0 + eids[i]);
+  }
+  r.w.assign(w, w + n_updates);
+  r.t_submit = now_s();
+  {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    r.ticket = sv->next_ticket++;
+    *ticket = r.ticket;
+    if (sv->first_submit < 0) sv->first_submit = r.t_submit;
+    sv->results[r.ticket] = ServerResult{};
+    sv->queue.push_back(std::move(r));
+  }
+  sv->cv_work.notify_one();
+  return CPG_OK;
+}
+
+cpg_status cpg_server_wait(cpg_server* sv, int64_t ticket, float* out, int64_t cap,
+                           int64_t* n_out, double* latency_ms, int32_t timeout_ms) {
+  if (!sv || cap < 0) return CPG_ERR_INVALID;
+  std::unique_lock<std::mutex> lk(sv->mu);
+  auto it = sv->results.find(ticket);
+  if (it == sv->results.end()) return CPG_ERR_INVALID;
+  auto ready = [&] { return sv->results[ticket].done; };
+  if (timeout_ms < 0) {
+    sv->cv_done.wait(lk, ready);
+  } else if (!sv->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready)) {
+    return CPG_ERR_TIMEOUT;
+  }
+  ServerResult res = std::move(sv->results[ticket]);
+  sv->results.erase(ticket);
+  if (res.status != CPG_OK) return res.status;
+  const int64_t n = std::min<int64_t>(cap, static_cast<int64_t>(res.costs.size()));
+  if (n > 0 && out) std::memcpy(out, res.costs.data(), n * 4);
+  if (n_out) *n_out = n;
+  if (latency_ms) *latency_ms = res.latency_ms;
+  return CPG_OK;
+}
+
+cpg_status cpg_server_get_stats(const cpg_server* svc, cpg_server_stats* out) {
+  cpg_server* sv = const_cast<cpg_server*>(svc);
+  if (!sv || !out) return CPG_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(sv->mu);
+  *out = cpg_server_stats{};
+  std::vector<double> l = sv->lat_ms;
+  std::sort(l.begin(), l.end());
+  out->completed = static_cast<int64_t>(l.size());
+  out->paths = sv->paths;
+  if (!l.empty()) {
+    auto q = [&](double f) {
+      const size_t i = std::min(l.size() - 1, static_cast<size_t>(std::ceil(f * l.size())) - 1);
+      return l[i];
+    };
+    out->p50_ms = q(0.50);
+    out->p99_ms = q(0.99);
+    double sum = 0;
+    for (double x : l) sum += x;
+    out->mean_ms = sum / l.size();
+    out->max_ms = l.back();
+  }
+  out->wall_s = sv->first_submit >= 0 ? sv->last_done - sv->first_submit : 0;
+  out->paths_per_s = out->wall_s > 0 ? sv->paths / out->wall_s : 0;
+  out->launches = sv->launches;
+  out->sfxt_rebuilds = sv->rebuilds;
+  out->busy_ms = sv->busy_ms;
+  out->max_batch_seen = sv->max_batch_seen;
   return CPG_OK;
 }
 

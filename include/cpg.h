@@ -229,6 +229,62 @@ cpg_status cpg_batch_get_stats(const cpg_batch* b, cpg_batch_stats* out);
  * Results are unchanged by the choice. */
 cpg_status cpg_batch_autotune(cpg_batch* b);
 
+/* ------------------------------------------------------------ served form */
+/* A C++ request loop over resident graphs.  Every graph's CSR and suffix tree
+ * stay on the device; a query may carry delay updates for its graph, after
+ * which only the affected levels of the suffix tree are rebuilt.  Queries
+ * that arrive while a launch is running are admitted into the next one as
+ * memory allows (predicted device footprint against hbm_budget_bytes), and
+ * all admitted queries run together in one persistent engine launch
+ * (continuous batching).  A query carrying updates starts a new launch, so
+ * each query sees exactly the graph state of arrival order.  Project-built
+ * form: no counterpart in the reference. */
+typedef struct cpg_server cpg_server;
+
+typedef struct {
+  int32_t max_batch;          /* queries per engine launch (1 = one at a time) */
+  int64_t hbm_budget_bytes;   /* admission budget for one launch; 0 = none */
+  int32_t reserved[6];
+} cpg_server_options;
+
+typedef struct {
+  int64_t completed;
+  int64_t paths;              /* paths returned over completed queries */
+  double p50_ms, p99_ms, mean_ms, max_ms;  /* submit -> result latency */
+  double wall_s;              /* first submit -> last completion */
+  double paths_per_s;         /* paths / wall_s */
+  int64_t launches;           /* engine launches */
+  int64_t sfxt_rebuilds;      /* incremental suffix-tree rebuilds */
+  double busy_ms;             /* device time of all launches */
+  int32_t max_batch_seen;
+  int32_t reserved;
+} cpg_server_stats;
+
+void cpg_server_options_init(cpg_server_options* o);
+cpg_status cpg_server_create(cpg_server** out, const cpg_options* opts,
+                             const cpg_server_options* sopts);
+cpg_status cpg_server_destroy(cpg_server* s);
+const char* cpg_server_last_error(const cpg_server* s);
+cpg_status cpg_server_add_graph(cpg_server* s, int32_t n, int32_t m,
+                                const int32_t* adjp, const int32_t* adjncy,
+                                const float* w, int32_t* graph_id);
+cpg_status cpg_server_add_dag(cpg_server* s, const cpg_dag* d, int32_t* graph_id);
+/* Upload the graphs, build their suffix trees, start the request loop. */
+cpg_status cpg_server_start(cpg_server* s);
+/* Queue a query: k paths of graph_id after re-sampling n_updates delays
+ * (edge ids in that graph's CSR order; may be 0).  Never blocks on the GPU. */
+cpg_status cpg_server_submit(cpg_server* s, int32_t graph_id, int64_t k,
+                             int32_t n_updates, const int32_t* eids,
+                             const float* w, int64_t* ticket);
+/* Wait (up to timeout_ms, < 0 = forever) for a ticket; copies up to cap
+ * costs.  CPG_ERR_TIMEOUT if not done in time. */
+cpg_status cpg_server_wait(cpg_server* s, int64_t ticket, float* out,
+                           int64_t cap, int64_t* n_out, double* latency_ms,
+                           int32_t timeout_ms);
+/* Finish the queued work and stop the loop. */
+cpg_status cpg_server_stop(cpg_server* s);
+cpg_status cpg_server_get_stats(const cpg_server* s, cpg_server_stats* out);
+
 /* ------------------------------------------------------------ top-K */
 /* The k smallest non-zero values of a device array of path costs, ascending,
  * written to the device buffer d_out (room for k floats); *n_out receives

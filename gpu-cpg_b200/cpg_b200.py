@@ -29,6 +29,7 @@ STATUS_NAMES = {
 DIV_REFERENCE = 0
 DIV_IEEE = 1
 FRONTIER_AUTO, FRONTIER_CSR, FRONTIER_BVSS = 0, 1, 2
+TILES_DENSITY, TILES_TENSOR, TILES_SCALAR = 0, 1, 2
 ROOTS_REFERENCE, ROOTS_ALL = 0, 1
 
 
@@ -43,7 +44,9 @@ class Options(C.Structure):
         ("device", C.c_int32), ("stream", C.c_void_p), ("division", C.c_int32),
         ("frontier", C.c_int32), ("hbm_budget_bytes", C.c_int64),
         ("spin_limit", C.c_uint32), ("root_seeding", C.c_int32),
-        ("reserved", C.c_int32 * 7),
+        ("host_stepped", C.c_int32), ("bvss_tiles", C.c_int32),
+        ("bvss_min_bits", C.c_int32), ("bvss_min_slices", C.c_int32),
+        ("reserved", C.c_int32 * 3),
     ]
 
 
@@ -69,6 +72,8 @@ class Stats(C.Structure):
         ("kernel_launches", C.c_int32), ("split", C.c_float),
         ("frontier_used", C.c_int32), ("retries", C.c_int32),
         ("engine_stage_ms", C.c_float * 8),
+        ("bvss_tiles_tensor", C.c_int64), ("bvss_tiles_scalar", C.c_int64),
+        ("bvss_bits_per_slice", C.c_double),
     ]
 
 
@@ -92,7 +97,31 @@ class ServerStats(C.Structure):
         ("p99_ms", C.c_double), ("mean_ms", C.c_double), ("max_ms", C.c_double),
         ("wall_s", C.c_double), ("paths_per_s", C.c_double), ("launches", C.c_int64),
         ("sfxt_rebuilds", C.c_int64), ("busy_ms", C.c_double), ("max_batch_seen", C.c_int32),
-        ("reserved", C.c_int32),
+        ("reserved", C.c_int32), ("sfxt_ms", C.c_double),
+    ]
+
+
+class BvssInfo(C.Structure):
+    _fields_ = [
+        ("sigma", C.c_int32), ("slices_per_thread", C.c_int32), ("slice_capacity", C.c_int32),
+        ("n_intervals", C.c_int32), ("n_vss", C.c_int32), ("n_rows", C.c_int32),
+        ("unpadded_slices", C.c_int64), ("total_set_bits", C.c_int64),
+        ("compression_ratio", C.c_double),
+    ]
+
+
+class BvssOpts(C.Structure):
+    _fields_ = [
+        ("device", C.c_int32), ("stream", C.c_void_p), ("tiles", C.c_int32),
+        ("min_bits", C.c_int32), ("min_slices", C.c_int32), ("half_slices", C.c_int32),
+        ("spin_limit", C.c_uint32), ("reserved", C.c_int32 * 3),
+    ]
+
+
+class BvssRunStats(C.Structure):
+    _fields_ = [
+        ("levels", C.c_int32), ("pad", C.c_int32), ("tiles_tensor", C.c_int64),
+        ("tiles_scalar", C.c_int64), ("mma_issued", C.c_int64), ("device_ms", C.c_double),
     ]
 
 
@@ -168,6 +197,22 @@ def _load():
                                       P(C.c_double), C.c_int32]),
         "cpg_server_stop": (C.c_int, [C.c_void_p]),
         "cpg_server_get_stats": (C.c_int, [C.c_void_p, P(ServerStats)]),
+        "cpg_bvss_opts_init": (None, [P(BvssOpts)]),
+        "cpg_bvss_build": (C.c_int, [P(C.c_void_p), C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
+        "cpg_bvss_build_compact": (C.c_int, [P(C.c_void_p), C.c_int32, C.c_void_p]),
+        "cpg_bvss_destroy": (None, [C.c_void_p]),
+        "cpg_bvss_last_error": (C.c_char_p, [C.c_void_p]),
+        "cpg_bvss_get_info": (C.c_int, [C.c_void_p, P(BvssInfo)]),
+        "cpg_bvss_get_arrays": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                          C.c_void_p, C.c_void_p]),
+        "cpg_bvss_decode_row": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32,
+                                          P(C.c_int32)]),
+        "cpg_bvss_verify": (C.c_int32, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
+        "cpg_bvss_levels": (C.c_int, [C.c_void_p, P(BvssOpts), C.c_void_p, C.c_int32, C.c_void_p,
+                                      P(BvssRunStats)]),
+        "cpg_bvss_discover_pairs": (C.c_int, [C.c_void_p, P(BvssOpts), C.c_void_p, C.c_int32,
+                                              C.c_void_p, C.c_int64, P(C.c_int64),
+                                              P(BvssRunStats)]),
         "cpg_gen_params_init": (None, [P(GenParams)]),
         "cpg_dag_generate": (C.c_int, [P(GenParams), P(C.c_void_p)]),
         "cpg_dag_sizes": (C.c_int, [C.c_void_p, P(C.c_int32), P(C.c_int32)]),
@@ -251,7 +296,9 @@ class CpGen:
     def __init__(self, device: int = 0, stream: int | None = None,
                  division: int = DIV_REFERENCE, frontier: int = FRONTIER_AUTO,
                  hbm_budget_bytes: int = 0, spin_limit: int = 0,
-                 root_seeding: int = ROOTS_REFERENCE, host_stepped: bool = False):
+                 root_seeding: int = ROOTS_REFERENCE, host_stepped: bool = False,
+                 bvss_tiles: int = TILES_DENSITY, bvss_min_bits: int = 0,
+                 bvss_min_slices: int = 0):
         o = Options()
         lib.cpg_options_init(C.byref(o))
         o.device = device
@@ -261,7 +308,10 @@ class CpGen:
         o.hbm_budget_bytes = hbm_budget_bytes
         o.spin_limit = spin_limit
         o.root_seeding = root_seeding
-        o.reserved[0] = 1 if host_stepped else 0
+        o.host_stepped = 1 if host_stepped else 0
+        o.bvss_tiles = bvss_tiles
+        o.bvss_min_bits = bvss_min_bits
+        o.bvss_min_slices = bvss_min_slices
         self._h = C.c_void_p()
         st = lib.cpg_create(C.byref(self._h), C.byref(o))
         if st != CPG_OK:
@@ -560,6 +610,112 @@ class Server:
         s = ServerStats()
         self._check(lib.cpg_server_get_stats(self._s, C.byref(s)), "stats")
         return {f: getattr(s, f) for f, _ in ServerStats._fields_ if f != "reserved"}
+
+
+class Bvss:
+    """A BVSS (sigma = 8) of a row -> column CSR: the fan-out form, or with
+    ``succs`` the transposed deviation matrix A_dev (see cpg_bvss_build)."""
+
+    def __init__(self, n: int, row_ptr, col_idx, succs=None, *, compact_offsets=None):
+        self._b = C.c_void_p()
+        if compact_offsets is not None:
+            off = np.ascontiguousarray(compact_offsets, np.int32)
+            st = lib.cpg_bvss_build_compact(C.byref(self._b), int(n), _ptr(off))
+        else:
+            rp = np.ascontiguousarray(row_ptr, np.int32)
+            ci = np.ascontiguousarray(col_idx, np.int32)
+            sc = None if succs is None else np.ascontiguousarray(succs, np.int32)
+            st = lib.cpg_bvss_build(C.byref(self._b), int(n), _ptr(rp), _ptr(ci), _ptr(sc))
+        if st != CPG_OK:
+            raise CpgError(st, "cpg_bvss_build failed")
+
+    def close(self):
+        if self._b:
+            lib.cpg_bvss_destroy(self._b)
+            self._b = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st: int, what: str):
+        if st != CPG_OK:
+            msg = lib.cpg_bvss_last_error(self._b)
+            raise CpgError(st, f"{what}: {msg.decode() if msg else ''}")
+
+    def info(self) -> dict:
+        i = BvssInfo()
+        self._check(lib.cpg_bvss_get_info(self._b, C.byref(i)), "info")
+        return {f: getattr(i, f) for f, _ in BvssInfo._fields_}
+
+    def arrays(self) -> dict:
+        i = self.info()
+        nv, ni = i["n_vss"], i["n_intervals"]
+        out = {
+            "real_ptrs": np.zeros(ni + 1, np.int32),
+            "virtual_to_real": np.zeros(nv, np.int32),
+            "slice_counts": np.zeros(nv, np.uint8),
+            "row_ids": np.zeros(128 * nv, np.int32),
+            "masks": np.zeros(32 * nv, np.uint32),
+        }
+        self._check(lib.cpg_bvss_get_arrays(self._b, *(_ptr(out[k]) for k in
+                    ("real_ptrs", "virtual_to_real", "slice_counts", "row_ids", "masks"))),
+                    "arrays")
+        return out
+
+    def decode_row(self, row: int) -> list[int]:
+        n = C.c_int32()
+        buf = np.zeros(1 << 16, np.int32)
+        self._check(lib.cpg_bvss_decode_row(self._b, int(row), _ptr(buf), buf.size, C.byref(n)),
+                    "decode_row")
+        return buf[: n.value].tolist()
+
+    def verify(self, n: int, row_ptr, col_idx, succs=None) -> bool:
+        rp = np.ascontiguousarray(row_ptr, np.int32)
+        ci = np.ascontiguousarray(col_idx, np.int32)
+        sc = None if succs is None else np.ascontiguousarray(succs, np.int32)
+        r = lib.cpg_bvss_verify(self._b, int(n), _ptr(rp), _ptr(ci), _ptr(sc))
+        if r < 0:
+            raise CpgError(1, "cpg_bvss_verify: invalid input")
+        return bool(r)
+
+    @staticmethod
+    def _opts(device, tiles, min_bits, min_slices, half_slices, stream):
+        o = BvssOpts()
+        lib.cpg_bvss_opts_init(C.byref(o))
+        o.device, o.tiles, o.min_bits = device, tiles, min_bits
+        o.min_slices, o.half_slices, o.stream = min_slices, half_slices, stream
+        return o
+
+    def levels(self, sinks=None, *, device: int = 0, tiles: int = TILES_DENSITY,
+               min_bits: int = 0, min_slices: int = 0, half_slices: int = 0,
+               stream: int | None = None):
+        """(levels int32[n_rows], run stats dict)."""
+        o = self._opts(device, tiles, min_bits, min_slices, half_slices, stream)
+        lv = np.zeros(self.info()["n_rows"], np.int32)
+        sk = None if sinks is None else np.ascontiguousarray(sinks, np.int32)
+        rs = BvssRunStats()
+        self._check(lib.cpg_bvss_levels(self._b, C.byref(o), _ptr(sk),
+                                        0 if sk is None else int(sk.size), _ptr(lv),
+                                        C.byref(rs)), "levels")
+        return lv, {f: getattr(rs, f) for f, _ in BvssRunStats._fields_ if f != "pad"}
+
+    def discover_pairs(self, sources, max_pairs: int = 1 << 20, *, device: int = 0,
+                       tiles: int = TILES_DENSITY, min_bits: int = 0, min_slices: int = 0,
+                       half_slices: int = 0, stream: int | None = None):
+        """(sorted (u, v) pairs as int32[P, 2], run stats dict)."""
+        o = self._opts(device, tiles, min_bits, min_slices, half_slices, stream)
+        src = np.ascontiguousarray(sources, np.int32)
+        buf = np.zeros(2 * max(int(max_pairs), 1), np.int32)
+        n = C.c_int64()
+        rs = BvssRunStats()
+        self._check(lib.cpg_bvss_discover_pairs(self._b, C.byref(o), _ptr(src), int(src.size),
+                                                _ptr(buf), int(max_pairs), C.byref(n),
+                                                C.byref(rs)), "discover_pairs")
+        return buf[: 2 * n.value].reshape(-1, 2), {f: getattr(rs, f) for f, _ in
+                                                   BvssRunStats._fields_ if f != "pad"}
 
 
 def select_topk(d_costs: int, n: int, k: int, d_out: int, stream: int | None = None) -> int:

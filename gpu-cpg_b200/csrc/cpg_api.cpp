@@ -55,6 +55,10 @@ struct cpg_handle {
   int32_t big_rows = 0, big_cap = 1;
   DevMem d_adjp, d_edges, d_iadjp, d_iadj, d_srcs, d_big_off, d_big_tmp,
       d_big_rows;
+  // BVSS form of the fan-out CSR, for the pull Kahn step
+  bool use_bvss = false;
+  double bvss_bps = 0;  // set bits per slice (sampled, or exact once built)
+  DevMem d_bv_ptr, d_bv_masks, d_bv_rows, d_bv_cnt, d_bv_deps, d_fbits, d_iact, d_act_list;
 
   // suffix tree
   bool sfxt_valid = false;
@@ -137,6 +141,50 @@ Status check_handle(cpg_handle* h) {
   return CPG_OK;
 }
 
+// Density at which the BVSS pull takes over the Kahn step: with b set bits
+// per slice the pull issues one atomic per slice where the CSR push issues
+// one per edge, so it pays from about two heads per interval on.
+constexpr double kBvssAutoBits = 2.0;
+
+// Frontier choice for the Kahn step, and the BVSS build when it is used.
+Status setup_bvss(cpg_handle* h, int32_t n, const int32_t* adjp, const int32_t* adj) {
+  h->use_bvss = false;
+  const int32_t mode = h->opts.frontier;
+  if (mode == CPG_FRONTIER_CSR || n == 0) {
+    h->bvss_bps = 0;
+    return CPG_OK;
+  }
+  if (mode == CPG_FRONTIER_AUTO) {
+    h->bvss_bps = bvss_density_sample(n, adjp, adj, 4096);
+    if (h->bvss_bps < kBvssAutoBits) return CPG_OK;
+  }
+  HostBvss b;
+  Status st = pack_bvss(n, adjp, adj, b, h->err);
+  if (st != CPG_OK) return st;
+  h->bvss_bps = b.unpadded_slices ? static_cast<double>(b.total_set_bits) /
+                                        static_cast<double>(b.unpadded_slices)
+                                  : 0.0;
+  const size_t fw = (static_cast<size_t>(n) + 31) / 32;
+  const size_t iw = (static_cast<size_t>(b.n_intervals) + 31) / 32;
+  CK(ensure(h->d_bv_ptr, b.ptr.size() * 4), "alloc BVSS");
+  CK(ensure(h->d_bv_masks, std::max<size_t>(b.masks.size(), 1) * 4), "alloc BVSS");
+  CK(ensure(h->d_bv_rows, std::max<size_t>(b.rows.size(), 1) * 4), "alloc BVSS");
+  CK(ensure(h->d_bv_cnt, std::max<size_t>(b.cnt.size(), 1)), "alloc BVSS");
+  CK(ensure(h->d_bv_deps, b.row_bits.size() * 4), "alloc BVSS");
+  CK(ensure(h->d_fbits, 2 * fw * 4), "alloc BVSS");
+  CK(ensure(h->d_iact, 2 * iw * 4), "alloc BVSS");
+  CK(ensure(h->d_act_list, static_cast<size_t>(n) * 4 + 4), "alloc BVSS");
+  CK(cudaMemcpy(h->d_bv_ptr.p, b.ptr.data(), b.ptr.size() * 4, cudaMemcpyHostToDevice), "H2D BVSS");
+  if (b.n_vss) {
+    CK(cudaMemcpy(h->d_bv_masks.p, b.masks.data(), b.masks.size() * 4, cudaMemcpyHostToDevice), "H2D BVSS");
+    CK(cudaMemcpy(h->d_bv_rows.p, b.rows.data(), b.rows.size() * 4, cudaMemcpyHostToDevice), "H2D BVSS");
+    CK(cudaMemcpy(h->d_bv_cnt.p, b.cnt.data(), b.cnt.size(), cudaMemcpyHostToDevice), "H2D BVSS");
+  }
+  CK(cudaMemcpy(h->d_bv_deps.p, b.row_bits.data(), b.row_bits.size() * 4, cudaMemcpyHostToDevice), "H2D BVSS");
+  h->use_bvss = true;
+  return CPG_OK;
+}
+
 // Upload a fan-out CSR and build the rest of the graph on the device: edge
 // words, fan-in CSR and source list.  The host keeps only the row offsets.
 Status upload_graph(cpg_handle* h, int32_t n, int32_t m, const int32_t* adjp,
@@ -158,6 +206,10 @@ Status upload_graph(cpg_handle* h, int32_t n, int32_t m, const int32_t* adjp,
   if (max_deg > kMaxRow)
     return fail(h, CPG_ERR_INVALID, "out-degree above 16384 is not supported");
   h->has_graph = false;
+  {
+    Status st = setup_bvss(h, n, adjp, adj);
+    if (st != CPG_OK) return st;
+  }
   h->g.n = n;
   h->g.m = m;
   h->g.adjp.assign(adjp, adjp + n + 1);
@@ -282,6 +334,20 @@ SfxtParams sfxt_params(cpg_handle* h, int32_t start_level) {
   p.known_levels = h->levels;
   p.spin_limit = h->opts.spin_limit ? h->opts.spin_limit : kDefaultSpinLimit;
   p.grid_limit = h->sfxt_grid_limit;
+  if (h->use_bvss) {
+    p.bvss = 1;
+    p.bv_ptr = P<int32_t>(h->d_bv_ptr);
+    p.bv_masks = P<unsigned int>(h->d_bv_masks);
+    p.bv_rows = P<int32_t>(h->d_bv_rows);
+    p.bv_cnt = P<uint8_t>(h->d_bv_cnt);
+    p.bv_deps = P<int32_t>(h->d_bv_deps);
+    p.fbits = P<unsigned int>(h->d_fbits);
+    p.iact = P<unsigned int>(h->d_iact);
+    p.act_list = P<int32_t>(h->d_act_list);
+    p.mma_mode = h->opts.bvss_tiles;
+    p.mma_min_bits = h->opts.bvss_min_bits > 0 ? h->opts.bvss_min_bits : 2;
+    p.mma_min_slices = h->opts.bvss_min_slices > 0 ? h->opts.bvss_min_slices : 32;
+  }
   return p;
 }
 
@@ -290,6 +356,11 @@ Status enqueue_sfxt(cpg_handle* h, int32_t start_level, int* launches) {
   cudaStream_t s = h->stream;
   CK(launch_init_sfxt_counters(P<SfxtCounters>(h->d_sctr), P<unsigned long long>(h->d_pool_mark),
                                start_level, s), "sfxt counters");
+  if (h->use_bvss && start_level == 0) {
+    // the pull leaves the bitmaps clear; a build cut short by an error may not
+    CK(cudaMemsetAsync(h->d_fbits.p, 0, h->d_fbits.bytes, s), "memset");
+    CK(cudaMemsetAsync(h->d_iact.p, 0, h->d_iact.bytes, s), "memset");
+  }
   int grid = 0;
   CK(launch_sfxt(sfxt_params(h, start_level), h->device, s, &grid, launches), "sfxt launch");
   *launches += 1;
@@ -310,7 +381,12 @@ int finish_sfxt(cpg_handle* h, int32_t start_level) {
     h->h_levels_cached = false;
   }
   h->stats.levels = h->levels;
-  h->stats.frontier_used = CPG_FRONTIER_CSR;
+  if (start_level == 0) {
+    h->stats.frontier_used = h->use_bvss ? CPG_FRONTIER_BVSS : CPG_FRONTIER_CSR;
+    h->stats.bvss_tiles_tensor = static_cast<int64_t>(out->vss_tensor);
+    h->stats.bvss_tiles_scalar = static_cast<int64_t>(out->vss_scalar);
+  }
+  h->stats.bvss_bits_per_slice = h->bvss_bps;
   h->sfxt_valid = true;
   h->h_sfxt_cached = false;
   h->dirty_level = -1;
@@ -890,7 +966,9 @@ cpg_status cpg_destroy(cpg_handle* h) {
                    &h->d_pctr, &h->d_selstate, &h->d_selhist, &h->d_counts,
                    &h->d_keys, &h->d_vals, &h->d_sorthist, &h->d_cnt,
                    &h->d_rank, &h->d_out_cost, &h->d_out_nodes, &h->d_pq,
-                   &h->d_qids, &h->d_ehist, &h->d_esort, &h->d_equery, &h->d_ectr};
+                   &h->d_qids, &h->d_ehist, &h->d_esort, &h->d_equery, &h->d_ectr,
+                   &h->d_bv_ptr, &h->d_bv_masks, &h->d_bv_rows, &h->d_bv_cnt,
+                   &h->d_bv_deps, &h->d_fbits, &h->d_iact, &h->d_act_list};
   for (DevMem* b : all) release(*b);
   for (auto& e : h->ev)
     if (e) cudaEventDestroy(e);
@@ -1046,7 +1124,7 @@ cpg_status cpg_report_paths(cpg_handle* h, int64_t k) {
   h->cap_paths = std::max(h->cap_paths, std::max<unsigned long long>(4 * uk, 1 << 16) + nsrc);
   h->cap_front = std::max(h->cap_front, std::max<unsigned long long>(2 * uk, 1 << 16));
   h->cap_pend = std::max(h->cap_pend, std::max<unsigned long long>(8 * uk, 1 << 17) + nsrc);
-  const bool host_stepped = h->opts.reserved[0] == 1;
+  const bool host_stepped = h->opts.host_stepped == 1;
   for (int attempt = 0; attempt < 10; ++attempt) {
     const int r = host_stepped ? try_query(h, uk) : engine_query(h, uk);
     if (r == kRetry) {
@@ -1608,7 +1686,7 @@ struct cpg_server {
   // statistics
   std::vector<double> lat_ms;
   int64_t paths = 0, launches = 0, rebuilds = 0;
-  double busy_ms = 0, first_submit = -1, last_done = 0;
+  double busy_ms = 0, sfxt_ms = 0, first_submit = -1, last_done = 0;
   int32_t max_batch_seen = 0;
 };
 
@@ -1668,29 +1746,36 @@ void server_loop(cpg_server* sv) {
       sv->cv_work.wait(lk, [&] { return sv->stopping || !sv->queue.empty(); });
       if (sv->queue.empty()) break;  // stopping and drained
       // admit in arrival order: up to max_batch queries whose predicted
-      // footprint fits the budget; a query that updates delays starts a new
-      // launch so every query sees arrival-order graph state
+      // footprint fits the budget.  Delay updates are applied before the
+      // launch, so an update may join only if no query already admitted
+      // reads the same graph: every query then sees arrival-order state.
       int64_t used = 0;
+      std::vector<char> graph_read;
       while (!sv->queue.empty() &&
              static_cast<int32_t>(batch.size()) < std::max(1, sv->so.max_batch)) {
         ServerReq& r = sv->queue.front();
-        if (!batch.empty() && !r.eids.empty()) break;
+        if (graph_read.size() <= static_cast<size_t>(r.graph)) graph_read.resize(r.graph + 1, 0);
+        if (!batch.empty() && !r.eids.empty() && graph_read[r.graph]) break;
         const int64_t need = predicted_bytes(r.k);
         if (!batch.empty() && sv->so.hbm_budget_bytes > 0 && used + need > sv->so.hbm_budget_bytes)
           break;
         used += need;
+        graph_read[r.graph] = 1;
         batch.push_back(std::move(r));
         sv->queue.pop_front();
       }
     }
     Status st = CPG_OK;
-    if (!batch[0].eids.empty()) {
-      st = cpg_update_delays(h, static_cast<int64_t>(batch[0].eids.size()), batch[0].eids.data(),
-                             batch[0].w.data());
-      if (st == CPG_OK) {
-        st = ensure_sfxt(h);  // incremental: levels at or above the change
-        sv->rebuilds += 1;
-      }
+    bool updated = false;
+    for (const ServerReq& r : batch) {
+      if (r.eids.empty() || st != CPG_OK) continue;
+      st = cpg_update_delays(h, static_cast<int64_t>(r.eids.size()), r.eids.data(), r.w.data());
+      updated = true;
+    }
+    if (st == CPG_OK && updated) {
+      st = ensure_sfxt(h);  // incremental: levels at or above the lowest change
+      sv->rebuilds += 1;
+      sv->sfxt_ms += h->stats.sfxt_ms;
     }
     std::vector<std::vector<float>> out;
     for (int attempt = 0; st == CPG_OK && attempt < 10; ++attempt) {
@@ -1883,6 +1968,7 @@ cpg_status cpg_server_get_stats(const cpg_server* svc, cpg_server_stats* out) {
   out->sfxt_rebuilds = sv->rebuilds;
   out->busy_ms = sv->busy_ms;
   out->max_batch_seen = sv->max_batch_seen;
+  out->sfxt_ms = sv->sfxt_ms;
   return CPG_OK;
 }
 

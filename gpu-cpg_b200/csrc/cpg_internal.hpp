@@ -93,12 +93,16 @@ enum DevErr : int {
 
 struct SfxtCounters {
   int tail;                  // order[] append cursor
+  int act_n;                 // BVSS: act_list append cursor
+  int level_end;             // tail and act_n snapshots taken at each level
+  int act_end;               // barrier (adjacent: one two-word snapshot)
   int err;
   int levels;
-  int level_end;             // tail snapshot taken at each level barrier
   int sort_beg;              // order[] range whose deviation rows were rebuilt
   int sort_end;
   unsigned long long hnode_used;
+  unsigned long long vss_tensor;  // BVSS tiles counted on the tensor cores
+  unsigned long long vss_scalar;  // ... and with scalar popc
   GridBarrier bar;
 };
 
@@ -131,7 +135,89 @@ struct SfxtParams {
   int32_t known_levels;    // level count when start_level > 0
   unsigned int spin_limit;
   int32_t grid_limit;      // persistent CTAs (0: one per co-resident slot)
+  // BVSS pull for the Kahn step of a full build; used when bvss != 0
+  int32_t bvss;
+  const int32_t* bv_ptr;       // VSS range of each interval of 8 vertices
+  const unsigned int* bv_masks;
+  const int32_t* bv_rows;
+  const uint8_t* bv_cnt;       // slices in each VSS
+  const int32_t* bv_deps;      // distinct fan-out heads of each vertex
+  unsigned int* fbits;         // frontier bitmap (n bits)
+  unsigned int* iact;          // active-interval bitmap
+  int32_t* act_list;           // active intervals, appended level after level
+  int32_t mma_min_bits;        // density test of a tile, as BvssDispatch
+  int32_t mma_min_slices;
+  int32_t mma_mode;
 };
+
+// BVSS (bit-vector slice sets, sigma = 8) of a row -> column relation.
+// Columns are grouped into intervals of 8; each row with columns in an
+// interval contributes one slice (row, 8-bit mask).  An interval's slices, in
+// row order, are packed 128 to a VSS: slice i of a VSS sits in lane i % 32,
+// chunk i / 32, i.e. bits 8*chunk.. of masks[vss*32 + lane] and
+// rows[vss*128 + lane*4 + chunk] (-1 pads).  The layout and the slice order
+// are the reference's (gpucpg/tc_sfxt_bvss.cuh:17-31, 73-156).
+struct HostBvss {
+  int32_t n_rows = 0;              // vertex count of the graph
+  int32_t n_intervals = 0, n_vss = 0;
+  uint64_t unpadded_slices = 0, total_set_bits = 0;
+  std::vector<int32_t> ptr;        // VSS range of each interval (n_intervals + 1)
+  std::vector<int32_t> v2r;        // interval of each VSS
+  std::vector<uint8_t> cnt;        // slices in each VSS
+  std::vector<int32_t> rows;       // 128 per VSS
+  std::vector<uint32_t> masks;     // 32 per VSS
+  std::vector<int32_t> row_bits;   // distinct columns of each row
+};
+// Packs row -> columns given as a CSR over n rows with columns in [0, n).
+Status pack_bvss(int32_t n, const int32_t* row_ptr, const int32_t* cols, HostBvss& out,
+                 std::string& err);
+// Packs one slice per (deviation, source) pair of a compact deviation CSR:
+// row = deviation index, column = its source vertex
+// (tc_pfxt_bvss.cuh:177-226).
+Status pack_bvss_compact(int32_t n, const int32_t* dev_off, HostBvss& out, std::string& err);
+// Sorted columns of one row, decoded from the packed form.
+std::vector<int32_t> bvss_decode_row(const HostBvss& b, int32_t row);
+// Average set bits per slice over the first `rows` rows of a CSR (the density
+// test for the suffix tree's frontier choice).
+double bvss_density_sample(int32_t n, const int32_t* row_ptr, const int32_t* cols,
+                           int32_t rows);
+
+// Device BVSS arrays.
+struct DevBvss {
+  int32_t n_rows, n_intervals, n_vss;
+  const int32_t* ptr;
+  const int32_t* v2r;
+  const uint8_t* cnt;
+  const int32_t* rows;
+  const unsigned int* masks;
+};
+struct BvssDispatch {
+  int32_t mode;            // 0 density test, 1 tensor cores always, 2 scalar always
+  int32_t min_bits;        // density test: frontier byte has >= min_bits bits
+  int32_t min_slices;      // ... and the VSS holds > min_slices slices
+  int32_t half_slices;     // skip the upper-half MMA when slices <= this
+};
+struct BvssCounters {
+  int err;
+  int level;
+  int qn[3];               // rotating queue sizes
+  int pad;
+  unsigned long long tiles_tensor, tiles_scalar, mma_issued;
+  unsigned long long pairs;
+  GridBarrier bar;
+};
+// Pull BFS levels from the sinks (min hops over fan-out edges), one
+// persistent launch.  scratch: 3 frontier bitmaps + 3 queued-interval
+// bitmaps + visited bitmap + 3 VSS queues (bvss_levels_scratch_words).
+size_t bvss_levels_scratch_words(int32_t n, int32_t n_intervals, int32_t n_vss);
+int launch_bvss_levels(const DevBvss& b, const int32_t* sinks, int32_t n_sinks,
+                       int32_t* levels, unsigned int* scratch, BvssCounters* ctr,
+                       BvssDispatch d, unsigned int spin_limit, int device, void* stream);
+// Pairs (source u in the frontier, row v) of an A_dev BVSS.
+size_t bvss_pairs_scratch_words(int32_t n_intervals, int32_t n_vss);
+int launch_bvss_pairs(const DevBvss& b, const int32_t* sources, int32_t n_sources,
+                      int32_t* pairs, long long max_pairs, unsigned int* scratch,
+                      BvssCounters* ctr, BvssDispatch d, void* stream);
 
 constexpr int kSfxtThreads = 1024;  // one block per SM: fewer grid-barrier arrivals
 constexpr int kSmemRow = 256;  // deviation rows up to this length sort in smem

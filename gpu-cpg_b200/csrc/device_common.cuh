@@ -19,14 +19,14 @@ __device__ __forceinline__ unsigned lanemask_lt() {
 // leaves the barrier, so a lost block can never hang the GPU.  Returns false
 // once any block has recorded an error.
 //
-// If snap_src is given, the last block to arrive copies *snap_src to
-// *snap_dst before releasing the others: a counter that blocks keep
+// If snap_src is given, the last block to arrive copies snap_src[0..snap_n)
+// to snap_dst before releasing the others: a counter that blocks keep
 // appending to after the barrier (a queue tail) can then be read as one
 // agreed value by every block.
 __device__ __forceinline__ bool grid_sync(GridBarrier* b, int* err,
                                           unsigned int limit,
                                           const int* snap_src = nullptr,
-                                          int* snap_dst = nullptr) {
+                                          int* snap_dst = nullptr, int snap_n = 1) {
   __syncthreads();
   if (threadIdx.x == 0) {
     volatile unsigned int* vgen = &b->gen;
@@ -34,8 +34,10 @@ __device__ __forceinline__ bool grid_sync(GridBarrier* b, int* err,
     __threadfence();
     const unsigned int arrived = atomicAdd(&b->count, 1u);
     if (arrived == gridDim.x - 1) {
-      if (snap_src) *reinterpret_cast<volatile int*>(snap_dst) =
-          *reinterpret_cast<const volatile int*>(snap_src);
+      if (snap_src)
+        for (int i = 0; i < snap_n; ++i)
+          reinterpret_cast<volatile int*>(snap_dst)[i] =
+              reinterpret_cast<const volatile int*>(snap_src)[i];
       atomicExch(&b->count, 0u);
       __threadfence();
       atomicAdd(&b->gen, 1u);

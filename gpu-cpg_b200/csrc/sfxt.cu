@@ -15,6 +15,7 @@
 // This file is compiled with --use_fast_math like the reference library.
 #include <climits>
 
+#include "bvss.cuh"
 #include "device_common.cuh"
 
 namespace cpg {
@@ -244,6 +245,66 @@ __device__ void heap_insert(const SfxtParams& p, int v) {
   p.ht_size[v] = static_cast<int>(pos);
 }
 
+// BVSS form of the Kahn step.  A vertex that joins level L sets its bit in
+// the level-parity frontier bitmap fbits[L & 1] and, first in its interval of
+// 8, appends the interval to act_list.  Pulling level L, one warp per active
+// interval counts for every slice (row u, mask of u's heads in the interval)
+// how many heads just finished, popc(mask & frontier byte) -- on the tensor
+// cores where the density test passes -- and takes that many off deps[u],
+// which starts at u's number of distinct heads.  The warp then clears the
+// interval's byte and bit so the bitmaps are clean for level L + 2.
+__device__ __forceinline__ void bvss_mark(const SfxtParams& p, int parity, int u) {
+  const size_t fw = (static_cast<size_t>(p.n) + 31) / 32;
+  const size_t iw = ((static_cast<size_t>(p.n) + 7) / 8 + 31) / 32;
+  atomicOr(p.fbits + parity * fw + (u >> 5), 1u << (u & 31));
+  const int iv = u >> 3;
+  const unsigned bit = 1u << (iv & 31);
+  if (!(atomicOr(p.iact + parity * iw + (iv >> 5), bit) & bit))
+    p.act_list[atomicAdd(&p.ctr->act_n, 1)] = iv;
+}
+
+__device__ void bvss_pull_interval(const SfxtParams& p, int iv, int lvl,
+                                   unsigned long long& n_tensor, unsigned long long& n_scalar) {
+  const int lane = threadIdx.x & 31;
+  const size_t fw = (static_cast<size_t>(p.n) + 31) / 32;
+  const size_t iw = ((static_cast<size_t>(p.n) + 7) / 8 + 31) / 32;
+  unsigned int* fr = p.fbits + (lvl & 1) * fw;
+  const unsigned fb = frontier_byte(fr, iv);
+  for (int vss = p.bv_ptr[iv]; vss < p.bv_ptr[iv + 1]; ++vss) {
+    const unsigned mask = p.bv_masks[static_cast<size_t>(vss) * 32 + lane];
+    const int4 rw = reinterpret_cast<const int4*>(p.bv_rows)[static_cast<size_t>(vss) * 32 + lane];
+    const int slices = p.bv_cnt[vss];
+    const bool tensor = bvss_use_tensor(p.mma_mode, fb, slices, p.mma_min_bits, p.mma_min_slices);
+    unsigned c[4];
+    bvss_counts(mask, fb, tensor, slices > 64, c);
+    n_tensor += tensor;
+    n_scalar += !tensor;
+    const int row[4] = {rw.x, rw.y, rw.z, rw.w};
+    bool ready[4];
+#pragma unroll
+    for (int ch = 0; ch < 4; ++ch) {
+      const int cnt = static_cast<int>(c[ch]);
+      ready[ch] = cnt > 0 && row[ch] >= 0 && atomicSub(&p.deps[row[ch]], cnt) == cnt;
+    }
+#pragma unroll
+    for (int ch = 0; ch < 4; ++ch) {
+      const int slot = warp_append(&p.ctr->tail, ready[ch]);
+      if (ready[ch]) {
+        p.order[slot] = row[ch];
+        p.level_of[row[ch]] = lvl + 1;
+        bvss_mark(p, (lvl + 1) & 1, row[ch]);
+      }
+    }
+  }
+  if (lane == 0) {
+    atomicAnd(fr + (iv >> 2), ~(0xffu << ((iv & 3) * 8)));
+    atomicAnd(p.iact + (lvl & 1) * iw + (iv >> 5), ~(1u << (iv & 31)));
+  }
+}
+
+// kBvss: the Kahn step pulls over the BVSS form (full builds only); a
+// separate instantiation keeps the CSR build's registers unchanged.
+template <bool kBvss>
 __global__ void __launch_bounds__(kSfxtThreads)
 sfxt_persistent_kernel(SfxtParams p) {
   const int warp_in_block = threadIdx.x >> 5;
@@ -262,7 +323,7 @@ sfxt_persistent_kernel(SfxtParams p) {
       bool sink = false;
       if (v < p.n) {
         const int od = p.adjp[v + 1] - p.adjp[v];
-        p.deps[v] = od;
+        p.deps[v] = kBvss ? p.bv_deps[v] : od;
         p.dist[v] = INT_MAX;
         p.succ[v] = -1;
         p.dev_cnt[v] = 0;
@@ -272,10 +333,13 @@ sfxt_persistent_kernel(SfxtParams p) {
         sink = od == 0;
       }
       const int slot = warp_append(&p.ctr->tail, sink);
-      if (sink) p.order[slot] = v;
+      if (sink) {
+        p.order[slot] = v;
+        if (kBvss) bvss_mark(p, 0, v);
+      }
     }
     if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit, &p.ctr->tail,
-                   &p.ctr->level_end))
+                   &p.ctr->level_end, 2))
       return;
     beg = 0;
     end = *reinterpret_cast<volatile int*>(&p.ctr->level_end);
@@ -291,6 +355,10 @@ sfxt_persistent_kernel(SfxtParams p) {
   int pend = beg;
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   const int nth = gridDim.x * blockDim.x;
+  const bool pull = kBvss && full;
+  int abeg = 0;            // act_list range of the level being pulled
+  int aend = pull ? *reinterpret_cast<volatile int*>(&p.ctr->act_end) : 0;
+  unsigned long long n_tensor = 0, n_scalar = 0;
   while (beg < end) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       p.lvlp[lvl] = beg;
@@ -301,18 +369,23 @@ sfxt_persistent_kernel(SfxtParams p) {
         p.pool_mark[lvl - 1] = *reinterpret_cast<volatile unsigned long long*>(&p.ctr->hnode_used);
     }
     for (int i = beg + gwarp; i < end; i += nwarps) {
-      build_vertex(p, __ldcg(p.order + i), lvl, full);
+      build_vertex(p, __ldcg(p.order + i), lvl, full && !kBvss);
     }
+    if (kBvss && pull)
+      for (int i = abeg + gwarp; i < aend; i += nwarps)
+        bvss_pull_interval(p, __ldcg(p.act_list + i), lvl, n_tensor, n_scalar);
     for (int i = pbeg + tid; i < pend; i += nth) heap_insert(p, __ldcg(p.order + i));
     // the tail keeps growing as soon as the next level starts appending, so
     // the level bound is the snapshot the last arriving block took
     if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit, &p.ctr->tail,
-                   &p.ctr->level_end))
+                   &p.ctr->level_end, 2))
       return;
     ++lvl;
     pbeg = beg;
     pend = end;
     beg = end;
+    abeg = aend;
+    if (pull) aend = *reinterpret_cast<volatile int*>(&p.ctr->act_end);
     if (full) {
       end = *reinterpret_cast<volatile int*>(&p.ctr->level_end);
     } else {
@@ -327,6 +400,10 @@ sfxt_persistent_kernel(SfxtParams p) {
     p.ctr->levels = lvl;
     p.lvlp[lvl] = beg;
     p.ctr->sort_end = beg;
+  }
+  if (kBvss && (threadIdx.x & 31) == 0 && (n_tensor | n_scalar)) {
+    atomicAdd(&p.ctr->vss_tensor, n_tensor);
+    atomicAdd(&p.ctr->vss_scalar, n_scalar);
   }
 }
 
@@ -467,8 +544,11 @@ int launch_sfxt(const SfxtParams& p, int device, void* stream, int* grid_out,
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   if (e != cudaSuccess) return e;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sfxt_persistent_kernel,
-                                                    kSfxtThreads, 0);
+  // the BVSS pull only serves full builds; incremental ones take the CSR kernel
+  const bool bvss = p.bvss && p.start_level == 0;
+  void* kern = bvss ? reinterpret_cast<void*>(sfxt_persistent_kernel<true>)
+                    : reinterpret_cast<void*>(sfxt_persistent_kernel<false>);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kSfxtThreads, 0);
   if (e != cudaSuccess) return e;
   if (per_sm < 1) per_sm = 1;
   int grid = sms * per_sm;
@@ -476,8 +556,7 @@ int launch_sfxt(const SfxtParams& p, int device, void* stream, int* grid_out,
   if (grid_out) *grid_out = grid;
   SfxtParams pp = p;
   void* args[] = {&pp};
-  e = cudaLaunchCooperativeKernel(reinterpret_cast<void*>(sfxt_persistent_kernel),
-                                  dim3(grid), dim3(kSfxtThreads), args, 0, st);
+  e = cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kSfxtThreads), args, 0, st);
   if (e != cudaSuccess) return e;
   sort_rows_kernel<<<sms * 8, kSortWarps * 32, 0, st>>>(
       p.order, &p.ctr->sort_beg, p.adjp, p.dev_cnt, p.dev);

@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define CPG_ABI_VERSION 1
+#define CPG_ABI_VERSION 2
 
 /* Replaces exit(1) in cudaCheckErrors / checkError_t (gpucpg.cu:87-98,
  * 269-275) and the std::runtime_error throws of read_input (gpucpg.cu:457). */
@@ -55,6 +55,15 @@ typedef enum {
   CPG_FRONTIER_BVSS = 2
 } cpg_frontier;
 
+/* Which BVSS tiles go to the tensor cores (b1 AND-popc MMA).  DENSITY: a tile
+ * whose frontier byte has at least min_bits bits and whose VSS holds more than
+ * min_slices slices; the rest use scalar popc.  Both give identical counts. */
+typedef enum {
+  CPG_BVSS_TILES_DENSITY = 0,
+  CPG_BVSS_TILES_TENSOR = 1,
+  CPG_BVSS_TILES_SCALAR = 2
+} cpg_bvss_tiles;
+
 /* Root seeding.  REFERENCE reproduces G-PathGen's initial split
  * (gpucpg.cu:19136-19179): with R reachable sources, the split is the cost at
  * sorted index (size_t)(0.005f*R) and only the first (int)(0.005f*R+1) roots
@@ -72,9 +81,14 @@ typedef struct {
   int64_t hbm_budget_bytes; /* cap on per-query device memory; 0 = none */
   uint32_t spin_limit;      /* grid-barrier poll limit; 0 = default */
   int32_t root_seeding;     /* cpg_root_seeding */
-  int32_t reserved[7];      /* [0] = 1: step the split raises from the host
-                               (one kernel sequence per raise) instead of the
+  int32_t host_stepped;     /* 1: step the split raises from the host (one
+                               kernel sequence per raise) instead of the
                                persistent device engine; for A/B checks */
+  int32_t bvss_tiles;       /* cpg_bvss_tiles for the BVSS frontier */
+  int32_t bvss_min_bits;    /* density test: frontier bits in the tile's byte
+                               (0 = default 2) */
+  int32_t bvss_min_slices;  /* density test: slices in the VSS (0 = default 32) */
+  int32_t reserved[3];
 } cpg_options;
 
 typedef struct cpg_handle cpg_handle;
@@ -110,6 +124,9 @@ typedef struct {
   /* device time of the query engine by stage (ms): seed, decide, select,
    * promote, closure, output select, output sort, emit */
   float engine_stage_ms[8];
+  int64_t bvss_tiles_tensor; /* BVSS tiles counted on the tensor cores */
+  int64_t bvss_tiles_scalar; /* ... and with scalar popc */
+  double bvss_bits_per_slice; /* measured density of the fan-out BVSS */
 } cpg_stats;
 
 /* ------------------------------------------------------------ lifecycle */
@@ -258,6 +275,7 @@ typedef struct {
   double busy_ms;             /* device time of all launches */
   int32_t max_batch_seen;
   int32_t reserved;
+  double sfxt_ms;             /* device time of the suffix-tree rebuilds */
 } cpg_server_stats;
 
 void cpg_server_options_init(cpg_server_options* o);
@@ -322,6 +340,91 @@ cpg_status cpg_select_topk(const float* d_costs, int64_t n, int64_t k,
  *  - Calls no cudaMalloc/cudaFree; returns after the result is written. */
 cpg_status cpg_select_topk_noalloc(const float* d_costs, int64_t n, int64_t k,
                                    float* d_out, int64_t* n_out, void* stream);
+
+/* ------------------------------------------------------------ BVSS */
+/* Bit-vector slice sets (sigma = 8) of a row -> column relation, the
+ * reference's HostBvss (gpucpg/tc_sfxt_bvss.cuh:17-31, tc_pfxt_bvss.cuh:7-25):
+ * columns in intervals of 8, one slice (row, 8-bit mask) per row and interval,
+ * slices packed 128 to a VSS (slice i in lane i % 32, chunk i / 32).  Built on
+ * the host; the device copy is made on the first device call. */
+typedef struct cpg_bvss cpg_bvss;
+
+typedef struct {
+  int32_t sigma;              /* 8 */
+  int32_t slices_per_thread;  /* 4 */
+  int32_t slice_capacity;     /* 128 */
+  int32_t n_intervals;
+  int32_t n_vss;
+  int32_t n_rows;             /* rows the slices refer to */
+  int64_t unpadded_slices;
+  int64_t total_set_bits;
+  double compression_ratio;   /* total_set_bits / (8 * unpadded_slices) */
+} cpg_bvss_info;
+
+typedef struct {
+  int32_t device;
+  void* stream;               /* cudaStream_t; NULL = the library's own */
+  int32_t tiles;              /* cpg_bvss_tiles */
+  int32_t min_bits;           /* density test (0 = default 2) */
+  int32_t min_slices;         /* density test (0 = default 32) */
+  int32_t half_slices;        /* skip the upper-half MMA of a VSS with at most
+                                 this many slices (0 = default 64; the
+                                 reference's shape dispatch) */
+  uint32_t spin_limit;        /* grid-barrier polls; 0 = default */
+  int32_t reserved[3];
+} cpg_bvss_opts;
+
+typedef struct {
+  int32_t levels;             /* BFS levels holding a row (levels call) */
+  int32_t pad;
+  int64_t tiles_tensor;       /* VSS tiles counted on the tensor cores */
+  int64_t tiles_scalar;       /* ... with scalar popc */
+  int64_t mma_issued;         /* m8n8k128 b1 MMAs issued */
+  double device_ms;
+} cpg_bvss_run_stats;
+
+void cpg_bvss_opts_init(cpg_bvss_opts* o);
+/* Fan-out BVSS: rows are tail vertices, columns their heads
+ * (build_bvss_from_fanout_csr, tc_sfxt_bvss.cuh:106-156).  With succs
+ * non-NULL: the transposed deviation matrix A_dev, rows are heads v and
+ * columns the tails u of edges u -> v with v != succs[u]
+ * (build_adev_bvss_from_fanout_csr, tc_pfxt_bvss.cuh:117-175). */
+cpg_status cpg_bvss_build(cpg_bvss** out, int32_t n, const int32_t* row_ptr,
+                          const int32_t* col_idx, const int32_t* succs);
+/* One slice per deviation d of source u: row d, column u
+ * (build_adev_bvss_from_compact_deviation_offsets, tc_pfxt_bvss.cuh:177-226). */
+cpg_status cpg_bvss_build_compact(cpg_bvss** out, int32_t n, const int32_t* deviation_offsets);
+void cpg_bvss_destroy(cpg_bvss* b);
+const char* cpg_bvss_last_error(const cpg_bvss* b);
+cpg_status cpg_bvss_get_info(const cpg_bvss* b, cpg_bvss_info* info);
+/* Copies the packed arrays; any NULL pointer is skipped.  Sizes:
+ * real_ptrs n_intervals + 1, virtual_to_real and slice_counts n_vss,
+ * row_ids 128 * n_vss, masks 32 * n_vss. */
+cpg_status cpg_bvss_get_arrays(const cpg_bvss* b, int32_t* real_ptrs, int32_t* virtual_to_real,
+                               uint8_t* slice_counts, int32_t* row_ids, uint32_t* masks);
+/* Sorted columns of a row (decode_row_neighbors, tc_sfxt_bvss.cuh:158-183). */
+cpg_status cpg_bvss_decode_row(const cpg_bvss* b, int32_t row, int32_t* out, int32_t cap,
+                               int32_t* n_out);
+/* 1 if the packed form holds exactly the distinct columns of every row of
+ * the given CSR (verify_bvss_matches_csr / verify_adev_bvss_matches_csr),
+ * 0 if not, negative on invalid input.  succs as in cpg_bvss_build. */
+int32_t cpg_bvss_verify(const cpg_bvss* b, int32_t n, const int32_t* row_ptr,
+                        const int32_t* col_idx, const int32_t* succs);
+/* Pull BFS levels from the sinks over a fan-out BVSS: a row gets level L+1 the
+ * first time one of its columns has level L; unreached rows get -1
+ * (run_tc_bvss_pull_bfs_levels / run_scalar_bvss_pull_bfs_levels,
+ * tc_sfxt_bvss.cuh:418-577; the tile choice is opts->tiles).  sinks = NULL
+ * uses every row without columns.  levels: host array of n_rows. */
+cpg_status cpg_bvss_levels(cpg_bvss* b, const cpg_bvss_opts* opts, const int32_t* sinks,
+                           int32_t n_sinks, int32_t* levels, cpg_bvss_run_stats* stats);
+/* Pairs (u, v) of an A_dev BVSS with u in the sources: every deviation edge
+ * leaving the sources (discover_pairs_for_sources, tc_pfxt_bvss.cuh:582-636).
+ * pairs: host array of 2 * max_pairs int32, sorted by (u, v) on return;
+ * *n_pairs is the full count, CPG_ERR_CAPACITY when above max_pairs. */
+cpg_status cpg_bvss_discover_pairs(cpg_bvss* b, const cpg_bvss_opts* opts,
+                                   const int32_t* sources, int32_t n_sources, int32_t* pairs,
+                                   int64_t max_pairs, int64_t* n_pairs,
+                                   cpg_bvss_run_stats* stats);
 
 /* ------------------------------------------------------------ generator */
 /* Seeded levelised timing DAG in the reference's text format conventions:

@@ -584,3 +584,86 @@ int64_t orc_closure_topk_ex(const orc_graph* g, const int32_t* dist,
   free(acc.a);
   return nout;
 }
+
+/* ------------------------------------------------------------ BVSS checks */
+
+void orc_bfs_levels(int32_t n, const int32_t* adjp, const int32_t* adj,
+                    const int32_t* sinks, int32_t n_sinks, int32_t* levels) {
+  /* fan-in lists, then a plain queue BFS from the sinks */
+  int32_t* ip = calloc((size_t)n + 1, sizeof(int32_t));
+  int32_t* ia = malloc(sizeof(int32_t) * (adjp[n] ? (size_t)adjp[n] : 1));
+  int32_t* fill = malloc(sizeof(int32_t) * (n ? (size_t)n : 1));
+  int32_t* q = malloc(sizeof(int32_t) * (n ? (size_t)n : 1));
+  for (int32_t u = 0; u < n; ++u)
+    for (int32_t e = adjp[u]; e < adjp[u + 1]; ++e) ip[adj[e] + 1]++;
+  for (int32_t v = 0; v < n; ++v) ip[v + 1] += ip[v];
+  for (int32_t v = 0; v < n; ++v) fill[v] = ip[v];
+  for (int32_t u = 0; u < n; ++u)
+    for (int32_t e = adjp[u]; e < adjp[u + 1]; ++e) ia[fill[adj[e]]++] = u;
+  for (int32_t v = 0; v < n; ++v) levels[v] = -1;
+  int32_t qh = 0, qt = 0;
+  for (int32_t i = 0; i < n_sinks; ++i) {
+    const int32_t t = sinks[i];
+    if (t < 0 || t >= n || levels[t] >= 0) continue;
+    levels[t] = 0;
+    q[qt++] = t;
+  }
+  while (qh < qt) {
+    const int32_t v = q[qh++];
+    for (int32_t e = ip[v]; e < ip[v + 1]; ++e) {
+      const int32_t u = ia[e];
+      if (levels[u] < 0) {
+        levels[u] = levels[v] + 1;
+        q[qt++] = u;
+      }
+    }
+  }
+  free(ip);
+  free(ia);
+  free(fill);
+  free(q);
+}
+
+static int cmp_pair(const void* a, const void* b) {
+  const int32_t* x = (const int32_t*)a;
+  const int32_t* y = (const int32_t*)b;
+  if (x[0] != y[0]) return x[0] < y[0] ? -1 : 1;
+  if (x[1] != y[1]) return x[1] < y[1] ? -1 : 1;
+  return 0;
+}
+
+int64_t orc_adev_pairs(int32_t n, const int32_t* adjp, const int32_t* adj,
+                       const int32_t* succ, const int32_t* sources, int32_t n_sources,
+                       int32_t* pairs, int64_t max_pairs) {
+  unsigned char* is_src = calloc(n ? (size_t)n : 1, 1);
+  for (int32_t i = 0; i < n_sources; ++i)
+    if (sources[i] >= 0 && sources[i] < n) is_src[sources[i]] = 1;
+  int64_t cap = adjp[n] ? adjp[n] : 1;
+  int32_t* all = malloc(sizeof(int32_t) * 2 * (size_t)cap);
+  int64_t cnt = 0;
+  for (int32_t u = 0; u < n; ++u) {
+    if (!is_src[u]) continue;
+    for (int32_t e = adjp[u]; e < adjp[u + 1]; ++e) {
+      if (adj[e] == succ[u]) continue;
+      all[2 * cnt] = u;
+      all[2 * cnt + 1] = adj[e];
+      ++cnt;
+    }
+  }
+  qsort(all, (size_t)cnt, 2 * sizeof(int32_t), cmp_pair);
+  int64_t uniq = 0;
+  for (int64_t i = 0; i < cnt; ++i) {
+    if (uniq > 0 && all[2 * i] == all[2 * (uniq - 1)] && all[2 * i + 1] == all[2 * (uniq - 1) + 1])
+      continue;
+    all[2 * uniq] = all[2 * i];
+    all[2 * uniq + 1] = all[2 * i + 1];
+    ++uniq;
+  }
+  for (int64_t i = 0; i < uniq && i < max_pairs; ++i) {
+    pairs[2 * i] = all[2 * i];
+    pairs[2 * i + 1] = all[2 * i + 1];
+  }
+  free(all);
+  free(is_src);
+  return uniq;
+}

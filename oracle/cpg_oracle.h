@@ -114,6 +114,21 @@ int32_t orc_deviation_csr(int32_t n, const int32_t* adjp, const int32_t* adj,
 /* Cost of one child, left to right as expand_short_pile writes it. */
 float orc_child_cost(float parent, int32_t dist_n, float w, int32_t dist_v);
 
+/* Pull BFS levels from the sinks over a fan-out CSR: a vertex gets level L+1
+ * the first time one of its heads has level L; -1 if never reached
+ * (run_scalar_bvss_pull_bfs_levels, tc_sfxt_bvss.cuh:418-495, restated on the
+ * CSR instead of the packed slices). */
+void orc_bfs_levels(int32_t n, const int32_t* adjp, const int32_t* adj,
+                    const int32_t* sinks, int32_t n_sinks, int32_t* levels);
+
+/* Distinct deviation pairs (u, v) leaving the sources: fan-out edges u -> v
+ * of a source u with v != succ[u] (discover_pairs_for_sources,
+ * tc_pfxt_bvss.cuh:582-636).  Writes at most max_pairs pairs sorted by
+ * (u, v) as 2 int32 each; returns the full count. */
+int64_t orc_adev_pairs(int32_t n, const int32_t* adjp, const int32_t* adj,
+                       const int32_t* succ, const int32_t* sources, int32_t n_sources,
+                       int32_t* pairs, int64_t max_pairs);
+
 #ifdef __cplusplus
 }
 #endif

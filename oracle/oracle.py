@@ -53,6 +53,12 @@ def _lib():
     lib.orc_deviation_csr.restype = C.c_int32
     lib.orc_child_cost.argtypes = [C.c_float, C.c_int32, C.c_float, C.c_int32]
     lib.orc_child_cost.restype = C.c_float
+    lib.orc_bfs_levels.argtypes = [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
+                                   C.c_void_p]
+    lib.orc_bfs_levels.restype = None
+    lib.orc_adev_pairs.argtypes = [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.c_int32, C.c_void_p, C.c_int64]
+    lib.orc_adev_pairs.restype = C.c_int64
     return lib
 
 
@@ -161,3 +167,26 @@ def deviation_csr(adjp, adj, w, succ, dist):
 
 def child_cost(parent: float, dist_n: int, w: float, dist_v: int) -> float:
     return lib().orc_child_cost(parent, dist_n, w, dist_v)
+
+
+def bfs_levels(n, adjp, adj, sinks) -> np.ndarray:
+    """Pull BFS levels from the sinks (orc_bfs_levels)."""
+    adjp = np.ascontiguousarray(adjp, np.int32)
+    adj = np.ascontiguousarray(adj, np.int32)
+    sinks = np.ascontiguousarray(sinks, np.int32)
+    out = np.zeros(int(n), np.int32)
+    lib().orc_bfs_levels(int(n), _p(adjp), _p(adj), _p(sinks), int(sinks.size), _p(out))
+    return out
+
+
+def adev_pairs(n, adjp, adj, succ, sources) -> np.ndarray:
+    """Distinct deviation pairs leaving the sources, sorted (orc_adev_pairs)."""
+    adjp = np.ascontiguousarray(adjp, np.int32)
+    adj = np.ascontiguousarray(adj, np.int32)
+    succ = np.ascontiguousarray(succ, np.int32)
+    sources = np.ascontiguousarray(sources, np.int32)
+    cap = max(int(adjp[-1]), 1)
+    out = np.zeros(2 * cap, np.int32)
+    got = lib().orc_adev_pairs(int(n), _p(adjp), _p(adj), _p(succ), _p(sources),
+                               int(sources.size), _p(out), cap)
+    return out[: 2 * got].reshape(-1, 2)

@@ -102,27 +102,42 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.rows)}
 
 
+def ranks():
+    """(world, rank, local rank) from the torchrun environment."""
+    return (int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
 def dist_setup(n_gpus):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    """Process group for N > 1 replicas: NCCL between GPUs, gloo without a
+    GPU (the host-side logic is exercised that way).  The replicas exchange
+    only the timing maximum and barriers; the path itself has no exchange."""
+    world, rank, local = ranks()
     if world > 1:
         import datetime
 
+        import torch
         import torch.distributed as dist
-        dist.init_process_group("nccl" if n_gpus > 0 else "gloo",
-                                timeout=datetime.timedelta(seconds=300))
+        backend = "nccl" if (n_gpus > 0 and torch.cuda.is_available()) else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
     return world, rank, local
 
 
-def max_over_ranks(x, world, device):
+def max_over_ranks(x, world, device=None):
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dev = device if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_value(paths_per_rank, ms_max, world):
+    """Whole-job K-paths/sec of N independent replicas: every rank's paths
+    over the slowest rank's time."""
+    return world * paths_per_rank / (ms_max / 1000.0)
 
 
 def barrier(world):
@@ -150,7 +165,9 @@ def cpu_reference(k_sample, dag=None):
 
 
 def run_reference(args):
-    world, rank, _ = dist_setup(args.gpus)
+    # rank 0 alone times the reference's CPU path; the other ranks exit
+    # without work (no process group is needed for that)
+    world, rank, _ = ranks()
     if rank != 0:
         return
     k_sample = args.cpu_k
@@ -222,7 +239,7 @@ def run_ours(args):
     ms = ev0.elapsed_time(ev1) / args.steps
     ms = max_over_ranks(ms, world, device)
     n_out = int(g.get_slacks(K).size)
-    value = world * n_out / (ms / 1000.0)
+    value = replica_value(n_out, ms, world)
     stats = g.stats()
 
     # ---- end-to-end through the C ABI from host buffers
@@ -273,7 +290,7 @@ def run_ours(args):
                          "paths_accepted": acc, "items_generated": items},
         "roofline": {"bound": "hbm", "kernel": kern, "achieved": ach, "peak": hbm,
                      "peak_source": src, "unit": "GB/s", "frac": ach / hbm, "traffic": None},
-        "e2e": {"value": world * n_out / (e2e / 1000.0), "unit": "paths/s",
+        "e2e": {"value": replica_value(n_out, e2e, world), "unit": "paths/s",
                 "ms_per_step": e2e, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": d2h},
         "gpu_launches": int(launches),
         "clocks": clk,
@@ -402,8 +419,9 @@ def served_stream(n_graphs, sizes, count=5000, rate=500.0, seed=9):
     return qs
 
 
-def _replay(dags, qs, max_batch):
-    """Submit at the stream's arrival times (open loop), then collect."""
+def _serve_replay(dags, qs, open_loop=True, max_batch=256):
+    """The served form: submit at the stream's arrival times (open loop) or
+    all at once (saturation), then collect every result."""
     import cpg_b200
     with cpg_b200.Server(max_batch=max_batch, hbm_budget_bytes=150 << 30) as s:
         for d in dags:
@@ -413,7 +431,7 @@ def _replay(dags, qs, max_batch):
         tickets = []
         for at, g, k, upd in qs:
             delay = at - (time.perf_counter() - t0)
-            if delay > 0:
+            if open_loop and delay > 0:
                 time.sleep(delay)
             tickets.append(s.submit(g, k, *(upd if upd else (None, None))))
         for tk in tickets:
@@ -423,11 +441,50 @@ def _replay(dags, qs, max_batch):
     return st
 
 
+def _plain_replay(dags, qs, open_loop=True):
+    """The plain form on the same stream: one resident handle per graph, one
+    query at a time in arrival order (update delays, report_paths, read the
+    costs back).  Latency is arrival to result, as for the server."""
+    import cpg_b200
+    handles = []
+    for d in dags:
+        h = cpg_b200.CpGen()
+        h.load_dag(d)
+        h.levelize()
+        handles.append(h)
+    lat, paths = [], 0
+    t0 = time.perf_counter()
+    done = 0.0
+    for at, g, k, upd in qs:
+        arrive = at if open_loop else 0.0
+        delay = arrive - (time.perf_counter() - t0)
+        if delay > 0:
+            time.sleep(delay)
+        h = handles[g]
+        if upd is not None:
+            h.update_delays(*upd)
+        h.report_paths(k)
+        paths += int(h.get_slacks(k).size)
+        done = time.perf_counter() - t0
+        lat.append((done - arrive) * 1e3)
+    for h in handles:
+        h.close()
+    lat = np.sort(np.asarray(lat))
+    first = qs[0][0] if open_loop else 0.0
+    wall = done - first
+    pick = lambda f: float(lat[min(lat.size - 1, int(np.ceil(f * lat.size)) - 1)])
+    return {"completed": len(qs), "paths": paths, "p50_ms": pick(0.50), "p99_ms": pick(0.99),
+            "mean_ms": float(lat.mean()), "max_ms": float(lat[-1]), "wall_s": wall,
+            "paths_per_s": paths / wall}
+
+
 def run_served(args):
     dags, _ = batch_workload(seed=5, count=32)
     qs = served_stream(len(dags), [d.m for d in dags], count=args.served_queries)
-    served = _replay(dags, qs, max_batch=256)
-    plain = _replay(dags, qs, max_batch=1)
+    served = _serve_replay(dags, qs, open_loop=True)
+    plain = _plain_replay(dags, qs, open_loop=True)
+    served_sat = _serve_replay(dags, qs, open_loop=False)
+    plain_sat = _plain_replay(dags, qs, open_loop=False)
     line = {
         "form": "served", "metric": METRIC, "value": served["paths_per_s"], "unit": "paths/s",
         "n_gpus": 1, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
@@ -438,6 +495,12 @@ def run_served(args):
         "plain_sequential": {"value": plain["paths_per_s"], "p50_ms": plain["p50_ms"],
                              "p99_ms": plain["p99_ms"], "stats": plain},
         "speedup_vs_plain": served["paths_per_s"] / max(plain["paths_per_s"], 1e-9),
+        # the same 5,000 queries submitted at once: the largest K-paths/sec
+        # each form sustains on this mix (the open-loop rate caps the above)
+        "capacity": {"served": served_sat["paths_per_s"], "plain": plain_sat["paths_per_s"],
+                     "speedup_vs_plain": served_sat["paths_per_s"] /
+                     max(plain_sat["paths_per_s"], 1e-9),
+                     "served_stats": served_sat, "plain_stats": plain_sat},
     }
     print(json.dumps(line), flush=True)
 

@@ -55,6 +55,12 @@ struct cpg_handle {
   int32_t big_rows = 0, big_cap = 1;
   DevMem d_adjp, d_edges, d_iadjp, d_iadj, d_srcs, d_big_off, d_big_tmp,
       d_big_rows;
+  // several side-by-side graphs (batched and served forms): delay updates
+  // rebuild only the changed graphs, from each one's lowest changed level
+  bool multi_graph = false;
+  std::vector<int32_t> graph_voff;  // first vertex of each graph
+  std::vector<int32_t> graph_from;  // per graph: lowest changed level (INT32_MAX: clean)
+  DevMem d_vgraph, d_graph_from, d_upd;
   // BVSS form of the fan-out CSR, for the pull Kahn step
   bool use_bvss = false;
   double bvss_bps = 0;  // set bits per slice (sampled, or exact once built)
@@ -206,6 +212,9 @@ Status upload_graph(cpg_handle* h, int32_t n, int32_t m, const int32_t* adjp,
   if (max_deg > kMaxRow)
     return fail(h, CPG_ERR_INVALID, "out-degree above 16384 is not supported");
   h->has_graph = false;
+  h->multi_graph = false;  // cpg_batch_commit sets it after the upload
+  h->graph_voff.clear();
+  h->graph_from.clear();
   {
     Status st = setup_bvss(h, n, adjp, adj);
     if (st != CPG_OK) return st;
@@ -334,6 +343,11 @@ SfxtParams sfxt_params(cpg_handle* h, int32_t start_level) {
   p.known_levels = h->levels;
   p.spin_limit = h->opts.spin_limit ? h->opts.spin_limit : kDefaultSpinLimit;
   p.grid_limit = h->sfxt_grid_limit;
+  if (h->multi_graph && start_level > 0) {
+    p.vgraph = P<int32_t>(h->d_vgraph);
+    p.graph_from = P<int32_t>(h->d_graph_from);
+    p.append_pool = 1;
+  }
   if (h->use_bvss) {
     p.bvss = 1;
     p.bv_ptr = P<int32_t>(h->d_bv_ptr);
@@ -354,8 +368,12 @@ SfxtParams sfxt_params(cpg_handle* h, int32_t start_level) {
 // Device work of one suffix-tree build, asynchronous and capturable.
 Status enqueue_sfxt(cpg_handle* h, int32_t start_level, int* launches) {
   cudaStream_t s = h->stream;
+  if (h->multi_graph && start_level > 0)
+    CK(cudaMemcpyAsync(h->d_graph_from.p, h->graph_from.data(), h->graph_from.size() * 4,
+                       cudaMemcpyHostToDevice, s), "H2D changed levels");
   CK(launch_init_sfxt_counters(P<SfxtCounters>(h->d_sctr), P<unsigned long long>(h->d_pool_mark),
-                               start_level, s), "sfxt counters");
+                               start_level, h->multi_graph && start_level > 0, s),
+     "sfxt counters");
   if (h->use_bvss && start_level == 0) {
     // the pull leaves the bitmaps clear; a build cut short by an error may not
     CK(cudaMemsetAsync(h->d_fbits.p, 0, h->d_fbits.bytes, s), "memset");
@@ -390,6 +408,7 @@ int finish_sfxt(cpg_handle* h, int32_t start_level) {
   h->sfxt_valid = true;
   h->h_sfxt_cached = false;
   h->dirty_level = -1;
+  std::fill(h->graph_from.begin(), h->graph_from.end(), INT32_MAX);
   return CPG_OK;
 }
 
@@ -414,9 +433,13 @@ Status run_sfxt(cpg_handle* h, int32_t start_level) {
     cudaEventElapsedTime(&ms, h->ev[0], h->ev[1]);
     h->stats.sfxt_ms = ms;
     if (r == kRetry) {
-      // chain heaps outgrew their pool: grow and rebuild from scratch
-      st = grow_heap_pool(h);
-      if (st != CPG_OK) return st;
+      // chain heaps outgrew their pool.  Incremental builds of side-by-side
+      // graphs append to the pool, so first rebuild from scratch (which
+      // compacts it); grow only if a full build overflows.
+      if (!(h->multi_graph && start_level > 0)) {
+        st = grow_heap_pool(h);
+        if (st != CPG_OK) return st;
+      }
       start_level = 0;
       continue;
     }
@@ -968,7 +991,8 @@ cpg_status cpg_destroy(cpg_handle* h) {
                    &h->d_rank, &h->d_out_cost, &h->d_out_nodes, &h->d_pq,
                    &h->d_qids, &h->d_ehist, &h->d_esort, &h->d_equery, &h->d_ectr,
                    &h->d_bv_ptr, &h->d_bv_masks, &h->d_bv_rows, &h->d_bv_cnt,
-                   &h->d_bv_deps, &h->d_fbits, &h->d_iact, &h->d_act_list};
+                   &h->d_bv_deps, &h->d_fbits, &h->d_iact, &h->d_act_list,
+                   &h->d_vgraph, &h->d_graph_from, &h->d_upd};
   for (DevMem* b : all) release(*b);
   for (auto& e : h->ev)
     if (e) cudaEventDestroy(e);
@@ -1056,23 +1080,30 @@ cpg_status cpg_update_delays(cpg_handle* h, int64_t count, const int32_t* eids,
   for (int64_t i = 0; i < count; ++i) {
     const int32_t e = eids[i];
     if (e < 0 || e >= h->g.m) return fail(h, CPG_ERR_INVALID, "edge id out of range");
-    if (have_levels) {
-      const auto it = std::upper_bound(h->g.adjp.begin(), h->g.adjp.end(), e);
-      const int32_t tail = static_cast<int32_t>(it - h->g.adjp.begin()) - 1;
-      const int32_t lv = h->h_level_of[tail];
-      if (lv >= 0) lowest = std::min(lowest, lv);
+  }
+  for (int64_t i = 0; have_levels && i < count; ++i) {
+    const auto it = std::upper_bound(h->g.adjp.begin(), h->g.adjp.end(), eids[i]);
+    const int32_t tail = static_cast<int32_t>(it - h->g.adjp.begin()) - 1;
+    const int32_t lv = h->h_level_of[tail];
+    if (lv < 0) continue;
+    lowest = std::min(lowest, lv);
+    if (h->multi_graph) {
+      const size_t g = static_cast<size_t>(
+          std::upper_bound(h->graph_voff.begin(), h->graph_voff.end(), tail) -
+          h->graph_voff.begin() - 1);
+      h->graph_from[g] = std::min(h->graph_from[g], lv);
     }
   }
-  DevMem tmp_e, tmp_w;
-  CK(ensure(tmp_e, count * 4), "alloc delay update");
-  CK(ensure(tmp_w, count * 4), "alloc delay update");
-  CK(cudaMemcpy(tmp_e.p, eids, count * 4, cudaMemcpyHostToDevice), "H2D eids");
-  CK(cudaMemcpy(tmp_w.p, w, count * 4, cudaMemcpyHostToDevice), "H2D delays");
-  CK(launch_scatter_delays(P<DevEdge>(h->d_edges), P<int32_t>(tmp_e),
-                           P<float>(tmp_w), count, h->stream), "scatter delays");
+  // staging kept by the handle: no allocation (and no device-wide
+  // synchronisation) per update
+  CK(ensure(h->d_upd, static_cast<size_t>(count) * 8), "alloc delay update");
+  int32_t* up_e = P<int32_t>(h->d_upd);
+  float* up_w = reinterpret_cast<float*>(up_e + count);
+  CK(cudaMemcpyAsync(up_e, eids, count * 4, cudaMemcpyHostToDevice, h->stream), "H2D eids");
+  CK(cudaMemcpyAsync(up_w, w, count * 4, cudaMemcpyHostToDevice, h->stream), "H2D delays");
+  CK(launch_scatter_delays(P<DevEdge>(h->d_edges), up_e, up_w, count, h->stream),
+     "scatter delays");
   CK(cudaStreamSynchronize(h->stream), "scatter delays");
-  release(tmp_e);
-  release(tmp_w);
   // incremental rebuild from the lowest changed level (levels never change
   // with delays); without levels a full rebuild follows
   if (have_levels && lowest != INT32_MAX && lowest >= 1)
@@ -1506,6 +1537,19 @@ cpg_status cpg_batch_commit(cpg_batch* b) {
     b->src_end[g] = static_cast<int32_t>(
         std::lower_bound(srcs.begin(), srcs.end(), b->voff[g + 1]) - srcs.begin());
   }
+  // per-vertex graph ids for incremental rebuilds of single graphs
+  h->multi_graph = true;
+  h->graph_voff = b->voff;
+  h->graph_from.assign(ng, INT32_MAX);
+  {
+    std::vector<int32_t> vg(static_cast<size_t>(n));
+    for (size_t g = 0; g < ng; ++g)
+      std::fill(vg.begin() + b->voff[g], vg.begin() + b->voff[g + 1], static_cast<int32_t>(g));
+    CK(ensure(h->d_vgraph, std::max<size_t>(vg.size(), 1) * 4), "alloc graph ids");
+    CK(ensure(h->d_graph_from, std::max<size_t>(ng, 1) * 4), "alloc graph ids");
+    if (n)
+      CK(cudaMemcpy(h->d_vgraph.p, vg.data(), vg.size() * 4, cudaMemcpyHostToDevice), "H2D graph ids");
+  }
   b->committed = true;
   b->prepared = false;
   batch_drop_graph(b);
@@ -1745,24 +1789,30 @@ void server_loop(cpg_server* sv) {
       std::unique_lock<std::mutex> lk(sv->mu);
       sv->cv_work.wait(lk, [&] { return sv->stopping || !sv->queue.empty(); });
       if (sv->queue.empty()) break;  // stopping and drained
-      // admit in arrival order: up to max_batch queries whose predicted
+      // Admit in arrival order, up to max_batch queries whose predicted
       // footprint fits the budget.  Delay updates are applied before the
-      // launch, so an update may join only if no query already admitted
-      // reads the same graph: every query then sees arrival-order state.
+      // launch, so an update joins only if no admitted query reads its
+      // graph; otherwise it waits for the next launch, and so does every
+      // later request on that graph (a graph's requests keep their order),
+      // while requests on other graphs behind it are still admitted.
+      const size_t max_batch = static_cast<size_t>(std::max(1, sv->so.max_batch));
+      const size_t window = 4 * max_batch;
       int64_t used = 0;
-      std::vector<char> graph_read;
-      while (!sv->queue.empty() &&
-             static_cast<int32_t>(batch.size()) < std::max(1, sv->so.max_batch)) {
-        ServerReq& r = sv->queue.front();
-        if (graph_read.size() <= static_cast<size_t>(r.graph)) graph_read.resize(r.graph + 1, 0);
-        if (!batch.empty() && !r.eids.empty() && graph_read[r.graph]) break;
+      std::vector<char> graph_read(sv->b->voff.size(), 0), blocked(sv->b->voff.size(), 0);
+      for (size_t i = 0; i < sv->queue.size() && i < window && batch.size() < max_batch;) {
+        ServerReq& r = sv->queue[i];
+        if (blocked[r.graph] || (!r.eids.empty() && graph_read[r.graph])) {
+          blocked[r.graph] = 1;
+          ++i;
+          continue;
+        }
         const int64_t need = predicted_bytes(r.k);
         if (!batch.empty() && sv->so.hbm_budget_bytes > 0 && used + need > sv->so.hbm_budget_bytes)
           break;
         used += need;
         graph_read[r.graph] = 1;
         batch.push_back(std::move(r));
-        sv->queue.pop_front();
+        sv->queue.erase(sv->queue.begin() + static_cast<std::ptrdiff_t>(i));
       }
     }
     Status st = CPG_OK;

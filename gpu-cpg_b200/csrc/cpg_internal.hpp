@@ -135,6 +135,13 @@ struct SfxtParams {
   int32_t known_levels;    // level count when start_level > 0
   unsigned int spin_limit;
   int32_t grid_limit;      // persistent CTAs (0: one per co-resident slot)
+  // Incremental rebuild of some of several side-by-side graphs: vertex v is
+  // rebuilt iff its level >= graph_from[vgraph[v]] (vgraph null: every vertex
+  // of the rebuilt levels).  append_pool: new chain-heap nodes go after every
+  // node in use instead of reusing the rebuilt levels' share of the pool.
+  const int32_t* vgraph;
+  const int32_t* graph_from;
+  int32_t append_pool;
   // BVSS pull for the Kahn step of a full build; used when bvss != 0
   int32_t bvss;
   const int32_t* bv_ptr;       // VSS range of each interval of 8 vertices
@@ -224,7 +231,7 @@ constexpr int kSmemRow = 256;  // deviation rows up to this length sort in smem
 
 // Zero a build's counters on the device (capturable: no host copy).
 int launch_init_sfxt_counters(SfxtCounters* c, const unsigned long long* pool_mark,
-                              int start_level, void* stream);
+                              int start_level, int append_pool, void* stream);
 
 // Launch the persistent SFXT kernel (cooperative) and the row sorts that
 // follow it.  Returns a cudaError_t; *launches counts the kernels.

@@ -181,6 +181,11 @@ __device__ void build_vertex(const SfxtParams& p, int v, int lvl, bool do_kahn) 
   }
 }
 
+// Whether an incremental build rebuilds v (at level lvl).
+__device__ __forceinline__ bool rebuilt(const SfxtParams& p, int v, int lvl) {
+  return !p.vgraph || lvl >= __ldg(p.graph_from + __ldg(p.vgraph + v));
+}
+
 // Chain heap of v: the heap of succ[v] with v's cheapest deviation inserted
 // at position size+1 of a complete binary heap, copying the root-to-position
 // path and carrying the larger element down.  One thread per vertex; runs one
@@ -365,16 +370,20 @@ sfxt_persistent_kernel(SfxtParams p) {
       p.lvlp[lvl + 1] = end;
       // heap nodes in use before the previous level's inserts (which start
       // in this pass)
-      if (lvl > first)
+      if (lvl > first && !p.append_pool)
         p.pool_mark[lvl - 1] = *reinterpret_cast<volatile unsigned long long*>(&p.ctr->hnode_used);
     }
     for (int i = beg + gwarp; i < end; i += nwarps) {
-      build_vertex(p, __ldcg(p.order + i), lvl, full && !kBvss);
+      const int v = __ldcg(p.order + i);
+      if (full || rebuilt(p, v, lvl)) build_vertex(p, v, lvl, full && !kBvss);
     }
     if (kBvss && pull)
       for (int i = abeg + gwarp; i < aend; i += nwarps)
         bvss_pull_interval(p, __ldcg(p.act_list + i), lvl, n_tensor, n_scalar);
-    for (int i = pbeg + tid; i < pend; i += nth) heap_insert(p, __ldcg(p.order + i));
+    for (int i = pbeg + tid; i < pend; i += nth) {
+      const int v = __ldcg(p.order + i);
+      if (full || rebuilt(p, v, lvl - 1)) heap_insert(p, v);
+    }
     // the tail keeps growing as soon as the next level starts appending, so
     // the level bound is the snapshot the last arriving block took
     if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit, &p.ctr->tail,
@@ -393,9 +402,12 @@ sfxt_persistent_kernel(SfxtParams p) {
     }
   }
   // heaps of the last level
-  if (blockIdx.x == 0 && threadIdx.x == 0 && lvl > first)
+  if (blockIdx.x == 0 && threadIdx.x == 0 && lvl > first && !p.append_pool)
     p.pool_mark[lvl - 1] = *reinterpret_cast<volatile unsigned long long*>(&p.ctr->hnode_used);
-  for (int i = pbeg + tid; i < pend; i += nth) heap_insert(p, __ldcg(p.order + i));
+  for (int i = pbeg + tid; i < pend; i += nth) {
+    const int v = __ldcg(p.order + i);
+    if (full || rebuilt(p, v, lvl - 1)) heap_insert(p, v);
+  }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     p.ctr->levels = lvl;
     p.lvlp[lvl] = beg;
@@ -420,7 +432,8 @@ __device__ __forceinline__ unsigned long long sort_word(float key, int idx) {
 
 __global__ void __launch_bounds__(kSortWarps * 32)
 sort_rows_kernel(const int32_t* order, const int* range, const int32_t* adjp,
-                 const int32_t* dev_cnt, DevSidetrack* dev) {
+                 const int32_t* dev_cnt, DevSidetrack* dev, const int32_t* vgraph,
+                 const int32_t* graph_from, const int32_t* level_of) {
   __shared__ unsigned long long skey[kSortWarps][kSmemRow];
   __shared__ DevSidetrack srec[kSortWarps][kSmemRow];
   const int lane = threadIdx.x & 31;
@@ -430,6 +443,7 @@ sort_rows_kernel(const int32_t* order, const int* range, const int32_t* adjp,
     const int v = order[i];
     const int cnt = dev_cnt[v];
     if (cnt <= 1 || cnt > kSmemRow) continue;
+    if (vgraph && level_of[v] < graph_from[vgraph[v]]) continue;  // not rebuilt
     DevSidetrack* row = dev + adjp[v];
     if (cnt <= 32) {
       DevSidetrack r;
@@ -496,11 +510,13 @@ sort_rows_kernel(const int32_t* order, const int* range, const int32_t* adjp,
 __global__ void sort_big_rows_kernel(const int32_t* rows, const int32_t* adjp,
                                      const int32_t* dev_cnt, DevSidetrack* dev,
                                      const int32_t* big_off, DevSidetrack* big_tmp,
-                                     int cap) {
+                                     int cap, const int32_t* vgraph,
+                                     const int32_t* graph_from, const int32_t* level_of) {
   extern __shared__ unsigned long long wbuf[];
   const int v = rows[blockIdx.x];
   const int cnt = dev_cnt[v];
   if (cnt <= kSmemRow) return;
+  if (vgraph && level_of[v] < graph_from[vgraph[v]]) return;  // not rebuilt
   DevSidetrack* row = dev + adjp[v];
   DevSidetrack* tmp = big_tmp + big_off[v];
   int n2 = 1;
@@ -559,7 +575,7 @@ int launch_sfxt(const SfxtParams& p, int device, void* stream, int* grid_out,
   e = cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kSfxtThreads), args, 0, st);
   if (e != cudaSuccess) return e;
   sort_rows_kernel<<<sms * 8, kSortWarps * 32, 0, st>>>(
-      p.order, &p.ctr->sort_beg, p.adjp, p.dev_cnt, p.dev);
+      p.order, &p.ctr->sort_beg, p.adjp, p.dev_cnt, p.dev, p.vgraph, p.graph_from, p.level_of);
   int n = 2;
   if (p.n_big_rows > 0) {
     const size_t smem = static_cast<size_t>(p.big_row_cap) * sizeof(unsigned long long);
@@ -570,7 +586,8 @@ int launch_sfxt(const SfxtParams& p, int device, void* stream, int* grid_out,
       if (e != cudaSuccess) return e;
     }
     sort_big_rows_kernel<<<p.n_big_rows, 1024, smem, st>>>(
-        p.big_rows, p.adjp, p.dev_cnt, p.dev, p.big_off, p.big_tmp, p.big_row_cap);
+        p.big_rows, p.adjp, p.dev_cnt, p.dev, p.big_off, p.big_tmp, p.big_row_cap, p.vgraph,
+        p.graph_from, p.level_of);
     ++n;
   }
   if (launches) *launches += n;
@@ -605,17 +622,17 @@ namespace {
 // rebuild, which restarts where the first rebuilt level's heaps began.
 __global__ void init_sfxt_counters_kernel(SfxtCounters* c,
                                           const unsigned long long* pool_mark,
-                                          int start_level) {
+                                          int start_level, int append_pool) {
   SfxtCounters z{};
-  if (start_level > 0) z.hnode_used = pool_mark[start_level];
+  if (start_level > 0) z.hnode_used = append_pool ? c->hnode_used : pool_mark[start_level];
   *c = z;
 }
 }  // namespace
 
 int launch_init_sfxt_counters(SfxtCounters* c, const unsigned long long* pool_mark,
-                              int start_level, void* stream) {
-  init_sfxt_counters_kernel<<<1, 1, 0, static_cast<cudaStream_t>(stream)>>>(c, pool_mark,
-                                                                            start_level);
+                              int start_level, int append_pool, void* stream) {
+  init_sfxt_counters_kernel<<<1, 1, 0, static_cast<cudaStream_t>(stream)>>>(
+      c, pool_mark, start_level, append_pool);
   return cudaGetLastError();
 }
 }  // namespace cpg

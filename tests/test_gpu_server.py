@@ -58,7 +58,8 @@ def test_server_mix_equals_alone():
     qs = _stream(dags, 48)
     mixed, st = _serve(dags, qs, max_batch=64)
     assert st["completed"] == len(qs) and st["max_batch_seen"] > 1
-    assert st["sfxt_rebuilds"] == sum(1 for q in qs if q[2] is not None)
+    n_upd = sum(1 for q in qs if q[2] is not None)
+    assert 1 <= st["sfxt_rebuilds"] <= n_upd
     one, _ = _serve(dags, qs, max_batch=1)
     csr = [_csr(d) for d in dags]
     for i, (g, k, upd) in enumerate(qs):
@@ -86,3 +87,28 @@ def test_server_admission_budget_splits_launches():
         st = s.stats()
     assert all(r.size == 2000 for r in res)
     assert st["max_batch_seen"] <= 2 and st["launches"] >= 8
+
+
+def test_server_many_updates_rebuild_only_changed_graphs():
+    """Every query updates delays: per-graph incremental rebuilds append to the
+    chain-heap pool until it overflows and a full rebuild compacts it; results
+    stay equal to each query answered alone."""
+    dags = _dags(3, seed=60)
+    rng = np.random.default_rng(8)
+    qs = []
+    for _ in range(90):
+        g = int(rng.integers(len(dags)))
+        m = dags[g].m
+        e = rng.choice(m, size=max(1, m // 50), replace=False).astype(np.int32)
+        qs.append((g, 500, (e, rng.uniform(0.1, 10.0, size=e.size).astype(np.float32))))
+    mixed, st = _serve(dags, qs, max_batch=16)
+    assert st["completed"] == len(qs)
+    csr = [_csr(d) for d in dags]
+    for i, (g, k, upd) in enumerate(qs):
+        adjp, adj, w = csr[g]
+        w[upd[0]] = upd[1]
+        with cpg_b200.CpGen() as h:
+            h.load_csr(dags[g].n, adjp, adj, w)
+            h.report_paths(k)
+            alone = h.get_slacks(k)
+        assert np.array_equal(mixed[i].view(np.uint32), alone.view(np.uint32)), i

@@ -505,6 +505,92 @@ def run_served(args):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- BVSS
+def local_dag_np(seed, levels, width, deg, span):
+    """A levelised DAG whose rows put `deg` heads in a window of `span`
+    consecutive pins of the next level (dense BVSS slices), vectorised."""
+    rng = np.random.default_rng(seed)
+    n = levels * width
+    src, dst = [], []
+    for lv in range(levels - 1):
+        off = rng.integers(0, width - span + 1, size=width)
+        pick = np.argsort(rng.random((width, span)), axis=1)[:, :deg]
+        src.append(np.repeat(np.arange(lv * width, (lv + 1) * width, dtype=np.int32), deg))
+        dst.append(((lv + 1) * width + off[:, None] + pick).astype(np.int32).ravel())
+    src = np.concatenate(src)
+    dst = np.concatenate(dst)
+    w = rng.uniform(0.1, 10.0, size=src.size).astype(np.float32)
+    return n, src, dst, w
+
+
+def _csr_np(n, src, dst):
+    order = np.argsort(src, kind="stable")
+    adjp = np.zeros(n + 1, np.int64)
+    np.add.at(adjp, src.astype(np.int64) + 1, 1)
+    return np.cumsum(adjp).astype(np.int32), dst[order].astype(np.int32)
+
+
+def run_bvss(args):
+    """BVSS pull BFS levels (tensor-core tiles vs scalar popc) and the suffix
+    tree with the BVSS pull against the CSR push, on the sparse 1M-pin
+    workload and on a dense level-local graph of the same size."""
+    import cpg_b200
+    import cases
+    out = {"form": "bvss", "graphs": {}}
+    graphs = {}
+    if args.bvss_graphs in ("both", "sparse"):
+        c = cases.CASES[WORKLOAD]
+        dag = cpg_b200.generate(cpg_b200.gen_params(**c["gen"]))
+        graphs["large1m_f32 (sparse slices)"] = (dag.n, dag.src, dag.dst, dag.w)
+    if args.bvss_graphs in ("both", "dense"):
+        graphs["local1m (dense slices: 16 heads in a 24-pin window, 200 x 5000 pins)"] = \
+            local_dag_np(3, 200, 5000, 16, 24)
+    for name, (n, src, dst, w) in graphs.items():
+        adjp, adj = _csr_np(n, src, dst)
+        b = cpg_b200.Bvss(n, adjp, adj)
+        info = b.info()
+        g = {"n": int(n), "m": int(src.size), "n_vss": info["n_vss"],
+             "bits_per_slice": info["total_set_bits"] / max(info["unpadded_slices"], 1),
+             "levels": {}}
+        sinks = np.nonzero(np.diff(adjp) == 0)[0].astype(np.int32)
+        ref = None
+        for tname, tiles in (("tensor", cpg_b200.TILES_TENSOR), ("scalar", cpg_b200.TILES_SCALAR),
+                             ("density", cpg_b200.TILES_DENSITY)):
+            times = []
+            for _ in range(args.warmup + args.steps):
+                lv, st = b.levels(sinks, tiles=tiles)
+                times.append(st["device_ms"])
+            if ref is None:
+                ref = lv
+            assert np.array_equal(lv, ref)
+            ms = float(np.median(times[args.warmup:]))
+            # slice bytes pulled: 128 B masks + 512 B rows + 1 B count per VSS
+            # tile, plus the 4 B level write per row
+            tiles_done = st["tiles_tensor"] + st["tiles_scalar"]
+            g["levels"][tname] = {"ms": ms, "bfs_levels": st["levels"],
+                                  "tiles_tensor": st["tiles_tensor"],
+                                  "tiles_scalar": st["tiles_scalar"], "mma": st["mma_issued"],
+                                  "slice_gbs": (641 * tiles_done + 4 * n) / (ms * 1e-3) / 1e9,
+                                  "b1_tops": st["mma_issued"] * 2 * 8 * 8 * 128 / (ms * 1e-3) / 1e12}
+        b.close()
+        sf = {}
+        for fname, fr in (("csr_push", cpg_b200.FRONTIER_CSR), ("bvss_pull", cpg_b200.FRONTIER_BVSS)):
+            with cpg_b200.CpGen(frontier=fr) as h:
+                h.load_edges(n, src, dst, w)
+                times = []
+                for _ in range(args.warmup + args.steps):
+                    h.levelize()  # a full build every time
+                    times.append(h.stats()["sfxt_ms"])
+                st = h.stats()
+                sf[fname] = {"ms": float(np.median(times[args.warmup:])),
+                             "frontier_used": st["frontier_used"],
+                             "tiles_tensor": st["bvss_tiles_tensor"],
+                             "tiles_scalar": st["bvss_tiles_scalar"]}
+        g["sfxt"] = sf
+        out["graphs"][name] = g
+    print(json.dumps(out), flush=True)
+
+
 def run_profile_case(args):
     """A short fixed sequence for ncu: one warm-up query, then one query
     (suffix tree + engine) on the same workload at --k."""
@@ -532,9 +618,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-case", action="store_true",
                     help="one warm-up and one measured query only (for ncu)")
-    ap.add_argument("--form", default="plain", choices=["plain", "batched", "served"])
+    ap.add_argument("--form", default="plain", choices=["plain", "batched", "served", "bvss"])
     ap.add_argument("--autotune", action="store_true")
     ap.add_argument("--served-queries", type=int, default=5000)
+    ap.add_argument("--bvss-graphs", default="both", choices=["both", "sparse", "dense"])
     args = ap.parse_args()
     if args.profile_case:
         run_profile_case(args)
@@ -542,6 +629,8 @@ def main():
         run_batched(args)
     elif args.form == "served":
         run_served(args)
+    elif args.form == "bvss":
+        run_bvss(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

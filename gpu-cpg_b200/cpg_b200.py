@@ -46,7 +46,7 @@ class Options(C.Structure):
         ("spin_limit", C.c_uint32), ("root_seeding", C.c_int32),
         ("host_stepped", C.c_int32), ("bvss_tiles", C.c_int32),
         ("bvss_min_bits", C.c_int32), ("bvss_min_slices", C.c_int32),
-        ("reserved", C.c_int32 * 3),
+        ("sfxt_level_sync", C.c_int32), ("reserved", C.c_int32 * 2),
     ]
 
 
@@ -298,7 +298,7 @@ class CpGen:
                  hbm_budget_bytes: int = 0, spin_limit: int = 0,
                  root_seeding: int = ROOTS_REFERENCE, host_stepped: bool = False,
                  bvss_tiles: int = TILES_DENSITY, bvss_min_bits: int = 0,
-                 bvss_min_slices: int = 0):
+                 bvss_min_slices: int = 0, sfxt_level_sync: bool = False):
         o = Options()
         lib.cpg_options_init(C.byref(o))
         o.device = device
@@ -312,6 +312,7 @@ class CpGen:
         o.bvss_tiles = bvss_tiles
         o.bvss_min_bits = bvss_min_bits
         o.bvss_min_slices = bvss_min_slices
+        o.sfxt_level_sync = 1 if sfxt_level_sync else 0
         self._h = C.c_void_p()
         st = lib.cpg_create(C.byref(self._h), C.byref(o))
         if st != CPG_OK:

@@ -60,7 +60,7 @@ struct cpg_handle {
   bool multi_graph = false;
   std::vector<int32_t> graph_voff;  // first vertex of each graph
   std::vector<int32_t> graph_from;  // per graph: lowest changed level (INT32_MAX: clean)
-  DevMem d_vgraph, d_graph_from, d_upd;
+  DevMem d_vgraph, d_graph_from, d_upd, d_queue;
   // BVSS form of the fan-out CSR, for the pull Kahn step
   bool use_bvss = false;
   double bvss_bps = 0;  // set bits per slice (sampled, or exact once built)
@@ -252,6 +252,7 @@ Status upload_graph(cpg_handle* h, int32_t n, int32_t m, const int32_t* adjp,
      "alloc big rows");
   // suffix tree storage (the deviation array doubles as upload staging)
   CK(ensure(h->d_order, nn * 4), "alloc order");
+  CK(ensure(h->d_queue, nn * 4 + 8), "alloc queue");
   CK(ensure(h->d_lvlp, (nn + 2) * 4), "alloc lvlp");
   CK(ensure(h->d_level_of, nn * 4), "alloc level_of");
   CK(ensure(h->d_dist, nn * 4), "alloc dist");
@@ -343,10 +344,16 @@ SfxtParams sfxt_params(cpg_handle* h, int32_t start_level) {
   p.known_levels = h->levels;
   p.spin_limit = h->opts.spin_limit ? h->opts.spin_limit : kDefaultSpinLimit;
   p.grid_limit = h->sfxt_grid_limit;
-  if (h->multi_graph && start_level > 0) {
-    p.vgraph = P<int32_t>(h->d_vgraph);
-    p.graph_from = P<int32_t>(h->d_graph_from);
+  p.queue = P<int32_t>(h->d_queue);
+  p.level_sync = h->opts.sfxt_level_sync == 1;
+  if (start_level > 0) {
+    // a dataflow build allocates heap nodes out of level order, so rebuilt
+    // levels take fresh nodes; a pool overflow falls back to a full build
     p.append_pool = 1;
+    if (h->multi_graph) {
+      p.vgraph = P<int32_t>(h->d_vgraph);
+      p.graph_from = P<int32_t>(h->d_graph_from);
+    }
   }
   if (h->use_bvss) {
     p.bvss = 1;
@@ -372,7 +379,7 @@ Status enqueue_sfxt(cpg_handle* h, int32_t start_level, int* launches) {
     CK(cudaMemcpyAsync(h->d_graph_from.p, h->graph_from.data(), h->graph_from.size() * 4,
                        cudaMemcpyHostToDevice, s), "H2D changed levels");
   CK(launch_init_sfxt_counters(P<SfxtCounters>(h->d_sctr), P<unsigned long long>(h->d_pool_mark),
-                               start_level, h->multi_graph && start_level > 0, s),
+                               start_level, start_level > 0, s),
      "sfxt counters");
   if (h->use_bvss && start_level == 0) {
     // the pull leaves the bitmaps clear; a build cut short by an error may not
@@ -433,10 +440,10 @@ Status run_sfxt(cpg_handle* h, int32_t start_level) {
     cudaEventElapsedTime(&ms, h->ev[0], h->ev[1]);
     h->stats.sfxt_ms = ms;
     if (r == kRetry) {
-      // chain heaps outgrew their pool.  Incremental builds of side-by-side
-      // graphs append to the pool, so first rebuild from scratch (which
-      // compacts it); grow only if a full build overflows.
-      if (!(h->multi_graph && start_level > 0)) {
+      // chain heaps outgrew their pool.  Incremental builds append to the
+      // pool, so first rebuild from scratch (which compacts it); grow only
+      // if a full build overflows.
+      if (start_level == 0) {
         st = grow_heap_pool(h);
         if (st != CPG_OK) return st;
       }
@@ -992,7 +999,7 @@ cpg_status cpg_destroy(cpg_handle* h) {
                    &h->d_qids, &h->d_ehist, &h->d_esort, &h->d_equery, &h->d_ectr,
                    &h->d_bv_ptr, &h->d_bv_masks, &h->d_bv_rows, &h->d_bv_cnt,
                    &h->d_bv_deps, &h->d_fbits, &h->d_iact, &h->d_act_list,
-                   &h->d_vgraph, &h->d_graph_from, &h->d_upd};
+                   &h->d_vgraph, &h->d_graph_from, &h->d_upd, &h->d_queue};
   for (DevMem* b : all) release(*b);
   for (auto& e : h->ev)
     if (e) cudaEventDestroy(e);

@@ -142,6 +142,9 @@ struct SfxtParams {
   const int32_t* vgraph;
   const int32_t* graph_from;
   int32_t append_pool;
+  // full CSR builds: dataflow work queue (n ints) unless level_sync is set
+  int32_t* queue;
+  int32_t level_sync;
   // BVSS pull for the Kahn step of a full build; used when bvss != 0
   int32_t bvss;
   const int32_t* bv_ptr;       // VSS range of each interval of 8 vertices

@@ -190,14 +190,27 @@ __device__ __forceinline__ bool rebuilt(const SfxtParams& p, int v, int lvl) {
 // at position size+1 of a complete binary heap, copying the root-to-position
 // path and carrying the larger element down.  One thread per vertex; runs one
 // level after v was relaxed, when succ[v]'s heap is complete.
+// kPublish: other threads poll ht_size[v] >= 0 for completion (the dataflow
+// build), so the root is made visible before the size.
+template <bool kPublish>
+__device__ __forceinline__ void heap_store(const SfxtParams& p, int v, int root, int size) {
+  p.ht_root[v] = root;
+  if (kPublish) {
+    __threadfence();
+    *reinterpret_cast<volatile int*>(p.ht_size + v) = size;
+  } else {
+    p.ht_size[v] = size;
+  }
+}
+
+template <bool kPublish = false>
 __device__ void heap_insert(const SfxtParams& p, int v) {
   const int s = __ldcg(p.succ + v);
   const int cnt = __ldcg(p.dev_cnt + v);
   const int base_root = s >= 0 ? __ldcg(p.ht_root + s) : -1;
   const int base_size = s >= 0 ? __ldcg(p.ht_size + s) : 0;
   if (cnt == 0) {
-    p.ht_root[v] = base_root;
-    p.ht_size[v] = base_size;
+    heap_store<kPublish>(p, v, base_root, base_size);
     return;
   }
   const float kmin = __int_as_float(__ldcg(p.deps + v));
@@ -207,8 +220,7 @@ __device__ void heap_insert(const SfxtParams& p, int v) {
       atomicAdd(&p.ctr->hnode_used, static_cast<unsigned long long>(depth + 1));
   if (a + depth + 1 > p.hnode_cap) {
     atomicCAS(&p.ctr->err, kDevOk, kDevCapacity);
-    p.ht_root[v] = -1;
-    p.ht_size[v] = 0;
+    heap_store<kPublish>(p, v, -1, 0);
     return;
   }
   int cv = v;
@@ -246,8 +258,7 @@ __device__ void heap_insert(const SfxtParams& p, int v) {
   leaf.left = -1;
   leaf.right = -1;
   p.hnodes[a + depth] = leaf;
-  p.ht_root[v] = static_cast<int>(a);
-  p.ht_size[v] = static_cast<int>(pos);
+  heap_store<kPublish>(p, v, static_cast<int>(a), static_cast<int>(pos));
 }
 
 // BVSS form of the Kahn step.  A vertex that joins level L sets its bit in
@@ -419,6 +430,170 @@ sfxt_persistent_kernel(SfxtParams p) {
   }
 }
 
+// ------------------------------------------------------------ dataflow build
+// Full CSR build without a barrier per level.  Kahn's algorithm runs as a
+// work queue: a vertex is appended to queue[] when its last head finishes,
+// and warp w builds the vertices in slots w, w + W, w + 2W, ... as they fill
+// (a warp waits only for its next slot).  Every warp takes its slots in
+// pushed order, so the earliest unfinished slot never waits on a later one
+// and the walk always progresses.  A head raises its tails' levels
+// (atomicMax) before taking its count off them, so a vertex's level is final
+// when it is queued.  The chain-heap insert follows the decrements, off the
+// build's critical path; it waits for the successor's heap (ht_size >= 0),
+// which lies on a lower level.  Afterwards the vertices are counting-sorted
+// by level into order[] / lvlp[] for the level-synchronous incremental
+// rebuilds.  Every wait is bounded by spin_limit polls (kDevTimeout).
+
+__device__ __forceinline__ int wait_slot(const SfxtParams& p, int s) {
+  int v = -1;
+  if ((threadIdx.x & 31) == 0) {
+    unsigned int it = 0;
+    const volatile int* q = p.queue + s;
+    while ((v = *q) < 0) {
+      if (++it > p.spin_limit || *reinterpret_cast<volatile int*>(&p.ctr->err) != kDevOk) {
+        atomicCAS(&p.ctr->err, kDevOk, kDevTimeout);
+        break;
+      }
+      __nanosleep(32);
+    }
+    __threadfence();  // acquire: the heads' dist / level writes
+  }
+  return __shfl_sync(0xffffffffu, v, 0);
+}
+
+__device__ __forceinline__ bool wait_heap(const SfxtParams& p, int s) {
+  if (s < 0) return true;
+  unsigned int it = 0;
+  const volatile int* hs = p.ht_size + s;
+  while (*hs < 0) {
+    if (++it > p.spin_limit || *reinterpret_cast<volatile int*>(&p.ctr->err) != kDevOk) {
+      atomicCAS(&p.ctr->err, kDevOk, kDevTimeout);
+      return false;
+    }
+    __nanosleep(32);
+  }
+  __threadfence();
+  return true;
+}
+
+// Kahn step of the dataflow build: raise the tails' levels, then take one
+// pending fan-out off each; tails reaching zero are queued.
+__device__ __forceinline__ void dataflow_push(const SfxtParams& p, int v, int lvl) {
+  const int lane = threadIdx.x & 31;
+  const int ib = p.iadjp[v];
+  const int ie = p.iadjp[v + 1];
+  for (int base = ib; base < ie; base += 4 * 32) {
+    int u[4];
+    bool ready[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const int e = base + c * 32 + lane;
+      u[c] = e < ie ? p.iadj[e] : -1;
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+      if (u[c] >= 0) atomicMax(p.level_of + u[c], lvl + 1);
+    __threadfence();  // release: v's dist and the levels before the counts
+#pragma unroll
+    for (int c = 0; c < 4; ++c) ready[c] = u[c] >= 0 && atomicSub(&p.deps[u[c]], 1) == 1;
+    __threadfence();
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const int slot = warp_append(&p.ctr->tail, ready[c]);
+      if (ready[c]) *reinterpret_cast<volatile int*>(p.queue + slot) = u[c];
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kSfxtThreads)
+sfxt_dataflow_kernel(SfxtParams p) {
+  __shared__ int s_hist[kSfxtThreads];
+  const int lane = threadIdx.x & 31;
+  const int gwarp = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int nwarps = gridDim.x * (blockDim.x >> 5);
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nth = gridDim.x * blockDim.x;
+  // phase 0: reset, clear the queue and the level histogram
+  for (int v = tid; v < p.n; v += nth) {
+    p.deps[v] = p.adjp[v + 1] - p.adjp[v];
+    p.dist[v] = INT_MAX;
+    p.succ[v] = -1;
+    p.dev_cnt[v] = 0;
+    p.ht_root[v] = -1;
+    p.ht_size[v] = -1;  // heap not built yet
+    p.level_of[v] = 0;
+    p.queue[v] = -1;
+  }
+  for (int i = tid; i < p.n + 2; i += nth) p.lvlp[i] = 0;
+  if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit)) return;
+  // the sinks start the queue
+  for (int base = blockIdx.x * blockDim.x; base < p.n; base += nth) {
+    const int v = base + threadIdx.x;
+    const bool sink = v < p.n && p.adjp[v + 1] == p.adjp[v];
+    const int slot = warp_append(&p.ctr->tail, sink);
+    if (sink) *reinterpret_cast<volatile int*>(p.queue + slot) = v;
+  }
+  int max_lvl = -1;
+  for (int s = gwarp; s < p.n; s += nwarps) {
+    const int v = wait_slot(p, s);
+    if (v < 0) break;
+    const int lvl = __ldcg(p.level_of + v);
+    max_lvl = max(max_lvl, lvl);
+    build_vertex(p, v, lvl, false);
+    __syncwarp();
+    dataflow_push(p, v, lvl);
+    if (lane == 0 && wait_heap(p, __ldcg(p.succ + v))) heap_insert<true>(p, v);
+    __syncwarp();
+  }
+  if (lane == 0) atomicMax(&p.ctr->levels, max_lvl + 1);
+  if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit)) return;
+  // counting sort by level: histogram (block-local when the levels fit)
+  const int L = *reinterpret_cast<volatile int*>(&p.ctr->levels);
+  if (L <= kSfxtThreads) {
+    for (int i = threadIdx.x; i < L; i += blockDim.x) s_hist[i] = 0;
+    __syncthreads();
+    for (int v = tid; v < p.n; v += nth) atomicAdd(&s_hist[p.level_of[v]], 1);
+    __syncthreads();
+    for (int i = threadIdx.x; i < L; i += blockDim.x)
+      if (s_hist[i]) atomicAdd(p.lvlp + i + 1, s_hist[i]);
+  } else {
+    for (int v = tid; v < p.n; v += nth) atomicAdd(p.lvlp + p.level_of[v] + 1, 1);
+  }
+  // the queue is free again: it holds the scatter cursors
+  for (int i = tid; i <= L; i += nth) p.queue[i] = 0;
+  if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit)) return;
+  if (blockIdx.x == 0) {
+    // inclusive scan of lvlp[1..L] by one block, kSfxtThreads at a time
+    __shared__ int carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int base = 1; base <= L; base += blockDim.x) {
+      const int i = base + threadIdx.x;
+      s_hist[threadIdx.x] = i <= L ? p.lvlp[i] : 0;
+      __syncthreads();
+      for (int o = 1; o < blockDim.x; o <<= 1) {
+        const int y = threadIdx.x >= o ? s_hist[threadIdx.x - o] : 0;
+        __syncthreads();
+        s_hist[threadIdx.x] += y;
+        __syncthreads();
+      }
+      if (i <= L) p.lvlp[i] = s_hist[threadIdx.x] + carry;
+      __syncthreads();
+      if (threadIdx.x == blockDim.x - 1) carry += s_hist[threadIdx.x];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      p.ctr->sort_beg = 0;
+      p.ctr->sort_end = p.n;
+    }
+  }
+  if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit)) return;
+  for (int v = tid; v < p.n; v += nth) {
+    const int l = p.level_of[v];
+    p.order[__ldcg(p.lvlp + l) + atomicAdd(p.queue + l, 1)] = v;
+  }
+}
+
 // ------------------------------------------------------------ row sorting
 // Orders each rebuilt vertex's deviation list by (key, edge position): one
 // warp per vertex, a register bitonic network for rows up to 32 and a shared
@@ -560,10 +735,13 @@ int launch_sfxt(const SfxtParams& p, int device, void* stream, int* grid_out,
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   if (e != cudaSuccess) return e;
-  // the BVSS pull only serves full builds; incremental ones take the CSR kernel
+  // full CSR builds run as a dataflow walk (unless asked to step the levels);
+  // the BVSS pull and incremental rebuilds step level by level
   const bool bvss = p.bvss && p.start_level == 0;
-  void* kern = bvss ? reinterpret_cast<void*>(sfxt_persistent_kernel<true>)
-                    : reinterpret_cast<void*>(sfxt_persistent_kernel<false>);
+  const bool dataflow = !bvss && p.start_level == 0 && !p.level_sync;
+  void* kern = bvss       ? reinterpret_cast<void*>(sfxt_persistent_kernel<true>)
+               : dataflow ? reinterpret_cast<void*>(sfxt_dataflow_kernel)
+                          : reinterpret_cast<void*>(sfxt_persistent_kernel<false>);
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kSfxtThreads, 0);
   if (e != cudaSuccess) return e;
   if (per_sm < 1) per_sm = 1;

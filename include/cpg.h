@@ -88,7 +88,10 @@ typedef struct {
   int32_t bvss_min_bits;    /* density test: frontier bits in the tile's byte
                                (0 = default 2) */
   int32_t bvss_min_slices;  /* density test: slices in the VSS (0 = default 32) */
-  int32_t reserved[3];
+  int32_t sfxt_level_sync;  /* 1: full suffix-tree builds step level by level
+                               with a grid barrier per level instead of the
+                               dataflow work queue; for A/B checks */
+  int32_t reserved[2];
 } cpg_options;
 
 typedef struct cpg_handle cpg_handle;

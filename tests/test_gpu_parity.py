@@ -260,3 +260,63 @@ def test_host_stepped_and_engine_agree(name):
             g.report_paths(k)
             out.append(g.get_slacks(k))
     assert np.array_equal(out[0].view(np.uint32), out[1].view(np.uint32))
+
+
+@pytest.mark.parametrize("name", ["simple", "tv80_unit_wgts", "single20k_f32", "small_int_s13"])
+def test_dataflow_build_equals_level_sync(name):
+    """The default full suffix-tree build (dataflow work queue) and the
+    level-synchronous one give the same levels, distances, successors and
+    paths; incremental rebuilds after either agree too."""
+    n, src, dst, w = _load(name)
+    rng = np.random.default_rng(3)
+    eids = rng.choice(src.size, size=max(1, src.size // 20), replace=False).astype(np.int32)
+    nw = rng.uniform(0.1, 10.0, size=eids.size).astype(np.float32)
+    out = []
+    for level_sync in (False, True):
+        with cpg_b200.CpGen(division=cpg_b200.DIV_IEEE, frontier=cpg_b200.FRONTIER_CSR,
+                            sfxt_level_sync=level_sync) as g:
+            g.load_edges(n, src, dst, w)
+            g.report_paths(2000)
+            first = (g.get_sfxt(), g.get_slacks(2000), g.num_levels())
+            g.update_delays(eids, nw)
+            g.report_paths(2000)
+            out.append((first, (g.get_sfxt(), g.get_slacks(2000))))
+    (a0, a1), (b0, b1) = out
+    for x, y in zip(a0[0], b0[0]):
+        np.testing.assert_array_equal(x, y)
+    assert a0[2] == b0[2]
+    assert np.array_equal(a0[1].view(np.uint32), b0[1].view(np.uint32))
+    for x, y in zip(a1[0], b1[0]):
+        np.testing.assert_array_equal(x, y)
+    assert np.array_equal(a1[1].view(np.uint32), b1[1].view(np.uint32))
+
+
+def test_many_incremental_updates_overflow_pool_and_stay_exact():
+    """Incremental rebuilds take fresh chain-heap nodes; after enough updates
+    the pool overflows and a full rebuild compacts it.  Results must equal a
+    fresh build of the final delays throughout."""
+    n, src, dst, w = _load("single20k_f32")
+    rng = np.random.default_rng(9)
+    with cpg_b200.CpGen(division=cpg_b200.DIV_IEEE) as g:
+        g.load_edges(n, src, dst, w)
+        g.levelize()
+        adjp, adj, ww = g.get_csr()
+        ww = ww.copy()
+        for it in range(40):
+            eids = rng.choice(adj.size, size=adj.size // 10, replace=False).astype(np.int32)
+            nw = rng.uniform(0.1, 10.0, size=eids.size).astype(np.float32)
+            ww[eids] = nw
+            g.update_delays(eids, nw)
+            g.levelize()
+        g.report_paths(3000)
+        got = g.get_slacks(3000)
+        d, s, lv = g.get_sfxt()
+    with cpg_b200.CpGen(division=cpg_b200.DIV_IEEE) as h:
+        h.load_csr(n, adjp, adj, ww)
+        h.report_paths(3000)
+        want = h.get_slacks(3000)
+        d2, s2, lv2 = h.get_sfxt()
+    np.testing.assert_array_equal(d, d2)
+    np.testing.assert_array_equal(s, s2)
+    np.testing.assert_array_equal(lv, lv2)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))

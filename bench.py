@@ -287,7 +287,10 @@ def run_ours(args):
                    "parallelism": f"replicas x{world}"},
         "breakdown_ms": {"sfxt": sfxt, "pfxt": pfxt, "select_sort": sel,
                          "phases": stats["phases"], "rounds": stats["rounds"],
-                         "paths_accepted": acc, "items_generated": items},
+                         "paths_accepted": acc, "items_generated": items,
+                         "engine_stages": dict(zip(
+                             ["seed", "decide", "select", "promote", "closure", "out_select",
+                              "out_sort", "emit"], stats["engine_stage_ms"]))},
         "roofline": {"bound": "hbm", "kernel": kern, "achieved": ach, "peak": hbm,
                      "peak_source": src, "unit": "GB/s", "frac": ach / hbm, "traffic": None},
         "e2e": {"value": replica_value(n_out, e2e, world), "unit": "paths/s",

@@ -46,7 +46,8 @@ class Options(C.Structure):
         ("spin_limit", C.c_uint32), ("root_seeding", C.c_int32),
         ("host_stepped", C.c_int32), ("bvss_tiles", C.c_int32),
         ("bvss_min_bits", C.c_int32), ("bvss_min_slices", C.c_int32),
-        ("sfxt_level_sync", C.c_int32), ("reserved", C.c_int32 * 2),
+        ("sfxt_level_sync", C.c_int32), ("sfxt_heap_warps", C.c_int32),
+        ("sfxt_late_push", C.c_int32),
     ]
 
 
@@ -298,7 +299,8 @@ class CpGen:
                  hbm_budget_bytes: int = 0, spin_limit: int = 0,
                  root_seeding: int = ROOTS_REFERENCE, host_stepped: bool = False,
                  bvss_tiles: int = TILES_DENSITY, bvss_min_bits: int = 0,
-                 bvss_min_slices: int = 0, sfxt_level_sync: bool = False):
+                 bvss_min_slices: int = 0, sfxt_level_sync: bool = False,
+                 sfxt_heap_warps: int = 0, sfxt_late_push: bool = False):
         o = Options()
         lib.cpg_options_init(C.byref(o))
         o.device = device
@@ -313,6 +315,8 @@ class CpGen:
         o.bvss_min_bits = bvss_min_bits
         o.bvss_min_slices = bvss_min_slices
         o.sfxt_level_sync = 1 if sfxt_level_sync else 0
+        o.sfxt_heap_warps = sfxt_heap_warps
+        o.sfxt_late_push = 1 if sfxt_late_push else 0
         self._h = C.c_void_p()
         st = lib.cpg_create(C.byref(self._h), C.byref(o))
         if st != CPG_OK:

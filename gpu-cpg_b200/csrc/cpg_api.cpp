@@ -60,7 +60,7 @@ struct cpg_handle {
   bool multi_graph = false;
   std::vector<int32_t> graph_voff;  // first vertex of each graph
   std::vector<int32_t> graph_from;  // per graph: lowest changed level (INT32_MAX: clean)
-  DevMem d_vgraph, d_graph_from, d_upd, d_queue;
+  DevMem d_vgraph, d_graph_from, d_upd, d_queue, d_dl;
   // BVSS form of the fan-out CSR, for the pull Kahn step
   bool use_bvss = false;
   double bvss_bps = 0;  // set bits per slice (sampled, or exact once built)
@@ -253,6 +253,7 @@ Status upload_graph(cpg_handle* h, int32_t n, int32_t m, const int32_t* adjp,
   // suffix tree storage (the deviation array doubles as upload staging)
   CK(ensure(h->d_order, nn * 4), "alloc order");
   CK(ensure(h->d_queue, nn * 4 + 8), "alloc queue");
+  CK(ensure(h->d_dl, nn * 8 + 8), "alloc queue");
   CK(ensure(h->d_lvlp, (nn + 2) * 4), "alloc lvlp");
   CK(ensure(h->d_level_of, nn * 4), "alloc level_of");
   CK(ensure(h->d_dist, nn * 4), "alloc dist");
@@ -264,8 +265,13 @@ Status upload_graph(cpg_handle* h, int32_t n, int32_t m, const int32_t* adjp,
   CK(ensure(h->d_pool_mark, (nn + 2) * 8), "alloc pool_mark");
   CK(ensure(h->d_deps, std::max(nn, build_scratch_words(n)) * 4), "alloc deps");
   CK(ensure(h->d_sctr, sizeof(SfxtCounters)), "alloc sfxt counters");
-  if (h->hnode_cap < nn * 10ull + 1024) {
-    h->hnode_cap = nn * 10ull + 1024;
+  // ~10 path-copied nodes per vertex, plus the warps' private pool chunks
+  // (64 nodes per warp of the dataflow build, 32 warps per SM)
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
+  const unsigned long long want = nn * 10ull + 1024 + 64ull * 32 * static_cast<unsigned>(sms);
+  if (h->hnode_cap < want) {
+    h->hnode_cap = want;
     release(h->d_hnodes);
   }
   CK(ensure(h->d_hnodes, h->hnode_cap * sizeof(HeapNode)), "alloc chain heaps");
@@ -346,6 +352,9 @@ SfxtParams sfxt_params(cpg_handle* h, int32_t start_level) {
   p.grid_limit = h->sfxt_grid_limit;
   p.queue = P<int32_t>(h->d_queue);
   p.level_sync = h->opts.sfxt_level_sync == 1;
+  p.heap_warps = std::min(std::max(h->opts.sfxt_heap_warps, 0), 16);
+  p.early_push = h->opts.sfxt_late_push != 1 && p.heap_warps == 0;
+  p.dl = P<unsigned long long>(h->d_dl);
   if (start_level > 0) {
     // a dataflow build allocates heap nodes out of level order, so rebuilt
     // levels take fresh nodes; a pool overflow falls back to a full build
@@ -999,7 +1008,7 @@ cpg_status cpg_destroy(cpg_handle* h) {
                    &h->d_qids, &h->d_ehist, &h->d_esort, &h->d_equery, &h->d_ectr,
                    &h->d_bv_ptr, &h->d_bv_masks, &h->d_bv_rows, &h->d_bv_cnt,
                    &h->d_bv_deps, &h->d_fbits, &h->d_iact, &h->d_act_list,
-                   &h->d_vgraph, &h->d_graph_from, &h->d_upd, &h->d_queue};
+                   &h->d_vgraph, &h->d_graph_from, &h->d_upd, &h->d_queue, &h->d_dl};
   for (DevMem* b : all) release(*b);
   for (auto& e : h->ev)
     if (e) cudaEventDestroy(e);

@@ -91,19 +91,22 @@ enum DevErr : int {
   kDevCapacity = 2,
 };
 
+// Hot words sit on their own 128-byte lines: queue appends, the heap-pool
+// cursor, the status word that waiting warps poll and the barrier do not
+// contend for one L2 line.
 struct SfxtCounters {
-  int tail;                  // order[] append cursor
+  alignas(128) int tail;     // order[] / queue[] append cursor
   int act_n;                 // BVSS: act_list append cursor
   int level_end;             // tail and act_n snapshots taken at each level
   int act_end;               // barrier (adjacent: one two-word snapshot)
-  int err;
+  alignas(128) int err;
   int levels;
   int sort_beg;              // order[] range whose deviation rows were rebuilt
   int sort_end;
-  unsigned long long hnode_used;
-  unsigned long long vss_tensor;  // BVSS tiles counted on the tensor cores
-  unsigned long long vss_scalar;  // ... and with scalar popc
-  GridBarrier bar;
+  alignas(128) unsigned long long hnode_used;
+  alignas(128) unsigned long long vss_tensor;  // BVSS tiles counted on the tensor cores
+  unsigned long long vss_scalar;               // ... and with scalar popc
+  alignas(128) GridBarrier bar;
 };
 
 struct SfxtParams {
@@ -145,6 +148,9 @@ struct SfxtParams {
   // full CSR builds: dataflow work queue (n ints) unless level_sync is set
   int32_t* queue;
   int32_t level_sync;
+  int32_t heap_warps;      // dataflow: warps per CTA that only insert heaps (0: none)
+  int32_t early_push;      // dataflow: push tails before the build, poll dl[]
+  unsigned long long* dl;  // dataflow: published (level << 32 | dist) per vertex
   // BVSS pull for the Kahn step of a full build; used when bvss != 0
   int32_t bvss;
   const int32_t* bv_ptr;       // VSS range of each interval of 8 vertices

@@ -51,10 +51,15 @@ __device__ __forceinline__ int cand_dist(int dh, float w) {
   return static_cast<int>(static_cast<unsigned>(dh) + static_cast<unsigned>(fixed_delay(w)));
 }
 
-__device__ void build_vertex(const SfxtParams& p, int v, int lvl, bool do_kahn) {
+// kLevel (dataflow build): the level is not known in advance; it is one
+// more than the heads' highest level (0 for a sink), read with their
+// distances, and written to level_of[v].  Returns the level.
+template <bool kLevel = false>
+__device__ int build_vertex(const SfxtParams& p, int v, int lvl, bool do_kahn) {
   const int lane = threadIdx.x & 31;
   const int rb = p.adjp[v];
   const int re = p.adjp[v + 1];
+  if (kLevel) lvl = re == rb ? 0 : 1;  // the exact value follows; only 0 matters below
   int best = INT_MAX;
   int s = -1;
   int cnt = 0;
@@ -74,6 +79,13 @@ __device__ void build_vertex(const SfxtParams& p, int v, int lvl, bool do_kahn) 
     }
 #pragma unroll
     for (int c = 0; c < kRegChunks; ++c) dh[c] = ed[c].head >= 0 ? __ldcg(p.dist + ed[c].head) : INT_MAX;
+    if (kLevel) {
+      int lmax = -1;
+#pragma unroll
+      for (int c = 0; c < kRegChunks; ++c)
+        if (ed[c].head >= 0) lmax = max(lmax, __ldcg(p.level_of + ed[c].head));
+      lvl = warp_max_i(lmax) + 1;
+    }
     if (lvl == 0) {
       best = 0;  // sinks (out-degree 0) start at distance 0 (gpucpg.cu:17034-17038)
     } else {
@@ -106,6 +118,11 @@ __device__ void build_vertex(const SfxtParams& p, int v, int lvl, bool do_kahn) 
     }
   } else {
     // long rows (a super-source, say): chunk by chunk
+    if (kLevel) {
+      int lmax = -1;
+      for (int e = rb + lane; e < re; e += 32) lmax = max(lmax, __ldcg(p.level_of + p.edges[e].head));
+      lvl = warp_max_i(lmax) + 1;
+    }
     if (lvl == 0) {
       best = 0;
     } else {
@@ -151,6 +168,7 @@ __device__ void build_vertex(const SfxtParams& p, int v, int lvl, bool do_kahn) 
     // carries the cheapest deviation key to the chain-heap insert, which runs
     // one level later, off this level's critical path
     p.deps[v] = __float_as_int(kmin);
+    if (kLevel) p.level_of[v] = lvl;
   }
 
   if (do_kahn) {
@@ -179,6 +197,7 @@ __device__ void build_vertex(const SfxtParams& p, int v, int lvl, bool do_kahn) 
       }
     }
   }
+  return lvl;
 }
 
 // Whether an incremental build rebuilds v (at level lvl).
@@ -203,8 +222,32 @@ __device__ __forceinline__ void heap_store(const SfxtParams& p, int v, int root,
   }
 }
 
+// Heap nodes for one insert: from the global cursor, or (chunk != nullptr)
+// from the calling thread's private chunk of the pool, refilled 64 nodes at
+// a time, so concurrent inserts neither contend for the cursor nor share
+// cache lines.  Returns ~0 when the pool is exhausted.
+constexpr unsigned kHeapChunk = 64;
+
+__device__ __forceinline__ unsigned long long heap_alloc(const SfxtParams& p, unsigned need,
+                                                         unsigned long long* chunk) {
+  if (!chunk) {
+    const unsigned long long a = atomicAdd(&p.ctr->hnode_used, static_cast<unsigned long long>(need));
+    return a + need > p.hnode_cap ? ~0ull : a;
+  }
+  if (chunk[0] + need > chunk[1]) {
+    const unsigned grab = need > kHeapChunk ? need : kHeapChunk;
+    const unsigned long long a = atomicAdd(&p.ctr->hnode_used, static_cast<unsigned long long>(grab));
+    if (a + grab > p.hnode_cap) return ~0ull;
+    chunk[0] = a;
+    chunk[1] = a + grab;
+  }
+  const unsigned long long a = chunk[0];
+  chunk[0] += need;
+  return a;
+}
+
 template <bool kPublish = false>
-__device__ void heap_insert(const SfxtParams& p, int v) {
+__device__ void heap_insert(const SfxtParams& p, int v, unsigned long long* chunk = nullptr) {
   const int s = __ldcg(p.succ + v);
   const int cnt = __ldcg(p.dev_cnt + v);
   const int base_root = s >= 0 ? __ldcg(p.ht_root + s) : -1;
@@ -216,9 +259,8 @@ __device__ void heap_insert(const SfxtParams& p, int v) {
   const float kmin = __int_as_float(__ldcg(p.deps + v));
   const unsigned pos = static_cast<unsigned>(base_size) + 1u;
   const int depth = 31 - __clz(pos);
-  const unsigned long long a =
-      atomicAdd(&p.ctr->hnode_used, static_cast<unsigned long long>(depth + 1));
-  if (a + depth + 1 > p.hnode_cap) {
+  const unsigned long long a = heap_alloc(p, static_cast<unsigned>(depth + 1), chunk);
+  if (a == ~0ull) {
     atomicCAS(&p.ctr->err, kDevOk, kDevCapacity);
     heap_store<kPublish>(p, v, -1, 0);
     return;
@@ -450,7 +492,8 @@ __device__ __forceinline__ int wait_slot(const SfxtParams& p, int s) {
     unsigned int it = 0;
     const volatile int* q = p.queue + s;
     while ((v = *q) < 0) {
-      if (++it > p.spin_limit || *reinterpret_cast<volatile int*>(&p.ctr->err) != kDevOk) {
+      if (++it > p.spin_limit ||
+          ((it & 31) == 0 && *reinterpret_cast<volatile int*>(&p.ctr->err) != kDevOk)) {
         atomicCAS(&p.ctr->err, kDevOk, kDevTimeout);
         break;
       }
@@ -466,7 +509,8 @@ __device__ __forceinline__ bool wait_heap(const SfxtParams& p, int s) {
   unsigned int it = 0;
   const volatile int* hs = p.ht_size + s;
   while (*hs < 0) {
-    if (++it > p.spin_limit || *reinterpret_cast<volatile int*>(&p.ctr->err) != kDevOk) {
+    if (++it > p.spin_limit ||
+        ((it & 31) == 0 && *reinterpret_cast<volatile int*>(&p.ctr->err) != kDevOk)) {
       atomicCAS(&p.ctr->err, kDevOk, kDevTimeout);
       return false;
     }
@@ -476,9 +520,208 @@ __device__ __forceinline__ bool wait_heap(const SfxtParams& p, int s) {
   return true;
 }
 
-// Kahn step of the dataflow build: raise the tails' levels, then take one
-// pending fan-out off each; tails reaching zero are queued.
-__device__ __forceinline__ void dataflow_push(const SfxtParams& p, int v, int lvl) {
+// Early-push build of v: v's tails were decremented when v was taken, so a
+// head may still be building; each head's (dist, level) word dl[] is polled
+// until it is published (not ~0).  Same results as build_vertex.  Returns
+// v's level, or -1 if a wait ran out (warp-uniform).
+__device__ __forceinline__ unsigned long long ld_dl(const SfxtParams& p, int h) {
+  return *reinterpret_cast<const volatile unsigned long long*>(p.dl + h);
+}
+
+__device__ int build_vertex_polled(const SfxtParams& p, int v) {
+  const int lane = threadIdx.x & 31;
+  const int rb = p.adjp[v];
+  const int re = p.adjp[v + 1];
+  int best = INT_MAX;
+  int s = -1;
+  int cnt = 0;
+  int lmax = -1;
+  float kmin = __int_as_float(0x7f800000);  // +inf
+  constexpr unsigned long long kNone = ~0ull;
+  if (re - rb <= kRegChunks * 32) {
+    DevEdge ed[kRegChunks];
+    int dh[kRegChunks];
+#pragma unroll
+    for (int c = 0; c < kRegChunks; ++c) {
+      const int e = rb + c * 32 + lane;
+      ed[c].head = -1;
+      ed[c].w = 0.f;
+      if (e < re) ed[c] = p.edges[e];
+    }
+    unsigned pending = 0;
+#pragma unroll
+    for (int c = 0; c < kRegChunks; ++c) {
+      dh[c] = INT_MAX;
+      if (ed[c].head >= 0) {
+        const unsigned long long x = ld_dl(p, ed[c].head);
+        if (x == kNone) {
+          pending |= 1u << c;
+        } else {
+          dh[c] = static_cast<int>(x & 0xffffffffu);
+          lmax = max(lmax, static_cast<int>(x >> 32));
+        }
+      }
+    }
+    unsigned int it = 0;
+    while (__any_sync(0xffffffffu, pending != 0)) {
+      // the lanes may read err differently: decide for the whole warp
+      ++it;
+      const bool bail = __any_sync(0xffffffffu, it > p.spin_limit ||
+                                   ((it & 31) == 0 &&
+                                    *reinterpret_cast<volatile int*>(&p.ctr->err) != kDevOk));
+      if (bail) {
+        if (lane == 0) atomicCAS(&p.ctr->err, kDevOk, kDevTimeout);
+        return -1;
+      }
+      __nanosleep(32);
+#pragma unroll
+      for (int c = 0; c < kRegChunks; ++c) {
+        if (pending & (1u << c)) {
+          const unsigned long long x = ld_dl(p, ed[c].head);
+          if (x != kNone) {
+            dh[c] = static_cast<int>(x & 0xffffffffu);
+            lmax = max(lmax, static_cast<int>(x >> 32));
+            pending &= ~(1u << c);
+          }
+        }
+      }
+    }
+    const int lvl = warp_max_i(lmax) + 1;
+    if (lvl == 0) {
+      best = 0;  // a sink
+    } else {
+#pragma unroll
+      for (int c = 0; c < kRegChunks; ++c)
+        if (ed[c].head >= 0) best = min(best, cand_dist(dh[c], ed[c].w));
+      best = warp_min_i(best);
+#pragma unroll
+      for (int c = 0; c < kRegChunks; ++c)
+        if (ed[c].head >= 0 && cand_dist(dh[c], ed[c].w) == best) s = max(s, ed[c].head);
+      s = warp_max_i(s);
+    }
+#pragma unroll
+    for (int c = 0; c < kRegChunks; ++c) {
+      if (rb + c * 32 >= re) break;
+      const bool valid = ed[c].head >= 0 && ed[c].head != s && dh[c] != INT_MAX;
+      const unsigned bal = __ballot_sync(0xffffffffu, valid);
+      if (valid) {
+        DevSidetrack rec;
+        rec.head = ed[c].head;
+        rec.w = ed[c].w;
+        rec.dist_head = dh[c];
+        rec.key = deviation_key(dh[c], best, ed[c].w);
+        p.dev[rb + cnt + __popc(bal & lanemask_lt())] = rec;
+        kmin = fminf(kmin, rec.key);
+      }
+      cnt += __popc(bal);
+    }
+    lmax = lvl;
+  } else {
+    // long rows: wait for every head once, then read the distances plainly
+    bool ok = true;
+    for (int e = rb + lane; e < re && ok; e += 32) {
+      const int h = p.edges[e].head;
+      unsigned int it = 0;
+      unsigned long long x;
+      while ((x = ld_dl(p, h)) == kNone) {
+        if (++it > p.spin_limit ||
+          ((it & 31) == 0 && *reinterpret_cast<volatile int*>(&p.ctr->err) != kDevOk)) {
+          atomicCAS(&p.ctr->err, kDevOk, kDevTimeout);
+          ok = false;
+          break;
+        }
+        __nanosleep(32);
+      }
+      if (ok) lmax = max(lmax, static_cast<int>(x >> 32));
+    }
+    if (!__all_sync(0xffffffffu, ok)) return -1;
+    __threadfence();  // acquire: the heads' dist[] words
+    const int lvl = warp_max_i(lmax) + 1;
+    for (int e = rb + lane; e < re; e += 32) {
+      const DevEdge ed = p.edges[e];
+      best = min(best, cand_dist(__ldcg(p.dist + ed.head), ed.w));
+    }
+    best = warp_min_i(best);
+    for (int e = rb + lane; e < re; e += 32) {
+      const DevEdge ed = p.edges[e];
+      if (cand_dist(__ldcg(p.dist + ed.head), ed.w) == best) s = max(s, ed.head);
+    }
+    s = warp_max_i(s);
+    for (int base = rb; base < re; base += 32) {
+      const int e = base + lane;
+      bool valid = false;
+      DevSidetrack rec;
+      if (e < re) {
+        const DevEdge ed = p.edges[e];
+        const int dh = __ldcg(p.dist + ed.head);
+        valid = ed.head != s && dh != INT_MAX;
+        rec.head = ed.head;
+        rec.w = ed.w;
+        rec.dist_head = dh;
+        rec.key = deviation_key(dh, best, ed.w);
+      }
+      const unsigned bal = __ballot_sync(0xffffffffu, valid);
+      if (valid) {
+        p.dev[rb + cnt + __popc(bal & lanemask_lt())] = rec;
+        kmin = fminf(kmin, rec.key);
+      }
+      cnt += __popc(bal);
+    }
+    lmax = lvl;
+  }
+  for (int o = 16; o > 0; o >>= 1) kmin = fminf(kmin, __shfl_xor_sync(0xffffffffu, kmin, o));
+  if (lane == 0) {
+    p.dist[v] = best;
+    p.succ[v] = s;
+    p.dev_cnt[v] = cnt;
+    p.deps[v] = __float_as_int(kmin);
+    p.level_of[v] = lmax;
+    __threadfence();  // release: dist / succ / level before the published word
+    *reinterpret_cast<volatile unsigned long long*>(p.dl + v) =
+        (static_cast<unsigned long long>(static_cast<unsigned>(lmax)) << 32) |
+        static_cast<unsigned>(best);
+  }
+  return lmax;
+}
+
+// A lane-granular wait for queue slot s (the heap workers).
+__device__ __forceinline__ int wait_slot_lane(const SfxtParams& p, int s) {
+  unsigned int it = 0;
+  const volatile int* q = p.queue + s;
+  int v;
+  while ((v = *q) < 0) {
+    if (++it > p.spin_limit ||
+        ((it & 31) == 0 && *reinterpret_cast<volatile int*>(&p.ctr->err) != kDevOk)) {
+      atomicCAS(&p.ctr->err, kDevOk, kDevTimeout);
+      return -1;
+    }
+    __nanosleep(32);
+  }
+  __threadfence();
+  return v;
+}
+
+// Wait until a vertex's build is published (its flag in order[] is set).
+__device__ __forceinline__ bool wait_built(const SfxtParams& p, int v) {
+  unsigned int it = 0;
+  const volatile int* f = p.order + v;
+  while (*f == 0) {
+    if (++it > p.spin_limit ||
+        ((it & 31) == 0 && *reinterpret_cast<volatile int*>(&p.ctr->err) != kDevOk)) {
+      atomicCAS(&p.ctr->err, kDevOk, kDevTimeout);
+      return false;
+    }
+    __nanosleep(32);
+  }
+  __threadfence();
+  return true;
+}
+
+// Kahn step of the dataflow build: take one pending fan-out off each tail;
+// tails reaching zero are queued.  kRelease: v's build precedes the push and
+// is published by it (late push); an early push publishes nothing.
+template <bool kRelease>
+__device__ __forceinline__ void dataflow_push(const SfxtParams& p, int v) {
   const int lane = threadIdx.x & 31;
   const int ib = p.iadjp[v];
   const int ie = p.iadjp[v + 1];
@@ -490,13 +733,10 @@ __device__ __forceinline__ void dataflow_push(const SfxtParams& p, int v, int lv
       const int e = base + c * 32 + lane;
       u[c] = e < ie ? p.iadj[e] : -1;
     }
-#pragma unroll
-    for (int c = 0; c < 4; ++c)
-      if (u[c] >= 0) atomicMax(p.level_of + u[c], lvl + 1);
-    __threadfence();  // release: v's dist and the levels before the counts
+    if (kRelease) __threadfence();  // release: v's dist and level before the counts
 #pragma unroll
     for (int c = 0; c < 4; ++c) ready[c] = u[c] >= 0 && atomicSub(&p.deps[u[c]], 1) == 1;
-    __threadfence();
+    if (kRelease) __threadfence();
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
       const int slot = warp_append(&p.ctr->tail, ready[c]);
@@ -509,8 +749,6 @@ __global__ void __launch_bounds__(kSfxtThreads)
 sfxt_dataflow_kernel(SfxtParams p) {
   __shared__ int s_hist[kSfxtThreads];
   const int lane = threadIdx.x & 31;
-  const int gwarp = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  const int nwarps = gridDim.x * (blockDim.x >> 5);
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   const int nth = gridDim.x * blockDim.x;
   // phase 0: reset, clear the queue and the level histogram
@@ -523,6 +761,8 @@ sfxt_dataflow_kernel(SfxtParams p) {
     p.ht_size[v] = -1;  // heap not built yet
     p.level_of[v] = 0;
     p.queue[v] = -1;
+    p.order[v] = 0;  // build-published flags until the final level sort
+    p.dl[v] = ~0ull;  // (dist, level) not published yet
   }
   for (int i = tid; i < p.n + 2; i += nth) p.lvlp[i] = 0;
   if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit)) return;
@@ -533,17 +773,51 @@ sfxt_dataflow_kernel(SfxtParams p) {
     const int slot = warp_append(&p.ctr->tail, sink);
     if (sink) *reinterpret_cast<volatile int*>(p.queue + slot) = v;
   }
+  // the last kHeapWarps warps of each CTA insert chain heaps, one vertex per
+  // lane, in queue order; the others build.  A build never waits on a heap.
   int max_lvl = -1;
-  for (int s = gwarp; s < p.n; s += nwarps) {
-    const int v = wait_slot(p, s);
-    if (v < 0) break;
-    const int lvl = __ldcg(p.level_of + v);
-    max_lvl = max(max_lvl, lvl);
-    build_vertex(p, v, lvl, false);
-    __syncwarp();
-    dataflow_push(p, v, lvl);
-    if (lane == 0 && wait_heap(p, __ldcg(p.succ + v))) heap_insert<true>(p, v);
-    __syncwarp();
+  const int wib = threadIdx.x >> 5;
+  // each warp's private share of the heap pool (used by its lane 0)
+  __shared__ unsigned long long s_chunk[kSfxtThreads / 32][2];
+  unsigned long long* chunk = s_chunk[wib];
+  if (lane == 0) chunk[0] = chunk[1] = 0;
+  __syncwarp();
+  const int heap_warps = p.heap_warps;  // 0: the build warp inserts the heap itself
+  const int build_warps = kSfxtThreads / 32 - heap_warps;
+  if (wib < build_warps) {
+    const int nbw = gridDim.x * build_warps;
+    for (int s = blockIdx.x * build_warps + wib; s < p.n; s += nbw) {
+      const int v = wait_slot(p, s);
+      if (v < 0) break;
+      if (p.early_push) {
+        // the tails learn of v before it is built; they wait on its word
+        dataflow_push<false>(p, v);
+        const int lvl = build_vertex_polled(p, v);
+        if (lvl < 0) break;
+        max_lvl = max(max_lvl, lvl);
+        if (lane == 0 && wait_heap(p, __ldcg(p.succ + v))) heap_insert<true>(p, v, chunk);
+        __syncwarp();
+        continue;
+      }
+      const int lvl = build_vertex<true>(p, v, 0, false);
+      max_lvl = max(max_lvl, lvl);
+      __syncwarp();
+      if (heap_warps > 0 && lane == 0) {  // publish the build for the heap workers
+        __threadfence();
+        *reinterpret_cast<volatile int*>(p.order + v) = 1;
+      }
+      dataflow_push<true>(p, v);
+      if (heap_warps == 0 && lane == 0 && wait_heap(p, __ldcg(p.succ + v)))
+        heap_insert<true>(p, v, chunk);
+      __syncwarp();
+    }
+  } else {
+    const int nhl = gridDim.x * heap_warps * 32;
+    for (int s = (blockIdx.x * heap_warps + (wib - build_warps)) * 32 + lane; s < p.n; s += nhl) {
+      const int v = wait_slot_lane(p, s);
+      if (v < 0 || !wait_built(p, v) || !wait_heap(p, __ldcg(p.succ + v))) break;
+      heap_insert<true>(p, v);
+    }
   }
   if (lane == 0) atomicMax(&p.ctr->levels, max_lvl + 1);
   if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit)) return;

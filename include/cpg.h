@@ -91,7 +91,11 @@ typedef struct {
   int32_t sfxt_level_sync;  /* 1: full suffix-tree builds step level by level
                                with a grid barrier per level instead of the
                                dataflow work queue; for A/B checks */
-  int32_t reserved[2];
+  int32_t sfxt_heap_warps;  /* dataflow build: warps per CTA (of 32) that only
+                               insert chain heaps; 0 = the building warp does */
+  int32_t sfxt_late_push;   /* dataflow build: 1 = a vertex's tails are
+                               decremented after it is built instead of when
+                               it is taken (A/B checks) */
 } cpg_options;
 
 typedef struct cpg_handle cpg_handle;

@@ -336,14 +336,15 @@ struct EngineQuery {
 };
 
 struct EngineCounters {
-  int err;
+  alignas(128) int err;
   int active;
   int sel_paths;              // some query selects over accepted paths
   int pad0;
-  unsigned long long paths;
-  unsigned long long frontier[3];
-  unsigned long long pend_out;
-  unsigned long long out_total;
+  // append cursors, each on its own 128-byte line
+  alignas(128) unsigned long long paths;
+  alignas(128) unsigned long long frontier[3];
+  alignas(128) unsigned long long pend_out;
+  alignas(128) unsigned long long out_total;
   int rounds;
   int phases;
   int sorted_buf;             // which vals[] holds the sorted path indices
@@ -351,7 +352,7 @@ struct EngineCounters {
   // device time per stage (ns): 0 seed, 1 decide/bookkeeping, 2 select,
   // 3 promote, 4 closure, 5 output select, 6 output sort, 7 emit
   unsigned long long t_ns[8];
-  GridBarrier bar;
+  alignas(128) GridBarrier bar;
 };
 
 struct EngineParams {

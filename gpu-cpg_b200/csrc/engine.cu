@@ -309,6 +309,23 @@ __device__ bool run_select(const EngineParams& p, unsigned long long n_paths,
 }
 
 // ------------------------------------------------------------------ closure
+// One reservation per warp for n items per lane (all lanes call): returns
+// this lane's first slot.
+__device__ __forceinline__ unsigned long long warp_reserve(unsigned long long* ctr, unsigned n) {
+  const int lane = threadIdx.x & 31;
+  unsigned incl = n;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  const unsigned tot = __shfl_sync(0xffffffffu, incl, 31);
+  unsigned long long base = 0;
+  if (lane == 31 && tot) base = atomicAdd(ctr, static_cast<unsigned long long>(tot));
+  base = __shfl_sync(0xffffffffu, base, 31);
+  return base + (incl - n);
+}
+
 // Route one candidate (all lanes call): cost <= lim joins the next round's
 // frontier, the rest the next phase's pending pile.  Returns 1 if deferred.
 __device__ __forceinline__ int route(const EngineParams& p, Item* out,
@@ -334,6 +351,8 @@ __device__ bool run_closure(const EngineParams& p, Item* pend_out) {
   const unsigned long long tid =
       static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   const unsigned long long nth = static_cast<unsigned long long>(gridDim.x) * blockDim.x;
+  const bool single = p.nq == 1;
+  unsigned acc_nz = 0, acc_pn = 0, acc_pnz = 0;
   int r = 0;
   for (;;) {
     volatile unsigned long long* fc = p.ctr->frontier;
@@ -391,62 +410,73 @@ __device__ bool run_closure(const EngineParams& p, Item* pend_out) {
           atomicCAS(&p.ctr->err, kDevOk, kDevCapacity);
         }
       }
-      qadd(p.q, QOFF(paths_nz), stored && it.cost != 0.0f, q, 1u);
+      if (single) acc_nz += stored && it.cost != 0.0f;
+      else qadd(p.q, QOFF(paths_nz), stored && it.cost != 0.0f, q, 1u);
       // a path costing exactly the final split is reported, not expanded
       const bool expand = stored && !(it.cost == tie);
-      unsigned ndef = 0, ndef_nz = 0;
       const bool sib = expand && it.node >= 0;
       const float pcost = sib ? __ldcg(p.ps.cost + it.parent) : 0.f;
-      {
-        Item c;
-        c.parent = it.parent;
-        int cn, cj;
-        bool ex;
-        cn = jj == 0 ? hn.left : it.node;
-        cj = jj == 0 ? 0 : 2 * jj + 1;
-        ex = sib && make_candidate(p.g, cn, cj, pcost, c.cost);
-        c.node = cn;
-        c.j = pack_j(q, cj);
-        if (route(p, out, out_cnt, pend_out, ex, c, lim)) {
-          ++ndef;
-          ndef_nz += c.cost != 0.0f;
-        }
-        cn = jj == 0 ? hn.right : it.node;
-        cj = jj == 0 ? 0 : 2 * jj + 2;
-        ex = sib && make_candidate(p.g, cn, cj, pcost, c.cost);
-        c.node = cn;
-        c.j = pack_j(q, cj);
-        if (route(p, out, out_cnt, pend_out, ex, c, lim)) {
-          ++ndef;
-          ndef_nz += c.cost != 0.0f;
-        }
-        ex = sib && jj == 0 && make_candidate(p.g, it.node, 1, pcost, c.cost);
-        c.node = it.node;
-        c.j = pack_j(q, 1);
-        if (route(p, out, out_cnt, pend_out, ex, c, lim)) {
-          ++ndef;
-          ndef_nz += c.cost != 0.0f;
-        }
-        ex = sib && jj == 0 && make_candidate(p.g, it.node, 2, pcost, c.cost);
-        c.j = pack_j(q, 2);
-        if (route(p, out, out_cnt, pend_out, ex, c, lim)) {
-          ++ndef;
-          ndef_nz += c.cost != 0.0f;
+      // the (up to) five children: heap left / right (or row 2j+1 / 2j+2),
+      // row entries 1 and 2 of a heap node's row, and the cross child
+      const int cross = expand ? __ldg(p.g.ht_root + to) : -1;
+      float cc[5];
+      unsigned exm = 0;
+      if (sib && make_candidate(p.g, jj == 0 ? hn.left : it.node, jj == 0 ? 0 : 2 * jj + 1,
+                                pcost, cc[0])) exm |= 1u;
+      if (sib && make_candidate(p.g, jj == 0 ? hn.right : it.node, jj == 0 ? 0 : 2 * jj + 2,
+                                pcost, cc[1])) exm |= 2u;
+      if (sib && jj == 0 && make_candidate(p.g, it.node, 1, pcost, cc[2])) exm |= 4u;
+      if (sib && jj == 0 && make_candidate(p.g, it.node, 2, pcost, cc[3])) exm |= 8u;
+      if (expand && make_candidate(p.g, cross, 0, it.cost, cc[4])) exm |= 16u;
+      unsigned tm = 0, dm = 0, dnz = 0;
+#pragma unroll
+      for (int k = 0; k < 5; ++k) {
+        if (!(exm & (1u << k))) continue;
+        if (cc[k] <= lim) tm |= 1u << k;
+        else {
+          dm |= 1u << k;
+          dnz += cc[k] != 0.0f;
         }
       }
-      {
+      // one reservation per warp and counter for all five
+      unsigned long long bt = warp_reserve(out_cnt, __popc(tm));
+      unsigned long long bd = warp_reserve(&p.ctr->pend_out, __popc(dm));
+#pragma unroll
+      for (int k = 0; k < 5; ++k) {
+        const unsigned bit = 1u << k;
+        if (!((tm | dm) & bit)) continue;
         Item c;
-        c.parent = static_cast<int>(qp);
-        c.node = expand ? __ldg(p.g.ht_root + to) : -1;
-        c.j = pack_j(q, 0);
-        const bool ex = expand && make_candidate(p.g, c.node, 0, it.cost, c.cost);
-        if (route(p, out, out_cnt, pend_out, ex, c, lim)) {
-          ++ndef;
-          ndef_nz += c.cost != 0.0f;
+        c.cost = cc[k];
+        c.parent = k == 4 ? static_cast<int>(qp) : it.parent;
+        const int cn = k == 4 ? cross : (k < 2 && jj == 0 ? (k == 0 ? hn.left : hn.right) : it.node);
+        const int cj = k == 4 ? 0 : k == 2 ? 1 : k == 3 ? 2 : (jj == 0 ? 0 : 2 * jj + 1 + k);
+        c.node = cn;
+        c.j = pack_j(q, cj);
+        if (tm & bit) {
+          if (bt < p.front_cap) out[bt] = c;
+          else atomicCAS(&p.ctr->err, kDevOk, kDevCapacity);
+          ++bt;
+        } else {
+          if (bd < p.pend_cap) pend_out[bd] = c;
+          else atomicCAS(&p.ctr->err, kDevOk, kDevCapacity);
+          ++bd;
         }
       }
-      qadd(p.q, QOFF(pend_next_n), valid, q, ndef);
-      qadd(p.q, QOFF(pend_next_nz), valid, q, ndef_nz);
+      const unsigned ndef = __popc(dm), ndef_nz = dnz;
+      if (single) {
+        acc_pn += ndef;
+        acc_pnz += ndef_nz;
+      } else {
+        qadd(p.q, QOFF(pend_next_n), valid, q, ndef);
+        qadd(p.q, QOFF(pend_next_nz), valid, q, ndef_nz);
+      }
+    }
+    if (single) {
+      // one query: counts kept per thread through the round, added once
+      qadd(p.q, QOFF(paths_nz), acc_nz != 0, 0u, acc_nz);
+      qadd(p.q, QOFF(pend_next_n), acc_pn != 0, 0u, acc_pn);
+      qadd(p.q, QOFF(pend_next_nz), acc_pnz != 0, 0u, acc_pnz);
+      acc_nz = acc_pn = acc_pnz = 0;
     }
     if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit)) return false;
     ++r;
@@ -645,6 +675,8 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
     // E. promote pending items under their query's limit
     {
       const unsigned long long pad = (n_pend + 31) & ~31ull;
+      const bool single = p.nq == 1;
+      unsigned acc_n = 0, acc_nz = 0;
       for (unsigned long long i = tid; i < pad; i += nth) {
         bool take = false, keep = false;
         Item it;
@@ -668,8 +700,17 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
           if (b < p.pend_cap) pend_next[b] = it;
           else atomicCAS(&p.ctr->err, kDevOk, kDevCapacity);
         }
-        qadd(p.q, QOFF(pend_next_n), keep, q_of(it), 1u);
-        qadd(p.q, QOFF(pend_next_nz), keep && it.cost != 0.0f, q_of(it), 1u);
+        if (single) {
+          acc_n += keep;
+          acc_nz += keep && it.cost != 0.0f;
+        } else {
+          qadd(p.q, QOFF(pend_next_n), keep, q_of(it), 1u);
+          qadd(p.q, QOFF(pend_next_nz), keep && it.cost != 0.0f, q_of(it), 1u);
+        }
+      }
+      if (single) {
+        qadd(p.q, QOFF(pend_next_n), acc_n != 0, 0u, acc_n);
+        qadd(p.q, QOFF(pend_next_nz), acc_nz != 0, 0u, acc_nz);
       }
     }
     ENG_SYNC();

@@ -835,6 +835,7 @@ Status engine_enqueue(cpg_handle* h, int nq, unsigned long long k_total) {
   p.ctr = P<EngineCounters>(h->d_ectr);
   p.spin_limit = h->opts.spin_limit ? h->opts.spin_limit : kDefaultSpinLimit;
   p.grid_limit = h->engine_grid_limit;
+  p.grow_cap_k = 1;
   if (h->sel_schedule == 1) {  // four 8-bit digits
     p.sel_passes = 4;
     for (int i = 0; i < 4; ++i) {

@@ -333,6 +333,7 @@ struct EngineQuery {
   unsigned long long k_out, out_off, out_lt, out_eq;
   int phases;
   int pad;
+  unsigned long long acc_prev, last_j;  // accepted before / promoted in the last growth phase
 };
 
 struct EngineCounters {
@@ -380,6 +381,7 @@ struct EngineParams {
   EngineCounters* ctr;
   unsigned int spin_limit;
   int grid_limit;             // persistent CTAs (0: one per co-resident slot)
+  int grow_cap_k;             // cap a growth phase's promotion at K - accepted
   int sel_passes;             // radix select digit schedule (sum of bits 32)
   int sel_shift[4];
   int sel_bits[4];

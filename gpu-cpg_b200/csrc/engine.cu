@@ -245,7 +245,8 @@ __device__ void select_hist(const EngineParams& p, unsigned long long n_paths,
     }
     const unsigned bin = (key >> shift) & ((1u << bits) - 1u);
     if (single) {
-      if (on) atomicAdd(&sh[bin], 1u);
+      // costs cluster, so many lanes share a bin: one add per distinct bin
+      agg_add_u32(sh, on, bin);
     } else {
       agg_add_u32(p.hist, on, q * kSelBins + bin);
     }
@@ -629,9 +630,28 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
         // closure is exponentially large (measured: a 3/4 cap accepted 77x
         // the paths needed)
         unsigned long long j = 4 * (Q.paths_nz + 1);
+        // Near K, aim at K: every promoted item is accepted with its closure
+        // below the split, and the last growth phase showed how many paths
+        // one promoted item brings.  Promote the missing paths over that
+        // ratio (with 20% to spare), so the phase that reaches K overshoots
+        // little; falling short costs one more phase, which is only worth
+        // risking when the overshoot would be large (an extra phase costs
+        // about as much as closing ~1e5 more paths).
+        if (p.grow_cap_k && static_cast<unsigned long long>(Q.k) - Q.paths_nz >= (1ull << 17)) {
+          const unsigned long long miss = static_cast<unsigned long long>(Q.k) - Q.paths_nz;
+          unsigned long long aim = miss;
+          if (Q.last_j > 0 && Q.paths_nz > Q.acc_prev) {
+            const double ratio = static_cast<double>(Q.paths_nz - Q.acc_prev) /
+                                 static_cast<double>(Q.last_j);
+            if (ratio > 1.0) aim = static_cast<unsigned long long>(1.2 * miss / ratio) + 64;
+          }
+          if (j > aim) j = aim;
+        }
         if (j < 64) j = 64;
         const unsigned long long half = (Q.pend_n + 1) / 2;
         if (j > half) j = half;
+        Q.acc_prev = Q.paths_nz;
+        Q.last_j = j;
         Q.krem = j;
         Q.ksel = j;
       } else {

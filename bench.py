@@ -38,6 +38,10 @@ WORKLOAD = "large1m_f32"
 WORKLOAD_DESC = ("levelised DAG, 1,000,000 pins / 200 levels, geometric out-degree mean 20 "
                  "(cap 256), fp32 delays U[0.1,10], 2,000 sources / 2,000 sinks, K=1e6")
 METRIC = "K-paths/sec"
+# DRAM bytes (read + write) per launch from the ncu capture summarised in
+# profiles/ (the suffix-tree build does not depend on K); engine traffic
+# depends on K and is not scaled here.
+KERNEL_TRAFFIC = {"sfxt_dataflow_kernel": 1_249_005_824}  # profiles/sfxt_dataflow_kernel_large1m.md
 
 
 def peaks():
@@ -223,12 +227,13 @@ def run_ours(args):
     clocks.start()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
-    sfxt_ms, pfxt_ms, sel_ms, launches = [], [], [], 0
+    sfxt_ms, sfxt_k_ms, pfxt_ms, sel_ms, launches = [], [], [], [], 0
     ev0.record(stream)
     for _ in range(args.steps):
         step()
         s = g.stats()
         sfxt_ms.append(s["sfxt_ms"])
+        sfxt_k_ms.append(s["sfxt_kernel_ms"])
         pfxt_ms.append(s["pfxt_ms"])
         sel_ms.append(s["select_ms"])
         launches += s["kernel_launches"]
@@ -265,16 +270,20 @@ def run_ours(args):
     # ---- roofline of the dominant kernel
     hbm, src = peaks()
     sfxt = float(np.mean(sfxt_ms))
+    sfxt_k = float(np.mean(sfxt_k_ms))
     pfxt = float(np.mean(pfxt_ms))
     sel = float(np.mean(sel_ms))
     b_sfxt = 36 * M + 32 * N            # algorithmic bytes of one suffix-tree build
     acc = stats["paths_accepted"]
     items = stats["items_generated"]
     b_pfxt = 16 * acc + 20 * acc + 16 * items + 36 * items
-    if sfxt >= pfxt:
-        kern, ach = "sfxt_persistent_kernel", b_sfxt / (sfxt * 1e-3) / 1e9
+    # the dominant kernel's average launch, timed with CUDA events on the
+    # handle's stream around that launch alone
+    if sfxt_k >= pfxt:
+        kern, ach, k_ms = "sfxt_dataflow_kernel", b_sfxt / (sfxt_k * 1e-3) / 1e9, sfxt_k
     else:
-        kern, ach = "closure_kernel (+promote/select)", b_pfxt / (pfxt * 1e-3) / 1e9
+        kern, ach, k_ms = "engine_kernel", b_pfxt / (pfxt * 1e-3) / 1e9, pfxt
+    traffic = KERNEL_TRAFFIC.get(kern)
 
     line = {
         "metric": METRIC, "value": value, "unit": "paths/s", "n_gpus": world,
@@ -292,7 +301,9 @@ def run_ours(args):
                              ["seed", "decide", "select", "promote", "closure", "out_select",
                               "out_sort", "emit"], stats["engine_stage_ms"]))},
         "roofline": {"bound": "hbm", "kernel": kern, "achieved": ach, "peak": hbm,
-                     "peak_source": src, "unit": "GB/s", "frac": ach / hbm, "traffic": None},
+                     "peak_source": src, "unit": "GB/s", "frac": ach / hbm,
+                     "traffic": traffic, "kernel_ms": k_ms,
+                     "algorithmic_bytes": b_sfxt if kern.startswith("sfxt") else b_pfxt},
         "e2e": {"value": replica_value(n_out, e2e, world), "unit": "paths/s",
                 "ms_per_step": e2e, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": d2h},
         "gpu_launches": int(launches),

@@ -74,7 +74,7 @@ class Stats(C.Structure):
         ("frontier_used", C.c_int32), ("retries", C.c_int32),
         ("engine_stage_ms", C.c_float * 8),
         ("bvss_tiles_tensor", C.c_int64), ("bvss_tiles_scalar", C.c_int64),
-        ("bvss_bits_per_slice", C.c_double),
+        ("bvss_bits_per_slice", C.c_double), ("sfxt_kernel_ms", C.c_double),
     ]
 
 

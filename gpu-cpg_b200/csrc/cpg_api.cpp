@@ -95,7 +95,7 @@ struct cpg_handle {
 
   // staging
   void* pinned = nullptr;
-  cudaEvent_t ev[6] = {};
+  cudaEvent_t ev[8] = {};  // [6], [7]: around the suffix-tree kernel alone
   cpg_stats stats{};
 };
 
@@ -382,7 +382,8 @@ SfxtParams sfxt_params(cpg_handle* h, int32_t start_level) {
 }
 
 // Device work of one suffix-tree build, asynchronous and capturable.
-Status enqueue_sfxt(cpg_handle* h, int32_t start_level, int* launches) {
+Status enqueue_sfxt(cpg_handle* h, int32_t start_level, int* launches,
+                    bool kernel_events = false) {
   cudaStream_t s = h->stream;
   if (h->multi_graph && start_level > 0)
     CK(cudaMemcpyAsync(h->d_graph_from.p, h->graph_from.data(), h->graph_from.size() * 4,
@@ -396,7 +397,9 @@ Status enqueue_sfxt(cpg_handle* h, int32_t start_level, int* launches) {
     CK(cudaMemsetAsync(h->d_iact.p, 0, h->d_iact.bytes, s), "memset");
   }
   int grid = 0;
-  CK(launch_sfxt(sfxt_params(h, start_level), h->device, s, &grid, launches), "sfxt launch");
+  CK(launch_sfxt(sfxt_params(h, start_level), h->device, s, &grid, launches,
+                 kernel_events ? h->ev[6] : nullptr, kernel_events ? h->ev[7] : nullptr),
+     "sfxt launch");
   *launches += 1;
   return CPG_OK;
 }
@@ -440,14 +443,16 @@ Status run_sfxt(cpg_handle* h, int32_t start_level) {
   for (int attempt = 0; attempt < 8; ++attempt) {
     CK(cudaEventRecord(h->ev[0], s), "event");
     int launches = 0;
-    Status st = enqueue_sfxt(h, start_level, &launches);
+    Status st = enqueue_sfxt(h, start_level, &launches, true);
     if (st != CPG_OK) return st;
     CK(cudaEventRecord(h->ev[1], s), "event");
     h->stats.kernel_launches += launches;
     const int r = finish_sfxt(h, start_level);
-    float ms = 0.f;
+    float ms = 0.f, kms = 0.f;
     cudaEventElapsedTime(&ms, h->ev[0], h->ev[1]);
+    cudaEventElapsedTime(&kms, h->ev[6], h->ev[7]);
     h->stats.sfxt_ms = ms;
+    h->stats.sfxt_kernel_ms = kms;
     if (r == kRetry) {
       // chain heaps outgrew their pool.  Incremental builds append to the
       // pool, so first rebuild from scratch (which compacts it); grow only

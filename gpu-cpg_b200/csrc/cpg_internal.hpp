@@ -245,7 +245,7 @@ int launch_init_sfxt_counters(SfxtCounters* c, const unsigned long long* pool_ma
 // Launch the persistent SFXT kernel (cooperative) and the row sorts that
 // follow it.  Returns a cudaError_t; *launches counts the kernels.
 int launch_sfxt(const SfxtParams& p, int device, void* stream, int* grid_out,
-                int* launches);
+                int* launches, void* ev_before = nullptr, void* ev_after = nullptr);
 
 // ---------------------------------------------------------------- PFXT
 struct PfxtCounters {

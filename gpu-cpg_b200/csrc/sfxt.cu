@@ -1004,7 +1004,7 @@ __global__ void sort_big_rows_kernel(const int32_t* rows, const int32_t* adjp,
 }  // namespace
 
 int launch_sfxt(const SfxtParams& p, int device, void* stream, int* grid_out,
-                int* launches) {
+                int* launches, void* ev_before, void* ev_after) {
   int sms = 0, per_sm = 0;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -1024,8 +1024,16 @@ int launch_sfxt(const SfxtParams& p, int device, void* stream, int* grid_out,
   if (grid_out) *grid_out = grid;
   SfxtParams pp = p;
   void* args[] = {&pp};
+  if (ev_before) {
+    e = cudaEventRecord(static_cast<cudaEvent_t>(ev_before), st);
+    if (e != cudaSuccess) return e;
+  }
   e = cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kSfxtThreads), args, 0, st);
   if (e != cudaSuccess) return e;
+  if (ev_after) {
+    e = cudaEventRecord(static_cast<cudaEvent_t>(ev_after), st);
+    if (e != cudaSuccess) return e;
+  }
   sort_rows_kernel<<<sms * 8, kSortWarps * 32, 0, st>>>(
       p.order, &p.ctr->sort_beg, p.adjp, p.dev_cnt, p.dev, p.vgraph, p.graph_from, p.level_of);
   int n = 2;

@@ -134,6 +134,8 @@ typedef struct {
   int64_t bvss_tiles_tensor; /* BVSS tiles counted on the tensor cores */
   int64_t bvss_tiles_scalar; /* ... and with scalar popc */
   double bvss_bits_per_slice; /* measured density of the fan-out BVSS */
+  double sfxt_kernel_ms;   /* the suffix-tree kernel alone (sfxt_ms adds the
+                              counter reset and the deviation-row sorts) */
 } cpg_stats;
 
 /* ------------------------------------------------------------ lifecycle */

@@ -47,6 +47,49 @@ __device__ __forceinline__ int fixed_delay(float w) {
 constexpr int kRegChunks = kSmemRow / 32;  // rows up to this many 32-edge chunks
                                           // stay in registers
 
+// (key, position) word ordering a deviation row: ascending exact key, ties
+// in edge order.
+__device__ __forceinline__ unsigned long long sort_word(float key, int idx) {
+  return (static_cast<unsigned long long>(float_key(key)) << 32) |
+         static_cast<unsigned>(idx);
+}
+
+// Bitonic sort of one word per lane across the warp, ascending by lane.
+__device__ __forceinline__ unsigned long long warp_sort32(unsigned long long x) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      const unsigned long long y = __shfl_xor_sync(0xffffffffu, x, j);
+      const bool up = (lane & k) == 0;
+      const bool lower = (lane & j) == 0;
+      x = (lower == up) ? (x < y ? x : y) : (x > y ? x : y);
+    }
+  }
+  return x;
+}
+
+// A row of at most 32 edges (one per lane) is sorted in registers and
+// written once, in order; longer rows are written in edge order and sorted
+// by sort_rows_kernel.  Returns the number of deviations written.
+__device__ __forceinline__ int write_short_row(const SfxtParams& p, int rb, bool valid,
+                                               const DevSidetrack& rec, float& kmin) {
+  const int lane = threadIdx.x & 31;
+  const unsigned bal = __ballot_sync(0xffffffffu, valid);
+  const unsigned long long x = warp_sort32(valid ? sort_word(rec.key, lane) : ~0ull);
+  const int src = static_cast<int>(x & 31u);
+  DevSidetrack o;
+  o.head = __shfl_sync(0xffffffffu, rec.head, src);
+  o.w = __shfl_sync(0xffffffffu, rec.w, src);
+  o.dist_head = __shfl_sync(0xffffffffu, rec.dist_head, src);
+  o.key = __shfl_sync(0xffffffffu, rec.key, src);
+  const int cnt = __popc(bal);
+  if (lane < cnt) p.dev[rb + lane] = o;
+  if (valid) kmin = fminf(kmin, rec.key);
+  return cnt;
+}
+
 __device__ __forceinline__ int cand_dist(int dh, float w) {
   return static_cast<int>(static_cast<unsigned>(dh) + static_cast<unsigned>(fixed_delay(w)));
 }
@@ -100,6 +143,16 @@ __device__ int build_vertex(const SfxtParams& p, int v, int lvl, bool do_kahn) {
     }
     // deviations: fan-out edges whose head is not the successor and has a
     // finite distance, compacted in edge order into v's own fan-out slots
+    // (a row of at most 32 edges already sorted)
+    if (re - rb <= 32) {
+      const bool valid = ed[0].head >= 0 && ed[0].head != s && dh[0] != INT_MAX;
+      DevSidetrack rec;
+      rec.head = ed[0].head;
+      rec.w = ed[0].w;
+      rec.dist_head = dh[0];
+      rec.key = deviation_key(dh[0], best, ed[0].w);
+      cnt = write_short_row(p, rb, valid, rec, kmin);
+    } else
 #pragma unroll
     for (int c = 0; c < kRegChunks; ++c) {
       if (rb + c * 32 >= re) break;
@@ -486,7 +539,7 @@ sfxt_persistent_kernel(SfxtParams p) {
 // by level into order[] / lvlp[] for the level-synchronous incremental
 // rebuilds.  Every wait is bounded by spin_limit polls (kDevTimeout).
 
-__device__ __forceinline__ int wait_slot(const SfxtParams& p, int s) {
+__device__ __forceinline__ int wait_slot(const SfxtParams& p, int s, bool acquire) {
   int v = -1;
   if ((threadIdx.x & 31) == 0) {
     unsigned int it = 0;
@@ -499,7 +552,7 @@ __device__ __forceinline__ int wait_slot(const SfxtParams& p, int s) {
       }
       __nanosleep(32);
     }
-    __threadfence();  // acquire: the heads' dist / level writes
+    if (acquire) __threadfence();  // late push: the heads' dist / level writes
   }
   return __shfl_sync(0xffffffffu, v, 0);
 }
@@ -599,6 +652,15 @@ __device__ int build_vertex_polled(const SfxtParams& p, int v) {
         if (ed[c].head >= 0 && cand_dist(dh[c], ed[c].w) == best) s = max(s, ed[c].head);
       s = warp_max_i(s);
     }
+    if (re - rb <= 32) {
+      const bool valid = ed[0].head >= 0 && ed[0].head != s && dh[0] != INT_MAX;
+      DevSidetrack rec;
+      rec.head = ed[0].head;
+      rec.w = ed[0].w;
+      rec.dist_head = dh[0];
+      rec.key = deviation_key(dh[0], best, ed[0].w);
+      cnt = write_short_row(p, rb, valid, rec, kmin);
+    } else
 #pragma unroll
     for (int c = 0; c < kRegChunks; ++c) {
       if (rb + c * 32 >= re) break;
@@ -635,16 +697,17 @@ __device__ int build_vertex_polled(const SfxtParams& p, int v) {
       if (ok) lmax = max(lmax, static_cast<int>(x >> 32));
     }
     if (!__all_sync(0xffffffffu, ok)) return -1;
-    __threadfence();  // acquire: the heads' dist[] words
     const int lvl = warp_max_i(lmax) + 1;
+    // the heads' distances come from their published words
+    auto dist_of = [&](int h) { return static_cast<int>(ld_dl(p, h) & 0xffffffffu); };
     for (int e = rb + lane; e < re; e += 32) {
       const DevEdge ed = p.edges[e];
-      best = min(best, cand_dist(__ldcg(p.dist + ed.head), ed.w));
+      best = min(best, cand_dist(dist_of(ed.head), ed.w));
     }
     best = warp_min_i(best);
     for (int e = rb + lane; e < re; e += 32) {
       const DevEdge ed = p.edges[e];
-      if (cand_dist(__ldcg(p.dist + ed.head), ed.w) == best) s = max(s, ed.head);
+      if (cand_dist(dist_of(ed.head), ed.w) == best) s = max(s, ed.head);
     }
     s = warp_max_i(s);
     for (int base = rb; base < re; base += 32) {
@@ -653,7 +716,7 @@ __device__ int build_vertex_polled(const SfxtParams& p, int v) {
       DevSidetrack rec;
       if (e < re) {
         const DevEdge ed = p.edges[e];
-        const int dh = __ldcg(p.dist + ed.head);
+        const int dh = dist_of(ed.head);
         valid = ed.head != s && dh != INT_MAX;
         rec.head = ed.head;
         rec.w = ed.w;
@@ -676,7 +739,8 @@ __device__ int build_vertex_polled(const SfxtParams& p, int v) {
     p.dev_cnt[v] = cnt;
     p.deps[v] = __float_as_int(kmin);
     p.level_of[v] = lmax;
-    __threadfence();  // release: dist / succ / level before the published word
+    // the word carries everything a tail's build reads of v, so it needs
+    // no fence before it
     *reinterpret_cast<volatile unsigned long long*>(p.dl + v) =
         (static_cast<unsigned long long>(static_cast<unsigned>(lmax)) << 32) |
         static_cast<unsigned>(best);
@@ -787,7 +851,7 @@ sfxt_dataflow_kernel(SfxtParams p) {
   if (wib < build_warps) {
     const int nbw = gridDim.x * build_warps;
     for (int s = blockIdx.x * build_warps + wib; s < p.n; s += nbw) {
-      const int v = wait_slot(p, s);
+      const int v = wait_slot(p, s, !p.early_push);
       if (v < 0) break;
       if (p.early_push) {
         // the tails learn of v before it is built; they wait on its word
@@ -874,11 +938,6 @@ sfxt_dataflow_kernel(SfxtParams p) {
 // memory one up to kSmemRow.  Longer rows go to sort_big_rows_kernel.
 constexpr int kSortWarps = 8;
 
-__device__ __forceinline__ unsigned long long sort_word(float key, int idx) {
-  return (static_cast<unsigned long long>(float_key(key)) << 32) |
-         static_cast<unsigned>(idx);
-}
-
 __global__ void __launch_bounds__(kSortWarps * 32)
 sort_rows_kernel(const int32_t* order, const int* range, const int32_t* adjp,
                  const int32_t* dev_cnt, DevSidetrack* dev, const int32_t* vgraph,
@@ -892,6 +951,7 @@ sort_rows_kernel(const int32_t* order, const int* range, const int32_t* adjp,
     const int v = order[i];
     const int cnt = dev_cnt[v];
     if (cnt <= 1 || cnt > kSmemRow) continue;
+    if (adjp[v + 1] - adjp[v] <= 32) continue;  // sorted when it was built
     if (vgraph && level_of[v] < graph_from[vgraph[v]]) continue;  // not rebuilt
     DevSidetrack* row = dev + adjp[v];
     if (cnt <= 32) {

@@ -405,8 +405,13 @@ class CpGen:
         and ignored (the method is fixed to levelize-then-relax + G-PathGen)."""
         self._check(lib.cpg_report_paths(self._h, int(k)), "report_paths")
 
-    def get_slacks(self, k: int) -> np.ndarray:
-        out = np.empty(max(int(k), 0), np.float32)
+    def get_slacks(self, k: int, out: np.ndarray | None = None) -> np.ndarray:
+        """The k lowest path costs, ascending; `out` (float32, >= k) may be a
+        caller-owned (e.g. pinned) buffer to copy into."""
+        if out is None:
+            out = np.empty(max(int(k), 0), np.float32)
+        elif out.dtype != np.float32 or out.size < k or not out.flags.c_contiguous:
+            raise ValueError("out must be a contiguous float32 array of at least k elements")
         n = C.c_int64()
         self._check(lib.cpg_get_costs(self._h, int(k), _ptr(out), C.byref(n)), "get_slacks")
         return out[: n.value]

@@ -95,6 +95,10 @@ struct cpg_handle {
 
   // staging
   void* pinned = nullptr;
+  // pinned ring for large host-to-device uploads (kStageSlots x kStageChunk)
+  char* stage = nullptr;
+  cudaEvent_t stage_ev[4] = {};
+  int stage_next = 0;
   cudaEvent_t ev[8] = {};  // [6], [7]: around the suffix-tree kernel alone
   cpg_stats stats{};
 };
@@ -144,6 +148,50 @@ T* P(DevMem& b) {
 
 Status check_handle(cpg_handle* h) {
   if (!h) return CPG_ERR_INVALID;
+  return CPG_OK;
+}
+
+// Host-to-device copy of a caller's (pageable) buffer.  Pageable copies run
+// at about a fifth of the link's pinned rate, so large ones go through a
+// pinned ring: host threads copy one chunk into a free slot while the copy
+// engine moves the previous ones.  Small copies go directly.
+constexpr size_t kStageChunk = size_t{16} << 20;
+constexpr int kStageSlots = 4;
+constexpr size_t kStageMin = size_t{8} << 20;
+
+Status upload_h2d(cpg_handle* h, void* dst, const void* src, size_t bytes) {
+  cudaStream_t s = h->stream;
+  cudaPointerAttributes attr{};
+  const bool pinned_src = cudaPointerGetAttributes(&attr, src) == cudaSuccess &&
+                          attr.type == cudaMemoryTypeHost;
+  cudaGetLastError();
+  if (bytes < kStageMin || pinned_src) {  // pinned sources copy at full rate as they are
+    CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s), "H2D");
+    return CPG_OK;
+  }
+  if (!h->stage) {
+    void* p = nullptr;
+    CK(cudaMallocHost(&p, kStageChunk * kStageSlots), "pinned staging");
+    h->stage = static_cast<char*>(p);
+    for (auto& e : h->stage_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+  }
+  const int threads = std::max(1, std::min(8, static_cast<int>(std::thread::hardware_concurrency())));
+  for (size_t off = 0; off < bytes; off += kStageChunk) {
+    const size_t len = std::min(kStageChunk, bytes - off);
+    const int slot = h->stage_next;
+    h->stage_next = (slot + 1) % kStageSlots;
+    CK(cudaEventSynchronize(h->stage_ev[slot]), "staging slot");  // its last copy is done
+    char* stg = h->stage + static_cast<size_t>(slot) * kStageChunk;
+    const char* from = static_cast<const char*>(src) + off;
+    const size_t part = (len + threads - 1) / threads;
+#pragma omp parallel for num_threads(threads) schedule(static)
+    for (int t = 0; t < threads; ++t) {
+      const size_t b = static_cast<size_t>(t) * part;
+      if (b < len) std::memcpy(stg + b, from + b, std::min(part, len - b));
+    }
+    CK(cudaMemcpyAsync(static_cast<char*>(dst) + off, stg, len, cudaMemcpyHostToDevice, s), "H2D");
+    CK(cudaEventRecord(h->stage_ev[slot], s), "event");
+  }
   return CPG_OK;
 }
 
@@ -206,9 +254,7 @@ Status upload_graph(cpg_handle* h, int32_t n, int32_t m, const int32_t* adjp,
     if (d < 0) return fail(h, CPG_ERR_INVALID, "CSR offsets must be non-decreasing");
     max_deg = std::max(max_deg, d);
   }
-  for (int64_t e = 0; e < m; ++e)
-    if (static_cast<uint32_t>(adj[e]) >= static_cast<uint32_t>(n))
-      return fail(h, CPG_ERR_INVALID, "edge head out of range");
+  // heads are range-checked on the device while the graph is built
   if (max_deg > kMaxRow)
     return fail(h, CPG_ERR_INVALID, "out-degree above 16384 is not supported");
   h->has_graph = false;
@@ -245,7 +291,7 @@ Status upload_graph(cpg_handle* h, int32_t n, int32_t m, const int32_t* adjp,
   CK(ensure(h->d_edges, mm * sizeof(DevEdge)), "alloc edges");
   CK(ensure(h->d_iadjp, (nn + 1) * 4), "alloc iadjp");
   CK(ensure(h->d_iadj, mm * 4), "alloc iadj");
-  CK(ensure(h->d_srcs, nn * 4 + 4), "alloc srcs");
+  CK(ensure(h->d_srcs, nn * 4 + 8), "alloc srcs");
   CK(ensure(h->d_big_off, nn * 4), "alloc big_off");
   CK(ensure(h->d_big_rows, big_rows.size() * 4), "alloc big rows");
   CK(ensure(h->d_big_tmp, static_cast<size_t>(big_total) * sizeof(DevSidetrack)),
@@ -278,10 +324,11 @@ Status upload_graph(cpg_handle* h, int32_t n, int32_t m, const int32_t* adjp,
   cudaStream_t s = h->stream;
   int32_t* stage_adj = reinterpret_cast<int32_t*>(h->d_dev.p);
   float* stage_w = reinterpret_cast<float*>(stage_adj + mm);
-  CK(cudaMemcpyAsync(h->d_adjp.p, adjp, (nn + 1) * 4, cudaMemcpyHostToDevice, s), "H2D adjp");
-  if (m) {
-    CK(cudaMemcpyAsync(stage_adj, adj, mm * 4, cudaMemcpyHostToDevice, s), "H2D adjncy");
-    CK(cudaMemcpyAsync(stage_w, w, mm * 4, cudaMemcpyHostToDevice, s), "H2D delays");
+  {
+    Status st = upload_h2d(h, h->d_adjp.p, adjp, (nn + 1) * 4);
+    if (st == CPG_OK && m) st = upload_h2d(h, stage_adj, adj, mm * 4);
+    if (st == CPG_OK && m) st = upload_h2d(h, stage_w, w, mm * 4);
+    if (st != CPG_OK) return st;
   }
   if (n) CK(cudaMemcpyAsync(h->d_big_off.p, big_off.data(), nn * 4, cudaMemcpyHostToDevice, s), "H2D big_off");
   if (!big_rows.empty())
@@ -292,8 +339,9 @@ Status upload_graph(cpg_handle* h, int32_t n, int32_t m, const int32_t* adjp,
                         P<int32_t>(h->d_iadj), P<int32_t>(h->d_srcs), nsrc_dev,
                         P<int32_t>(h->d_deps), s), "build graph");
   int32_t* hn = static_cast<int32_t*>(h->pinned);
-  CK(cudaMemcpyAsync(hn, nsrc_dev, 4, cudaMemcpyDeviceToHost, s), "D2H sources");
+  CK(cudaMemcpyAsync(hn, nsrc_dev, 8, cudaMemcpyDeviceToHost, s), "D2H sources");
   CK(cudaStreamSynchronize(s), "upload");
+  if (hn[1] != 0) return fail(h, CPG_ERR_INVALID, "edge head out of range");
   h->n_srcs = *hn;
   // sources in vertex-id order, as the reference's _srcs list (gpucpg.cu:
   // 531-533): G-PathGen's root seeding keeps the first roots in that order
@@ -1019,6 +1067,11 @@ cpg_status cpg_destroy(cpg_handle* h) {
   for (auto& e : h->ev)
     if (e) cudaEventDestroy(e);
   if (h->pinned) cudaFreeHost(h->pinned);
+  if (h->stage) {
+    cudaFreeHost(h->stage);
+    for (auto& e : h->stage_ev)
+      if (e) cudaEventDestroy(e);
+  }
   if (h->own_stream) cudaStreamDestroy(h->stream);
   delete h;
   return CPG_OK;

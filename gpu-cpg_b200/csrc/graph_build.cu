@@ -22,10 +22,19 @@ __global__ void interleave_kernel(const int32_t* adj, const float* w, int64_t m,
   }
 }
 
-__global__ void indegree_kernel(const int32_t* adj, int64_t m, int32_t* indeg) {
+// Also validates the heads: one outside [0, n) sets *bad and is skipped, so
+// the host learns of it after the build without an O(M) host pass.
+__global__ void indegree_kernel(const int32_t* adj, int64_t m, int32_t n, int32_t* indeg,
+                                int32_t* bad) {
   for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < m;
-       e += static_cast<int64_t>(gridDim.x) * blockDim.x)
-    atomicAdd(&indeg[adj[e]], 1);
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int h = adj[e];
+    if (static_cast<unsigned>(h) >= static_cast<unsigned>(n)) {
+      *bad = 1;
+      continue;
+    }
+    atomicAdd(&indeg[h], 1);
+  }
 }
 
 // exclusive scan of x[0..n) into y[0..n], y[n] = total; three-kernel
@@ -111,6 +120,7 @@ __global__ void fanin_scatter_kernel(const int32_t* adjp, const int32_t* adj, in
   for (int u = gw; u < n; u += nw) {
     for (int e = adjp[u] + lane; e < adjp[u + 1]; e += 32) {
       const int h = adj[e];
+      if (static_cast<unsigned>(h) >= static_cast<unsigned>(n)) continue;  // reported
       iadj[atomicAdd(&fill[h], 1)] = u;
     }
   }
@@ -141,7 +151,8 @@ size_t build_scratch_words(int32_t n) {
 }
 
 // adj/w: uploaded fan-out heads and delays; outputs edges, iadjp (n+1), iadj
-// (m), srcs (n) and *n_srcs (device int).  scratch: build_scratch_words(n) ints.
+// (m), srcs (n), n_srcs[0] (source count) and n_srcs[1] (1 if a head lies
+// outside [0, n)).  scratch: build_scratch_words(n) ints.
 int launch_build_graph(const int32_t* adjp, const int32_t* adj, const float* w,
                        int32_t n, int64_t m, DevEdge* edges, int32_t* iadjp,
                        int32_t* iadj, int32_t* srcs, int32_t* n_srcs,
@@ -151,10 +162,10 @@ int launch_build_graph(const int32_t* adjp, const int32_t* adj, const float* w,
   int32_t* sums = scratch + n;
   const int ntiles = static_cast<int>((static_cast<int64_t>(n) + kScanTile - 1) / kScanTile);
   cudaMemsetAsync(indeg, 0, static_cast<size_t>(n) * 4, s);
-  cudaMemsetAsync(n_srcs, 0, 4, s);
+  cudaMemsetAsync(n_srcs, 0, 8, s);  // source count, bad-head flag
   if (m > 0) {
     interleave_kernel<<<grid_of(m, 256), 256, 0, s>>>(adj, w, m, edges);
-    indegree_kernel<<<grid_of(m, 256), 256, 0, s>>>(adj, m, indeg);
+    indegree_kernel<<<grid_of(m, 256), 256, 0, s>>>(adj, m, n, indeg, n_srcs + 1);
   }
   if (n > 0) {
     tile_sum_kernel<<<ntiles, 256, 0, s>>>(indeg, n, sums);

@@ -248,44 +248,10 @@ Status upload_graph(cpg_handle* h, int32_t n, int32_t m, const int32_t* adjp,
   if (adjp[0] != 0 || adjp[n] != m)
     return fail(h, CPG_ERR_INVALID, "CSR offsets must start at 0 and end at m");
   CK(cudaSetDevice(h->device), "cudaSetDevice");
-  int32_t max_deg = 0;
-  for (int32_t v = 0; v < n; ++v) {
-    const int32_t d = adjp[v + 1] - adjp[v];
-    if (d < 0) return fail(h, CPG_ERR_INVALID, "CSR offsets must be non-decreasing");
-    max_deg = std::max(max_deg, d);
-  }
-  // heads are range-checked on the device while the graph is built
-  if (max_deg > kMaxRow)
-    return fail(h, CPG_ERR_INVALID, "out-degree above 16384 is not supported");
   h->has_graph = false;
   h->multi_graph = false;  // cpg_batch_commit sets it after the upload
   h->graph_voff.clear();
   h->graph_from.clear();
-  {
-    Status st = setup_bvss(h, n, adjp, adj);
-    if (st != CPG_OK) return st;
-  }
-  h->g.n = n;
-  h->g.m = m;
-  h->g.adjp.assign(adjp, adjp + n + 1);
-  h->g.adj.clear();
-  h->g.w.clear();
-  h->max_outdeg = max_deg;
-  std::vector<int32_t> big_off(n, -1), big_rows;
-  int64_t big_total = 0;
-  int32_t big_cap = 1;
-  for (int32_t v = 0; v < n; ++v) {
-    const int32_t od = adjp[v + 1] - adjp[v];
-    if (od > kSmemRow) {
-      big_off[v] = static_cast<int32_t>(big_total);
-      big_total += od;
-      big_rows.push_back(v);
-      while (big_cap < od) big_cap <<= 1;
-    }
-  }
-  h->big_total = big_total;
-  h->big_rows = static_cast<int32_t>(big_rows.size());
-  h->big_cap = big_cap;
   const size_t nn = static_cast<size_t>(n), mm = static_cast<size_t>(m);
   CK(ensure(h->d_adjp, (nn + 1) * 4), "alloc adjp");
   CK(ensure(h->d_edges, mm * sizeof(DevEdge)), "alloc edges");
@@ -293,9 +259,6 @@ Status upload_graph(cpg_handle* h, int32_t n, int32_t m, const int32_t* adjp,
   CK(ensure(h->d_iadj, mm * 4), "alloc iadj");
   CK(ensure(h->d_srcs, nn * 4 + 8), "alloc srcs");
   CK(ensure(h->d_big_off, nn * 4), "alloc big_off");
-  CK(ensure(h->d_big_rows, big_rows.size() * 4), "alloc big rows");
-  CK(ensure(h->d_big_tmp, static_cast<size_t>(big_total) * sizeof(DevSidetrack)),
-     "alloc big rows");
   // suffix tree storage (the deviation array doubles as upload staging)
   CK(ensure(h->d_order, nn * 4), "alloc order");
   CK(ensure(h->d_queue, nn * 4 + 8), "alloc queue");
@@ -324,15 +287,66 @@ Status upload_graph(cpg_handle* h, int32_t n, int32_t m, const int32_t* adjp,
   cudaStream_t s = h->stream;
   int32_t* stage_adj = reinterpret_cast<int32_t*>(h->d_dev.p);
   float* stage_w = reinterpret_cast<float*>(stage_adj + mm);
+  // the copies start first; the host checks below overlap them
   {
     Status st = upload_h2d(h, h->d_adjp.p, adjp, (nn + 1) * 4);
     if (st == CPG_OK && m) st = upload_h2d(h, stage_adj, adj, mm * 4);
     if (st == CPG_OK && m) st = upload_h2d(h, stage_w, w, mm * 4);
     if (st != CPG_OK) return st;
   }
-  if (n) CK(cudaMemcpyAsync(h->d_big_off.p, big_off.data(), nn * 4, cudaMemcpyHostToDevice, s), "H2D big_off");
-  if (!big_rows.empty())
+  int32_t max_deg = 0, bad = 0;
+#pragma omp parallel for reduction(max : max_deg) reduction(| : bad) schedule(static)
+  for (int32_t v = 0; v < n; ++v) {
+    const int32_t d = adjp[v + 1] - adjp[v];
+    bad |= d < 0;
+    max_deg = std::max(max_deg, d);
+  }
+  if (bad || max_deg > kMaxRow) {
+    cudaStreamSynchronize(s);  // the copies still read the caller's buffers
+    return fail(h, CPG_ERR_INVALID, bad ? "CSR offsets must be non-decreasing"
+                                        : "out-degree above 16384 is not supported");
+  }
+  // heads are range-checked on the device while the graph is built
+  {
+    Status st = setup_bvss(h, n, adjp, adj);
+    if (st != CPG_OK) {
+      cudaStreamSynchronize(s);
+      return st;
+    }
+  }
+  h->g.n = n;
+  h->g.m = m;
+  h->g.adjp.assign(adjp, adjp + n + 1);
+  h->g.adj.clear();
+  h->g.w.clear();
+  h->max_outdeg = max_deg;
+  // rows too long for the shared-memory row sort (none in most graphs)
+  std::vector<int32_t> big_off, big_rows;
+  int64_t big_total = 0;
+  int32_t big_cap = 1;
+  if (max_deg > kSmemRow) {
+    big_off.assign(nn, -1);
+    for (int32_t v = 0; v < n; ++v) {
+      const int32_t od = adjp[v + 1] - adjp[v];
+      if (od > kSmemRow) {
+        big_off[v] = static_cast<int32_t>(big_total);
+        big_total += od;
+        big_rows.push_back(v);
+        while (big_cap < od) big_cap <<= 1;
+      }
+    }
+  }
+  h->big_total = big_total;
+  h->big_rows = static_cast<int32_t>(big_rows.size());
+  h->big_cap = big_cap;
+  CK(ensure(h->d_big_rows, big_rows.size() * 4), "alloc big rows");
+  CK(ensure(h->d_big_tmp, static_cast<size_t>(big_total) * sizeof(DevSidetrack)),
+     "alloc big rows");
+  if (!big_rows.empty()) {
+    // only the long rows' offsets are ever read
+    CK(cudaMemcpyAsync(h->d_big_off.p, big_off.data(), nn * 4, cudaMemcpyHostToDevice, s), "H2D big_off");
     CK(cudaMemcpyAsync(h->d_big_rows.p, big_rows.data(), big_rows.size() * 4, cudaMemcpyHostToDevice, s), "H2D big rows");
+  }
   int32_t* nsrc_dev = P<int32_t>(h->d_srcs) + nn;
   CK(launch_build_graph(P<int32_t>(h->d_adjp), stage_adj, stage_w, n, m,
                         P<DevEdge>(h->d_edges), P<int32_t>(h->d_iadjp),

@@ -640,7 +640,8 @@ def main():
     ap.add_argument("--profile-case", action="store_true",
                     help="one warm-up and one measured query only (for ncu)")
     ap.add_argument("--form", default="plain", choices=["plain", "batched", "served", "bvss"])
-    ap.add_argument("--autotune", action="store_true")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="batched form: skip cpg_batch_autotune before timing")
     ap.add_argument("--served-queries", type=int, default=5000)
     ap.add_argument("--bvss-graphs", default="both", choices=["both", "sparse", "dense"])
     args = ap.parse_args()

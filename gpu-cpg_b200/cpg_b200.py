@@ -84,6 +84,9 @@ class BatchStats(C.Structure):
         ("phases", C.c_int32), ("rounds", C.c_int32), ("graph_captured", C.c_int32),
         ("retries", C.c_int32), ("bytes_reserved", C.c_int64),
         ("sfxt_ctas_per_sm", C.c_int32), ("engine_ctas_per_sm", C.c_int32),
+        ("select_schedule", C.c_int32), ("sfxt_mode", C.c_int32),
+        ("frontier_used", C.c_int32), ("bvss_tiles", C.c_int32),
+        ("tuned_candidates", C.c_int32), ("pad", C.c_int32),
     ]
 
 

@@ -1724,6 +1724,10 @@ cpg_status cpg_batch_get_stats(const cpg_batch* b, cpg_batch_stats* out) {
   *out = b->stats;
   out->sfxt_ctas_per_sm = b->h->sfxt_grid_limit;
   out->engine_ctas_per_sm = b->h->engine_grid_limit;
+  out->select_schedule = b->h->sel_schedule;
+  out->sfxt_mode = b->h->opts.sfxt_level_sync == 1 ? 2 : (b->h->opts.sfxt_late_push == 1 ? 1 : 0);
+  out->frontier_used = b->h->use_bvss ? CPG_FRONTIER_BVSS : CPG_FRONTIER_CSR;
+  out->bvss_tiles = b->h->opts.bvss_tiles;
   return CPG_OK;
 }
 
@@ -1733,21 +1737,41 @@ cpg_status cpg_batch_autotune(cpg_batch* b) {
   cpg_handle* h = b->h;
   int sms = 0;
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device), "attribute");
-  // candidates: persistent CTAs for each kernel (all SMs, half of them) and
-  // the select's digit schedule; each timed over two steps after a warm-up
+  // The BVSS frontier is a candidate only when its slices are dense enough
+  // to have a chance; it is built once, from the host CSR, when it is.
+  const bool try_bvss = h->use_bvss || h->bvss_bps >= 1.5 ||
+                        bvss_density_sample(b->voff.back(), b->adjp.data(), b->adj.data(), 4096) >= 1.5;
+  if (try_bvss && !h->use_bvss) {
+    const int32_t keep = h->opts.frontier;
+    h->opts.frontier = CPG_FRONTIER_BVSS;
+    Status st = setup_bvss(h, b->voff.back(), b->adjp.data(), b->adj.data());
+    h->opts.frontier = keep;
+    if (st != CPG_OK) return static_cast<cpg_status>(st);
+    h->use_bvss = false;  // built; each candidate below turns it on or off
+  }
   struct Cand {
-    int sfxt, engine, sched;
+    int sfxt, engine, sched, mode, bvss, tiles;
   };
-  const Cand cands[] = {{0, 0, 0}, {0, 0, 1}, {sms / 2, 0, 0}, {0, sms / 2, 0},
-                        {sms / 2, sms / 2, 0}};
-  double best = 1e30;
-  Cand pick = cands[0];
-  for (const Cand& c : cands) {
+  std::vector<Cand> cands = {{0, 0, 0, 0, 0, 0}, {0, 0, 1, 0, 0, 0}, {sms / 2, 0, 0, 0, 0, 0},
+                             {0, sms / 2, 0, 0, 0, 0}, {sms / 2, sms / 2, 0, 0, 0, 0},
+                             {0, 0, 0, 1, 0, 0}, {0, 0, 0, 2, 0, 0}};
+  if (try_bvss)
+    for (int t = 0; t < 3; ++t) cands.push_back({0, 0, 0, 2, 1, t});
+  auto apply = [&](const Cand& c) {
     h->sfxt_grid_limit = c.sfxt;
     h->engine_grid_limit = c.engine;
     h->sel_schedule = c.sched;
+    h->opts.sfxt_late_push = c.mode == 1;
+    h->opts.sfxt_level_sync = c.mode == 2;
+    h->use_bvss = c.bvss != 0;
+    h->opts.bvss_tiles = c.tiles;
     b->prepared = false;  // sort scratch depends on the engine grid
     batch_drop_graph(b);
+  };
+  double best = 1e30;
+  Cand pick = cands[0];
+  for (const Cand& c : cands) {
+    apply(c);
     cpg_status st = cpg_batch_run(b, 1);
     if (st != CPG_OK) return st;
     double t = 0;
@@ -1761,11 +1785,8 @@ cpg_status cpg_batch_autotune(cpg_batch* b) {
       pick = c;
     }
   }
-  h->sfxt_grid_limit = pick.sfxt;
-  h->engine_grid_limit = pick.engine;
-  h->sel_schedule = pick.sched;
-  b->prepared = false;
-  batch_drop_graph(b);
+  apply(pick);
+  b->stats.tuned_candidates = static_cast<int32_t>(cands.size());
   return CPG_OK;
 }
 

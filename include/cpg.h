@@ -228,6 +228,12 @@ typedef struct {
   int64_t bytes_reserved;
   int32_t sfxt_ctas_per_sm;   /* launch shape chosen by cpg_batch_autotune */
   int32_t engine_ctas_per_sm;
+  int32_t select_schedule;    /* 0: 11/11/10-bit radix digits, 1: 8/8/8/8 */
+  int32_t sfxt_mode;          /* 0 dataflow (early push), 1 dataflow (late push), 2 level-synchronous */
+  int32_t frontier_used;      /* cpg_frontier of the suffix-tree build */
+  int32_t bvss_tiles;         /* cpg_bvss_tiles when the frontier is BVSS */
+  int32_t tuned_candidates;   /* candidates timed by the last cpg_batch_autotune */
+  int32_t pad;
 } cpg_batch_stats;
 
 cpg_status cpg_batch_create(cpg_batch** out, const cpg_options* opts);
@@ -250,9 +256,12 @@ cpg_status cpg_batch_run(cpg_batch* b, int32_t rebuild_sfxt);
 cpg_status cpg_batch_get_costs(const cpg_batch* b, int32_t q, float* out,
                                int64_t cap, int64_t* n_out);
 cpg_status cpg_batch_get_stats(const cpg_batch* b, cpg_batch_stats* out);
-/* Time the candidate launch shapes on the current queries and keep the
- * fastest (persistent CTAs per SM for the suffix-tree and engine kernels).
- * Results are unchanged by the choice. */
+/* Times candidate configurations over the set queries and keeps the fastest:
+ * persistent grid sizes of the suffix-tree and engine kernels, the radix
+ * digit schedule, the suffix-tree build mode and, when the side-by-side
+ * graph's slices hold at least 1.5 heads on average (the BVSS density test),
+ * the BVSS frontier with each tile policy.  Results are unchanged by any
+ * choice. */
 cpg_status cpg_batch_autotune(cpg_batch* b);
 
 /* ------------------------------------------------------------ served form */

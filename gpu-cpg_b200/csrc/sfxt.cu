@@ -71,8 +71,9 @@ __device__ __forceinline__ unsigned long long warp_sort32(unsigned long long x) 
 }
 
 // A row of at most 32 edges (one per lane) is sorted in registers and
-// written once, in order; longer rows are written in edge order and sorted
-// by sort_rows_kernel.  Returns the number of deviations written.
+// written once, in order (write_row64 does the same up to 64 edges); longer
+// rows are written in edge order and sorted by sort_rows_kernel.  Returns the
+// number of deviations written.
 __device__ __forceinline__ int write_short_row(const SfxtParams& p, int rb, bool valid,
                                                const DevSidetrack& rec, float& kmin) {
   const int lane = threadIdx.x & 31;
@@ -87,6 +88,62 @@ __device__ __forceinline__ int write_short_row(const SfxtParams& p, int rb, bool
   const int cnt = __popc(bal);
   if (lane < cnt) p.dev[rb + lane] = o;
   if (valid) kmin = fminf(kmin, rec.key);
+  return cnt;
+}
+
+// Rows of 33..64 edges: two words per lane (element i = 32 * chunk + lane),
+// one 64-element bitonic network (partners across chunks swap in
+// registers), then each sorted slot fetches its record from the lane and
+// chunk it came from.
+__device__ __forceinline__ int write_row64(const SfxtParams& p, int rb, bool v0,
+                                           const DevSidetrack& r0, bool v1,
+                                           const DevSidetrack& r1, float& kmin) {
+  const int lane = threadIdx.x & 31;
+  const unsigned b0 = __ballot_sync(0xffffffffu, v0);
+  const unsigned b1 = __ballot_sync(0xffffffffu, v1);
+  unsigned long long x[2] = {v0 ? sort_word(r0.key, lane) : ~0ull,
+                             v1 ? sort_word(r1.key, 32 + lane) : ~0ull};
+#pragma unroll
+  for (int k = 2; k <= 64; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      if (j == 32) {  // only at k == 64: ascending across the chunks
+        const unsigned long long lo = x[0] < x[1] ? x[0] : x[1];
+        const unsigned long long hi = x[0] < x[1] ? x[1] : x[0];
+        x[0] = lo;
+        x[1] = hi;
+      } else {
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          const int i = 32 * c + lane;
+          const unsigned long long y = __shfl_xor_sync(0xffffffffu, x[c], j);
+          const bool up = (i & k) == 0;
+          const bool lower = (i & j) == 0;
+          x[c] = (lower == up) ? (x[c] < y ? x[c] : y) : (x[c] > y ? x[c] : y);
+        }
+      }
+    }
+  }
+  const int cnt = __popc(b0) + __popc(b1);
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+    const int src = static_cast<int>(x[c] & 63u);
+    const int sl = src & 31;
+    const bool hi = src >= 32;
+    DevSidetrack o;
+    const int h0 = __shfl_sync(0xffffffffu, r0.head, sl), h1 = __shfl_sync(0xffffffffu, r1.head, sl);
+    const float w0 = __shfl_sync(0xffffffffu, r0.w, sl), w1 = __shfl_sync(0xffffffffu, r1.w, sl);
+    const int d0 = __shfl_sync(0xffffffffu, r0.dist_head, sl), d1 = __shfl_sync(0xffffffffu, r1.dist_head, sl);
+    const float k0 = __shfl_sync(0xffffffffu, r0.key, sl), k1 = __shfl_sync(0xffffffffu, r1.key, sl);
+    o.head = hi ? h1 : h0;
+    o.w = hi ? w1 : w0;
+    o.dist_head = hi ? d1 : d0;
+    o.key = hi ? k1 : k0;
+    const int i = 32 * c + lane;
+    if (i < cnt) p.dev[rb + i] = o;
+  }
+  if (v0) kmin = fminf(kmin, r0.key);
+  if (v1) kmin = fminf(kmin, r1.key);
   return cnt;
 }
 
@@ -143,7 +200,7 @@ __device__ int build_vertex(const SfxtParams& p, int v, int lvl, bool do_kahn) {
     }
     // deviations: fan-out edges whose head is not the successor and has a
     // finite distance, compacted in edge order into v's own fan-out slots
-    // (a row of at most 32 edges already sorted)
+    // (a row of at most 64 edges already sorted)
     if (re - rb <= 32) {
       const bool valid = ed[0].head >= 0 && ed[0].head != s && dh[0] != INT_MAX;
       DevSidetrack rec;
@@ -152,6 +209,18 @@ __device__ int build_vertex(const SfxtParams& p, int v, int lvl, bool do_kahn) {
       rec.dist_head = dh[0];
       rec.key = deviation_key(dh[0], best, ed[0].w);
       cnt = write_short_row(p, rb, valid, rec, kmin);
+    } else if (re - rb <= 64) {
+      DevSidetrack r[2];
+      bool v[2];
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        v[c] = ed[c].head >= 0 && ed[c].head != s && dh[c] != INT_MAX;
+        r[c].head = ed[c].head;
+        r[c].w = ed[c].w;
+        r[c].dist_head = dh[c];
+        r[c].key = deviation_key(dh[c], best, ed[c].w);
+      }
+      cnt = write_row64(p, rb, v[0], r[0], v[1], r[1], kmin);
     } else
 #pragma unroll
     for (int c = 0; c < kRegChunks; ++c) {
@@ -660,6 +729,18 @@ __device__ int build_vertex_polled(const SfxtParams& p, int v) {
       rec.dist_head = dh[0];
       rec.key = deviation_key(dh[0], best, ed[0].w);
       cnt = write_short_row(p, rb, valid, rec, kmin);
+    } else if (re - rb <= 64) {
+      DevSidetrack r[2];
+      bool v[2];
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        v[c] = ed[c].head >= 0 && ed[c].head != s && dh[c] != INT_MAX;
+        r[c].head = ed[c].head;
+        r[c].w = ed[c].w;
+        r[c].dist_head = dh[c];
+        r[c].key = deviation_key(dh[c], best, ed[c].w);
+      }
+      cnt = write_row64(p, rb, v[0], r[0], v[1], r[1], kmin);
     } else
 #pragma unroll
     for (int c = 0; c < kRegChunks; ++c) {
@@ -951,7 +1032,7 @@ sort_rows_kernel(const int32_t* order, const int* range, const int32_t* adjp,
     const int v = order[i];
     const int cnt = dev_cnt[v];
     if (cnt <= 1 || cnt > kSmemRow) continue;
-    if (adjp[v + 1] - adjp[v] <= 32) continue;  // sorted when it was built
+    if (adjp[v + 1] - adjp[v] <= 64) continue;  // sorted when it was built
     if (vgraph && level_of[v] < graph_from[vgraph[v]]) continue;  // not rebuilt
     DevSidetrack* row = dev + adjp[v];
     if (cnt <= 32) {

@@ -60,7 +60,7 @@ struct cpg_handle {
   bool multi_graph = false;
   std::vector<int32_t> graph_voff;  // first vertex of each graph
   std::vector<int32_t> graph_from;  // per graph: lowest changed level (INT32_MAX: clean)
-  DevMem d_vgraph, d_graph_from, d_upd, d_queue, d_dl;
+  DevMem d_vgraph, d_graph_from, d_upd, d_queue, d_dl, d_long;
   // BVSS form of the fan-out CSR, for the pull Kahn step
   bool use_bvss = false;
   double bvss_bps = 0;  // set bits per slice (sampled, or exact once built)
@@ -261,7 +261,8 @@ Status upload_graph(cpg_handle* h, int32_t n, int32_t m, const int32_t* adjp,
   CK(ensure(h->d_big_off, nn * 4), "alloc big_off");
   // suffix tree storage (the deviation array doubles as upload staging)
   CK(ensure(h->d_order, nn * 4), "alloc order");
-  CK(ensure(h->d_queue, nn * 4 + 8), "alloc queue");
+  CK(ensure(h->d_queue, (nn + 64) * 4), "alloc queue");
+  CK(ensure(h->d_long, nn * 4 + 4), "alloc row list");
   CK(ensure(h->d_dl, nn * 8 + 8), "alloc queue");
   CK(ensure(h->d_lvlp, (nn + 2) * 4), "alloc lvlp");
   CK(ensure(h->d_level_of, nn * 4), "alloc level_of");
@@ -413,6 +414,7 @@ SfxtParams sfxt_params(cpg_handle* h, int32_t start_level) {
   p.spin_limit = h->opts.spin_limit ? h->opts.spin_limit : kDefaultSpinLimit;
   p.grid_limit = h->sfxt_grid_limit;
   p.queue = P<int32_t>(h->d_queue);
+  p.long_rows = P<int32_t>(h->d_long);
   p.level_sync = h->opts.sfxt_level_sync == 1;
   p.heap_warps = std::min(std::max(h->opts.sfxt_heap_warps, 0), 16);
   p.early_push = h->opts.sfxt_late_push != 1 && p.heap_warps == 0;
@@ -1076,7 +1078,8 @@ cpg_status cpg_destroy(cpg_handle* h) {
                    &h->d_qids, &h->d_ehist, &h->d_esort, &h->d_equery, &h->d_ectr,
                    &h->d_bv_ptr, &h->d_bv_masks, &h->d_bv_rows, &h->d_bv_cnt,
                    &h->d_bv_deps, &h->d_fbits, &h->d_iact, &h->d_act_list,
-                   &h->d_vgraph, &h->d_graph_from, &h->d_upd, &h->d_queue, &h->d_dl};
+                   &h->d_vgraph, &h->d_graph_from, &h->d_upd, &h->d_queue, &h->d_dl,
+                   &h->d_long};
   for (DevMem* b : all) release(*b);
   for (auto& e : h->ev)
     if (e) cudaEventDestroy(e);

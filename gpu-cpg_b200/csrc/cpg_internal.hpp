@@ -104,6 +104,9 @@ struct SfxtCounters {
   int sort_beg;              // order[] range whose deviation rows were rebuilt
   int sort_end;
   alignas(128) unsigned long long hnode_used;
+  alignas(128) int n_long;   // rows left for the row-sort pass (long_rows[])
+  // dataflow build: append cursors of the kSfxtQueues work queues, one line each
+  alignas(128) int qtail[8][32];
   alignas(128) unsigned long long vss_tensor;  // BVSS tiles counted on the tensor cores
   unsigned long long vss_scalar;               // ... and with scalar popc
   alignas(128) GridBarrier bar;
@@ -147,6 +150,7 @@ struct SfxtParams {
   int32_t append_pool;
   // full CSR builds: dataflow work queue (n ints) unless level_sync is set
   int32_t* queue;
+  int32_t* long_rows;      // rows over 64 edges, written unsorted (n ints)
   int32_t level_sync;
   int32_t heap_warps;      // dataflow: warps per CTA that only insert heaps (0: none)
   int32_t early_push;      // dataflow: push tails before the build, poll dl[]

@@ -286,6 +286,8 @@ __device__ int build_vertex(const SfxtParams& p, int v, int lvl, bool do_kahn) {
     p.dist[v] = best;
     p.succ[v] = s;
     p.dev_cnt[v] = cnt;
+    if (re - rb > 64 && cnt > 1 && cnt <= kSmemRow)  // left for sort_rows_kernel
+      p.long_rows[atomicAdd(&p.ctr->n_long, 1)] = v;
     // v's fan-outs are all processed, so its dependency counter is free: it
     // carries the cheapest deviation key to the chain-heap insert, which runs
     // one level later, off this level's critical path
@@ -818,6 +820,8 @@ __device__ int build_vertex_polled(const SfxtParams& p, int v) {
     p.dist[v] = best;
     p.succ[v] = s;
     p.dev_cnt[v] = cnt;
+    if (re - rb > 64 && cnt > 1 && cnt <= kSmemRow)  // left for sort_rows_kernel
+      p.long_rows[atomicAdd(&p.ctr->n_long, 1)] = v;
     p.deps[v] = __float_as_int(kmin);
     p.level_of[v] = lmax;
     // the word carries everything a tail's build reads of v, so it needs
@@ -862,6 +866,34 @@ __device__ __forceinline__ bool wait_built(const SfxtParams& p, int v) {
   return true;
 }
 
+// The dataflow work queue is split in kSfxtQueues queues (vertex v goes to
+// queue v % kSfxtQueues, whose segment of queue[] holds exactly those
+// vertices), so appends spread over several counters instead of one.
+constexpr int kSfxtQueues = 1;
+
+__device__ __forceinline__ int queue_seg(const SfxtParams& p) {
+  return (p.n + kSfxtQueues - 1) / kSfxtQueues;
+}
+__device__ __forceinline__ int queue_count(const SfxtParams& p, int q) {
+  return p.n > q ? (p.n - 1 - q) / kSfxtQueues + 1 : 0;
+}
+
+// Append the lanes' u (where on) to their queues: one atomic per distinct
+// queue among the warp's lanes.  All lanes call.
+__device__ __forceinline__ void queue_push(const SfxtParams& p, bool on, int u) {
+  const int lane = threadIdx.x & 31;
+  const unsigned key = on ? static_cast<unsigned>(u) % kSfxtQueues : 0xffffffffu;
+  const unsigned m = __match_any_sync(0xffffffffu, key);
+  const int leader = __ffs(m) - 1;
+  int base = 0;
+  if (on && lane == leader) base = atomicAdd(&p.ctr->qtail[key][0], __popc(m));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (on) {
+    const int slot = static_cast<int>(key) * queue_seg(p) + base + __popc(m & lanemask_lt());
+    *reinterpret_cast<volatile int*>(p.queue + slot) = u;
+  }
+}
+
 // Kahn step of the dataflow build: take one pending fan-out off each tail;
 // tails reaching zero are queued.  kRelease: v's build precedes the push and
 // is published by it (late push); an early push publishes nothing.
@@ -883,10 +915,7 @@ __device__ __forceinline__ void dataflow_push(const SfxtParams& p, int v) {
     for (int c = 0; c < 4; ++c) ready[c] = u[c] >= 0 && atomicSub(&p.deps[u[c]], 1) == 1;
     if (kRelease) __threadfence();
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      const int slot = warp_append(&p.ctr->tail, ready[c]);
-      if (ready[c]) *reinterpret_cast<volatile int*>(p.queue + slot) = u[c];
-    }
+    for (int c = 0; c < 4; ++c) queue_push(p, ready[c], u[c]);
   }
 }
 
@@ -905,18 +934,17 @@ sfxt_dataflow_kernel(SfxtParams p) {
     p.ht_root[v] = -1;
     p.ht_size[v] = -1;  // heap not built yet
     p.level_of[v] = 0;
-    p.queue[v] = -1;
     p.order[v] = 0;  // build-published flags until the final level sort
     p.dl[v] = ~0ull;  // (dist, level) not published yet
   }
+  for (int i = tid; i < kSfxtQueues * queue_seg(p); i += nth) p.queue[i] = -1;
   for (int i = tid; i < p.n + 2; i += nth) p.lvlp[i] = 0;
   if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit)) return;
   // the sinks start the queue
   for (int base = blockIdx.x * blockDim.x; base < p.n; base += nth) {
     const int v = base + threadIdx.x;
     const bool sink = v < p.n && p.adjp[v + 1] == p.adjp[v];
-    const int slot = warp_append(&p.ctr->tail, sink);
-    if (sink) *reinterpret_cast<volatile int*>(p.queue + slot) = v;
+    queue_push(p, sink, v);
   }
   // the last kHeapWarps warps of each CTA insert chain heaps, one vertex per
   // lane, in queue order; the others build.  A build never waits on a heap.
@@ -930,9 +958,15 @@ sfxt_dataflow_kernel(SfxtParams p) {
   const int heap_warps = p.heap_warps;  // 0: the build warp inserts the heap itself
   const int build_warps = kSfxtThreads / 32 - heap_warps;
   if (wib < build_warps) {
+    // build warp bw serves queue bw % kSfxtQueues, taking every nwq-th slot
     const int nbw = gridDim.x * build_warps;
-    for (int s = blockIdx.x * build_warps + wib; s < p.n; s += nbw) {
-      const int v = wait_slot(p, s, !p.early_push);
+    const int bw = blockIdx.x * build_warps + wib;
+    const int q = bw % kSfxtQueues;
+    const int nwq = (nbw - q + kSfxtQueues - 1) / kSfxtQueues;
+    const int cnt_q = queue_count(p, q);
+    const int seg0 = q * queue_seg(p);
+    for (int k = bw / kSfxtQueues; k < cnt_q; k += nwq) {
+      const int v = wait_slot(p, seg0 + k, !p.early_push);
       if (v < 0) break;
       if (p.early_push) {
         // the tails learn of v before it is built; they wait on its word
@@ -958,8 +992,12 @@ sfxt_dataflow_kernel(SfxtParams p) {
     }
   } else {
     const int nhl = gridDim.x * heap_warps * 32;
-    for (int s = (blockIdx.x * heap_warps + (wib - build_warps)) * 32 + lane; s < p.n; s += nhl) {
-      const int v = wait_slot_lane(p, s);
+    const int seg = queue_seg(p);
+    for (int g = (blockIdx.x * heap_warps + (wib - build_warps)) * 32 + lane;
+         g < kSfxtQueues * seg; g += nhl) {
+      const int q = g % kSfxtQueues, k = g / kSfxtQueues;
+      if (k >= queue_count(p, q)) continue;
+      const int v = wait_slot_lane(p, q * seg + k);
       if (v < 0 || !wait_built(p, v) || !wait_heap(p, __ldcg(p.succ + v))) break;
       heap_insert<true>(p, v);
     }
@@ -1020,20 +1058,16 @@ sfxt_dataflow_kernel(SfxtParams p) {
 constexpr int kSortWarps = 8;
 
 __global__ void __launch_bounds__(kSortWarps * 32)
-sort_rows_kernel(const int32_t* order, const int* range, const int32_t* adjp,
-                 const int32_t* dev_cnt, DevSidetrack* dev, const int32_t* vgraph,
-                 const int32_t* graph_from, const int32_t* level_of) {
+sort_rows_kernel(const int32_t* rows, const int* n_rows, const int32_t* adjp,
+                 const int32_t* dev_cnt, DevSidetrack* dev) {
   __shared__ unsigned long long skey[kSortWarps][kSmemRow];
   __shared__ DevSidetrack srec[kSortWarps][kSmemRow];
   const int lane = threadIdx.x & 31;
   const int w = threadIdx.x >> 5;
-  const int beg = range[0], end = range[1];
-  for (int i = beg + blockIdx.x * kSortWarps + w; i < end; i += gridDim.x * kSortWarps) {
-    const int v = order[i];
+  const int end = *n_rows;  // the build listed the rows it left unsorted
+  for (int i = blockIdx.x * kSortWarps + w; i < end; i += gridDim.x * kSortWarps) {
+    const int v = rows[i];
     const int cnt = dev_cnt[v];
-    if (cnt <= 1 || cnt > kSmemRow) continue;
-    if (adjp[v + 1] - adjp[v] <= 64) continue;  // sorted when it was built
-    if (vgraph && level_of[v] < graph_from[vgraph[v]]) continue;  // not rebuilt
     DevSidetrack* row = dev + adjp[v];
     if (cnt <= 32) {
       DevSidetrack r;
@@ -1175,8 +1209,8 @@ int launch_sfxt(const SfxtParams& p, int device, void* stream, int* grid_out,
     e = cudaEventRecord(static_cast<cudaEvent_t>(ev_after), st);
     if (e != cudaSuccess) return e;
   }
-  sort_rows_kernel<<<sms * 8, kSortWarps * 32, 0, st>>>(
-      p.order, &p.ctr->sort_beg, p.adjp, p.dev_cnt, p.dev, p.vgraph, p.graph_from, p.level_of);
+  sort_rows_kernel<<<sms * 8, kSortWarps * 32, 0, st>>>(p.long_rows, &p.ctr->n_long, p.adjp,
+                                                        p.dev_cnt, p.dev);
   int n = 2;
   if (p.n_big_rows > 0) {
     const size_t smem = static_cast<size_t>(p.big_row_cap) * sizeof(unsigned long long);

@@ -216,6 +216,9 @@ __device__ void select_hist(const EngineParams& p, unsigned long long n_paths,
   const unsigned long long tot = np + n_pend;
   const unsigned long long pad = (tot + 31) & ~31ull;
   const bool single = p.nq == 1;
+  // one query: its mode and prefix hold for every element
+  const int mode0 = single ? __ldcg(&p.q[0].mode) : 0;
+  const unsigned prefix0 = single ? __ldcg(&p.q[0].prefix) : 0u;
   if (single) {
     for (int i = threadIdx.x; i < kSelBins; i += blockDim.x) sh[i] = 0;
     __syncthreads();
@@ -227,20 +230,20 @@ __device__ void select_hist(const EngineParams& p, unsigned long long n_paths,
       float c;
       int mode;
       if (i < np) {
-        q = static_cast<unsigned>(__ldcg(p.pq + i));
+        q = single ? 0u : static_cast<unsigned>(__ldcg(p.pq + i));
         c = __ldcg(p.ps.cost + i);
-        mode = __ldcg(&p.q[q].mode);
+        mode = single ? mode0 : __ldcg(&p.q[q].mode);
         on = (mode == 2 || mode == 3) && c != 0.0f;
       } else {
         const Item it = load_item(pend, i - np);
         q = q_of(it);
         c = it.cost;
-        mode = __ldcg(&p.q[q].mode);
+        mode = single ? mode0 : __ldcg(&p.q[q].mode);
         on = (mode == 2 && c != 0.0f) || mode == 1;
       }
       if (on) {
         key = float_key(c);
-        on = (key & hmask) == (__ldcg(&p.q[q].prefix) & hmask);
+        on = (key & hmask) == ((single ? prefix0 : __ldcg(&p.q[q].prefix)) & hmask);
       }
     }
     const unsigned bin = (key >> shift) & ((1u << bits) - 1u);
@@ -353,6 +356,8 @@ __device__ bool run_closure(const EngineParams& p, Item* pend_out) {
       static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   const unsigned long long nth = static_cast<unsigned long long>(gridDim.x) * blockDim.x;
   const bool single = p.nq == 1;
+  const float lim0 = single ? __ldcg(&p.q[0].lim) : 0.f;
+  const float tie0 = single ? __ldcg(&p.q[0].tie) : 0.f;
   unsigned acc_nz = 0, acc_pn = 0, acc_pnz = 0;
   int r = 0;
   for (;;) {
@@ -387,8 +392,8 @@ __device__ bool run_closure(const EngineParams& p, Item* pend_out) {
       hn.right = -1;
       float lim = 0.f, tie = 0.f;
       if (valid) {
-        lim = __ldcg(&p.q[q].lim);
-        tie = __ldcg(&p.q[q].tie);
+        lim = single ? lim0 : __ldcg(&p.q[q].lim);
+        tie = single ? tie0 : __ldcg(&p.q[q].tie);
         int from = -1, level = 0;
         if (it.node <= -2) {
           to = -(it.node + 2);
@@ -696,6 +701,9 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
     {
       const unsigned long long pad = (n_pend + 31) & ~31ull;
       const bool single = p.nq == 1;
+      const int mode0 = single ? __ldcg(&p.q[0].mode) : 0;
+      const int done0 = single ? __ldcg(&p.q[0].done) : 0;
+      const float lim0 = single ? __ldcg(&p.q[0].lim) : 0.f;
       unsigned acc_n = 0, acc_nz = 0;
       for (unsigned long long i = tid; i < pad; i += nth) {
         bool take = false, keep = false;
@@ -705,9 +713,9 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
         if (i < n_pend) {
           it = load_item(pend, i);
           const EngineQuery& Q = p.q[q_of(it)];
-          const int mode = __ldcg(&Q.mode);
-          const int done = __ldcg(&Q.done);
-          take = mode != 0 && it.cost <= __ldcg(&Q.lim);
+          const int mode = single ? mode0 : __ldcg(&Q.mode);
+          const int done = single ? done0 : __ldcg(&Q.done);
+          take = mode != 0 && it.cost <= (single ? lim0 : __ldcg(&Q.lim));
           keep = !take && !done;
         }
         const unsigned long long a = warp_append(&p.ctr->frontier[0], take);

@@ -166,6 +166,7 @@ def _load():
         "cpg_get_sfxt": (C.c_int, [H, C.c_void_p, C.c_void_p, C.c_void_p]),
         "cpg_num_levels": (C.c_int32, [H]),
         "cpg_report_paths": (C.c_int, [H, C.c_int64]),
+        "cpg_report_paths_batch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
         "cpg_get_costs": (C.c_int, [H, C.c_int64, C.c_void_p, P(C.c_int64)]),
         "cpg_get_paths": (C.c_int, [H, C.c_int64, C.c_void_p, P(C.c_int64)]),
         "cpg_get_costs_device": (C.c_int, [H, P(C.c_void_p), P(C.c_int64)]),
@@ -729,6 +730,15 @@ class Bvss:
                                                 C.byref(rs)), "discover_pairs")
         return buf[: 2 * n.value].reshape(-1, 2), {f: getattr(rs, f) for f, _ in
                                                    BvssRunStats._fields_ if f != "pad"}
+
+
+def report_paths_batch(handles, ks) -> None:
+    """cpg_report_paths_batch over CpGen handles."""
+    arr = (C.c_void_p * len(handles))(*[h._h.value for h in handles])
+    kk = np.ascontiguousarray(ks, np.int64)
+    st = lib.cpg_report_paths_batch(arr, _ptr(kk), len(handles))
+    if st != CPG_OK:
+        raise CpgError(st, "cpg_report_paths_batch failed")
 
 
 def select_topk(d_costs: int, n: int, k: int, d_out: int, stream: int | None = None) -> int:

@@ -1224,6 +1224,16 @@ cpg_status cpg_get_sfxt(cpg_handle* h, int32_t* dist, int32_t* succ,
 
 int32_t cpg_num_levels(const cpg_handle* h) { return h ? h->levels : 0; }
 
+cpg_status cpg_report_paths_batch(cpg_handle* const* handles, const int64_t* ks, int32_t n) {
+  if (n < 0 || (n > 0 && (!handles || !ks))) return CPG_ERR_INVALID;
+  cpg_status first = CPG_OK;
+  for (int32_t i = 0; i < n; ++i) {
+    const cpg_status st = cpg_report_paths(handles[i], ks[i]);
+    if (st != CPG_OK && first == CPG_OK) first = st;
+  }
+  return first;
+}
+
 cpg_status cpg_report_paths(cpg_handle* h, int64_t k) {
   if (check_handle(h) != CPG_OK || k < 0) return CPG_ERR_INVALID;
   if (!h->has_graph) return fail(h, CPG_ERR_STATE, "no graph loaded");

@@ -188,6 +188,11 @@ int32_t cpg_num_levels(const cpg_handle* h);
  * ascending, kept on the device until fetched.  Builds the suffix tree first
  * if it is not current.  Fewer than k paths are returned if fewer exist. */
 cpg_status cpg_report_paths(cpg_handle* h, int64_t k);
+/* report_paths on n handles (query i asks handles[i] for ks[i] paths), the
+ * same as n cpg_report_paths calls; all queries are attempted and the first
+ * failing status is returned (cpg_last_error of that handle says why).  For
+ * many queries in one launch over side-by-side graphs, see cpg_batch_*. */
+cpg_status cpg_report_paths_batch(cpg_handle* const* handles, const int64_t* ks, int32_t n);
 /* get_slacks(k) (gpucpg.cu:21409-21420): copies min(k, available) costs. */
 cpg_status cpg_get_costs(const cpg_handle* h, int64_t k, float* out,
                          int64_t* n_out);

@@ -323,3 +323,21 @@ def test_many_incremental_updates_overflow_pool_and_stay_exact():
     np.testing.assert_array_equal(s, s2)
     np.testing.assert_array_equal(lv, lv2)
     assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+def test_report_paths_batch_equals_single_calls():
+    names = ["simple", "single20k_f32", "small_int_s13"]
+    ks = [500, 3000, 2000]
+    handles = []
+    for name in names:
+        n, src, dst, w = _load(name)
+        g = cpg_b200.CpGen(division=cpg_b200.DIV_IEEE)
+        g.load_edges(n, src, dst, w)
+        handles.append(g)
+    cpg_b200.report_paths_batch(handles, ks)
+    got = [g.get_slacks(k) for g, k in zip(handles, ks)]
+    for g, k, name, a in zip(handles, ks, names, got):
+        n, src, dst, w = _load(name)
+        b, _, _, _ = _run(n, src, dst, w, k)
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), name
+        g.close()

@@ -612,6 +612,54 @@ def run_bvss(args):
     print(json.dumps(out), flush=True)
 
 
+def run_ingest(args):
+    """Graph ingestion on the 1M-pin workload: the text file parsed on the host
+    threads, read_input to a device graph, the binary CSR file to a device
+    graph, and the oracle's sequential text parser beside them."""
+    import tempfile
+    import cpg_b200
+    import cases
+    import oracle
+    c = cases.CASES[WORKLOAD]
+    with tempfile.TemporaryDirectory() as tmp:
+        txt, binp = os.path.join(tmp, "g.txt"), os.path.join(tmp, "g.bin")
+        dag = cpg_b200.generate(cpg_b200.gen_params(**c["gen"]), text_path=txt, csr_bin_path=binp)
+        out = {"form": "ingest", "workload": WORKLOAD, "n": dag.n, "m": dag.m,
+               "text_bytes": os.path.getsize(txt), "bin_bytes": os.path.getsize(binp),
+               "host_threads": os.cpu_count()}
+
+        def timed(fn):
+            ts = []
+            for _ in range(args.warmup + args.steps):
+                t0 = time.perf_counter()
+                fn()
+                ts.append(time.perf_counter() - t0)
+            return float(np.median(ts[args.warmup:]))
+
+        t = timed(lambda: cpg_b200.read_text(txt))
+        out["text_parse"] = {"s": t, "medges_per_s": dag.m / t / 1e6}
+        with cpg_b200.CpGen() as g:
+            def load_text():
+                g.read_input(txt)
+                g.sync()
+
+            def load_bin():
+                g.load_csr_bin(binp)
+                g.sync()
+            t = timed(load_text)
+            out["read_input_to_device"] = {"s": t, "medges_per_s": dag.m / t / 1e6}
+            t = timed(load_bin)
+            out["csr_bin_to_device"] = {"s": t, "medges_per_s": dag.m / t / 1e6,
+                                        "gb_per_s": out["bin_bytes"] / t / 1e9}
+        t0 = time.perf_counter()
+        oracle.OracleGraph.from_text(txt)
+        t = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": dag.m / t / 1e6, "unit": "M edges/s", "cores": 1,
+                               "kind": "port", "sample": "the whole text file, once",
+                               "s": t}
+    print(json.dumps(out), flush=True)
+
+
 def run_profile_case(args):
     """A short fixed sequence for ncu: one warm-up query, then one query
     (suffix tree + engine) on the same workload at --k."""
@@ -639,7 +687,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-case", action="store_true",
                     help="one warm-up and one measured query only (for ncu)")
-    ap.add_argument("--form", default="plain", choices=["plain", "batched", "served", "bvss"])
+    ap.add_argument("--form", default="plain", choices=["plain", "batched", "served", "bvss", "ingest"])
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="batched form: skip cpg_batch_autotune before timing")
     ap.add_argument("--served-queries", type=int, default=5000)
@@ -653,6 +701,8 @@ def main():
         run_served(args)
     elif args.form == "bvss":
         run_bvss(args)
+    elif args.form == "ingest":
+        run_ingest(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

@@ -26,6 +26,7 @@ STATUS_NAMES = {
     4: "CPG_ERR_CAPACITY", 5: "CPG_ERR_TIMEOUT", 6: "CPG_ERR_CUDA",
     7: "CPG_ERR_STATE", 8: "CPG_ERR_NO_DEVICE",
 }
+CPG_ERR_INVALID, CPG_ERR_IO, CPG_ERR_OOM = 1, 2, 3
 DIV_REFERENCE = 0
 DIV_IEEE = 1
 FRONTIER_AUTO, FRONTIER_CSR, FRONTIER_BVSS = 0, 1, 2
@@ -223,6 +224,12 @@ def _load():
         "cpg_dag_sizes": (C.c_int, [C.c_void_p, P(C.c_int32), P(C.c_int32)]),
         "cpg_dag_edges": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
         "cpg_dag_write_text": (C.c_int, [C.c_void_p, C.c_char_p]),
+        "cpg_dag_read_text": (C.c_int, [C.c_char_p, C.c_int32, P(C.c_void_p)]),
+        "cpg_dag_last_error": (C.c_char_p, []),
+        "cpg_dag_read_csr_bin": (C.c_int, [C.c_char_p, P(C.c_void_p)]),
+        "cpg_dag_write_csr_bin": (C.c_int, [C.c_void_p, C.c_char_p]),
+        "cpg_load_csr_bin": (C.c_int, [H, C.c_char_p]),
+        "cpg_write_csr_bin": (C.c_int, [H, C.c_char_p]),
         "cpg_load_dag": (C.c_int, [H, C.c_void_p]),
         "cpg_dag_free": (None, [C.c_void_p]),
     }
@@ -263,26 +270,79 @@ def gen_params(**kw) -> GenParams:
     return p
 
 
-def generate(params: GenParams, text_path: str | None = None) -> Dag:
-    """Seeded levelised DAG (host-only; no GPU needed)."""
+def _dag_from_handle(h) -> Dag:
+    n, m = C.c_int32(), C.c_int32()
+    lib.cpg_dag_sizes(h, C.byref(n), C.byref(m))
+    src = np.empty(m.value, np.int32)
+    dst = np.empty(m.value, np.int32)
+    w = np.empty(m.value, np.float32)
+    lib.cpg_dag_edges(h, _ptr(src), _ptr(dst), _ptr(w))
+    return Dag(n.value, src, dst, w)
+
+
+def generate(params: GenParams, text_path: str | None = None,
+             csr_bin_path: str | None = None) -> Dag:
+    """Seeded levelised DAG (host-only; no GPU needed), optionally also
+    written as a text file and as a binary CSR file."""
     h = C.c_void_p()
     st = lib.cpg_dag_generate(C.byref(params), C.byref(h))
     if st != CPG_OK:
         raise CpgError(st, "generator rejected the parameters")
     try:
-        n, m = C.c_int32(), C.c_int32()
-        lib.cpg_dag_sizes(h, C.byref(n), C.byref(m))
-        src = np.empty(m.value, np.int32)
-        dst = np.empty(m.value, np.int32)
-        w = np.empty(m.value, np.float32)
-        lib.cpg_dag_edges(h, _ptr(src), _ptr(dst), _ptr(w))
         if text_path is not None:
             st = lib.cpg_dag_write_text(h, text_path.encode())
             if st != CPG_OK:
                 raise CpgError(st, f"cannot write {text_path}")
-        return Dag(n.value, src, dst, w)
+        if csr_bin_path is not None:
+            st = lib.cpg_dag_write_csr_bin(h, csr_bin_path.encode())
+            if st != CPG_OK:
+                raise CpgError(st, lib.cpg_dag_last_error().decode())
+        return _dag_from_handle(h)
     finally:
         lib.cpg_dag_free(h)
+
+
+def read_text(path: str, ignore_wgts: bool = False) -> Dag:
+    """Parse a graph in the reference's text format on the host threads
+    (the parsing half of CpGen::read_input, gpucpg.cu:453-548)."""
+    h = C.c_void_p()
+    st = lib.cpg_dag_read_text(path.encode(), int(ignore_wgts), C.byref(h))
+    if st != CPG_OK:
+        raise CpgError(st, lib.cpg_dag_last_error().decode())
+    try:
+        return _dag_from_handle(h)
+    finally:
+        lib.cpg_dag_free(h)
+
+
+def read_csr_bin(path: str) -> Dag:
+    """Binary CSR file (the layout of Graph::read_from_bin, gpucpg/graph.h:40-56)
+    as an edge list in row order."""
+    h = C.c_void_p()
+    st = lib.cpg_dag_read_csr_bin(path.encode(), C.byref(h))
+    if st != CPG_OK:
+        raise CpgError(st, lib.cpg_dag_last_error().decode())
+    try:
+        return _dag_from_handle(h)
+    finally:
+        lib.cpg_dag_free(h)
+
+
+def write_csr_bin(dag: Dag, path: str) -> None:
+    """Binary CSR file of an edge list (rows keep the list's order)."""
+    n = dag.n
+    src = np.ascontiguousarray(dag.src, np.int32)
+    dst = np.ascontiguousarray(dag.dst, np.int32)
+    w = np.ascontiguousarray(dag.w, np.float32)
+    order = np.argsort(src, kind="stable")
+    adjp = np.zeros(n + 1, np.int64)
+    np.add.at(adjp, src.astype(np.int64) + 1, 1)
+    adjp = np.cumsum(adjp).astype(np.int32)
+    with open(path, "wb") as f:
+        f.write(np.array([n, src.size], np.int32).tobytes())
+        f.write(adjp.tobytes())
+        f.write(dst[order].tobytes())
+        f.write(w[order].tobytes())
 
 
 def write_text(dag: Dag, path: str) -> None:
@@ -368,6 +428,14 @@ class CpGen:
         w = np.ascontiguousarray(w, np.float32)
         self._check(lib.cpg_load_csr(self._h, int(n), int(adjncy.size), _ptr(adjp), _ptr(adjncy), _ptr(w)),
                     "load_csr")
+
+    def load_csr_bin(self, path: str):
+        """Binary CSR file (Graph::read_from_bin layout, gpucpg/graph.h:40-56)."""
+        self._check(lib.cpg_load_csr_bin(self._h, path.encode()), "load_csr_bin")
+
+    def write_csr_bin(self, path: str):
+        """CpGen::write_to_csr_bin (gpucpg.cuh:313-324), with the real offsets."""
+        self._check(lib.cpg_write_csr_bin(self._h, path.encode()), "write_csr_bin")
 
     def num_verts(self) -> int:
         return int(lib.cpg_num_verts(self._h))

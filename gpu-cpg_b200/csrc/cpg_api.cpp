@@ -1106,6 +1106,26 @@ cpg_status cpg_load_text(cpg_handle* h, const char* path, int32_t ignore_wgts) {
   return load_edgelist(h, el);
 }
 
+cpg_status cpg_load_csr_bin(cpg_handle* h, const char* path) {
+  if (check_handle(h) != CPG_OK || !path) return CPG_ERR_INVALID;
+  HostGraph g;
+  Status st = read_csr_bin(path, g, h->err);
+  if (st != CPG_OK) return st;
+  return upload_graph(h, g.n, g.m, g.adjp.data(), g.adj.data(), g.w.data());
+}
+
+cpg_status cpg_write_csr_bin(const cpg_handle* h, const char* path) {
+  if (!h || !path) return CPG_ERR_INVALID;
+  if (!h->has_graph) return CPG_ERR_STATE;
+  const int32_t n = h->g.n, m = h->g.m;
+  std::vector<int32_t> adjp(static_cast<size_t>(n) + 1), adj(static_cast<size_t>(m));
+  std::vector<float> w(static_cast<size_t>(m));
+  Status st = cpg_get_csr(h, adjp.data(), adj.data(), w.data());
+  if (st != CPG_OK) return st;
+  cpg_handle* hm = const_cast<cpg_handle*>(h);
+  return write_csr_bin(n, m, adjp.data(), adj.data(), w.data(), path, hm->err);
+}
+
 cpg_status cpg_load_edges(cpg_handle* h, int32_t n, int32_t m,
                           const int32_t* src, const int32_t* dst,
                           const float* w) {
@@ -1431,6 +1451,12 @@ cpg_status cpg_select_topk(const float* d_costs, int64_t n, int64_t k, float* d_
 struct cpg_dag {
   EdgeList el;
 };
+
+// message of the last failing host-side graph call on this thread
+static std::string& dag_err() {
+  static thread_local std::string e;
+  return e;
+}
 
 struct cpg_batch {
   cpg_handle* h = nullptr;          // owns the side-by-side device graph
@@ -2176,8 +2202,7 @@ cpg_status cpg_dag_generate(const cpg_gen_params* p, cpg_dag** out) {
   if (!p || !out) return CPG_ERR_INVALID;
   cpg_dag* d = new (std::nothrow) cpg_dag();
   if (!d) return CPG_ERR_OOM;
-  std::string err;
-  Status st = generate_dag(*p, d->el, err);
+  Status st = generate_dag(*p, d->el, dag_err());
   if (st != CPG_OK) {
     delete d;
     return st;
@@ -2202,10 +2227,55 @@ cpg_status cpg_dag_edges(const cpg_dag* d, int32_t* src, int32_t* dst, float* w)
   return CPG_OK;
 }
 
+cpg_status cpg_dag_read_text(const char* path, int32_t ignore_wgts, cpg_dag** out) {
+  if (!path || !out) {
+    dag_err() = "null argument";
+    return CPG_ERR_INVALID;
+  }
+  cpg_dag* d = new (std::nothrow) cpg_dag();
+  if (!d) return CPG_ERR_OOM;
+  Status st = read_text_graph(path, ignore_wgts != 0, d->el, dag_err());
+  if (st != CPG_OK) {
+    delete d;
+    return st;
+  }
+  *out = d;
+  return CPG_OK;
+}
+
+cpg_status cpg_dag_read_csr_bin(const char* path, cpg_dag** out) {
+  if (!path || !out) {
+    dag_err() = "null argument";
+    return CPG_ERR_INVALID;
+  }
+  HostGraph g;
+  Status st = read_csr_bin(path, g, dag_err());
+  if (st != CPG_OK) return st;
+  cpg_dag* d = new (std::nothrow) cpg_dag();
+  if (!d) return CPG_ERR_OOM;
+  d->el.n = g.n;
+  d->el.src.resize(static_cast<size_t>(g.m));
+  for (int32_t v = 0; v < g.n; ++v)
+    std::fill(d->el.src.begin() + g.adjp[v], d->el.src.begin() + g.adjp[v + 1], v);
+  d->el.dst = std::move(g.adj);
+  d->el.w = std::move(g.w);
+  *out = d;
+  return CPG_OK;
+}
+
+cpg_status cpg_dag_write_csr_bin(const cpg_dag* d, const char* path) {
+  if (!d || !path) return CPG_ERR_INVALID;
+  HostGraph g;
+  Status st = edges_to_csr(d->el, g, dag_err());
+  if (st != CPG_OK) return st;
+  return write_csr_bin(g.n, g.m, g.adjp.data(), g.adj.data(), g.w.data(), path, dag_err());
+}
+
+const char* cpg_dag_last_error(void) { return dag_err().c_str(); }
+
 cpg_status cpg_dag_write_text(const cpg_dag* d, const char* path) {
   if (!d || !path) return CPG_ERR_INVALID;
-  std::string err;
-  return write_text_graph(d->el, path, err);
+  return write_text_graph(d->el, path, dag_err());
 }
 
 cpg_status cpg_load_dag(cpg_handle* h, const cpg_dag* d) {

@@ -38,6 +38,9 @@ Status csr_to_graph(int32_t n, int32_t m, const int32_t* adjp,
                     std::string& err);
 Status generate_dag(const cpg_gen_params& p, EdgeList& out, std::string& err);
 Status write_text_graph(const EdgeList& el, const char* path, std::string& err);
+Status write_csr_bin(int32_t n, int32_t m, const int32_t* adjp, const int32_t* adj,
+                     const float* w, const char* path, std::string& err);
+Status read_csr_bin(const char* path, HostGraph& g, std::string& err);
 
 // ---------------------------------------------------------------- device data
 // One fan-out edge: head vertex and delay, loaded as one 8-byte word.

@@ -165,6 +165,16 @@ int64_t cpg_num_edges(const cpg_handle* h);
 /* Copy the fan-out CSR back (host buffers of n+1, m, m; any may be NULL). */
 cpg_status cpg_get_csr(const cpg_handle* h, int32_t* adjp, int32_t* adjncy,
                        float* w);
+/* Binary CSR file: int32 N, int32 M, int32 adjp[N+1], int32 adjncy[M],
+ * float w[M] in host byte order (the layout of Graph::write_to_bin and
+ * read_from_bin, gpucpg/graph.h:24-56), read on the host threads and checked
+ * (size against the header, offsets rising from 0 to M, heads in range).
+ * cpg_load_csr_bin stands for read_input + the CSR build on such a file;
+ * cpg_write_csr_bin for CpGen::write_to_csr_bin (gpucpg.cuh:313-324), which
+ * writes the adjacency where the offsets belong, so files it wrote fail the
+ * offset check here. */
+cpg_status cpg_load_csr_bin(cpg_handle* h, const char* path);
+cpg_status cpg_write_csr_bin(const cpg_handle* h, const char* path);
 
 /* ------------------------------------------------------------ suffix tree */
 /* LEVELIZE_THEN_RELAX + update_successors_bu (gpucpg.cu:17642-17963,
@@ -476,6 +486,19 @@ cpg_status cpg_dag_sizes(const cpg_dag* d, int32_t* n, int32_t* m);
 cpg_status cpg_dag_edges(const cpg_dag* d, int32_t* src, int32_t* dst,
                          float* w);
 cpg_status cpg_dag_write_text(const cpg_dag* d, const char* path);
+/* Parse a graph in the reference's text format (the header line N, N vertex
+ * name lines, then edge lines "u" -> "v"[, w];) into a host-side graph, in
+ * parallel on the host threads.  Replaces the parsing half of
+ * CpGen::read_input (gpucpg.cu:453-548); edges keep file order, blank lines
+ * are skipped, and a malformed edge line fails with CPG_ERR_IO and its line
+ * number in cpg_dag_last_error().  Host-only. */
+cpg_status cpg_dag_read_text(const char* path, int32_t ignore_wgts, cpg_dag** out);
+/* The binary CSR file above, to and from a host-side graph (rows keep the
+ * edge order of the file).  Host-only. */
+cpg_status cpg_dag_read_csr_bin(const char* path, cpg_dag** out);
+cpg_status cpg_dag_write_csr_bin(const cpg_dag* d, const char* path);
+/* Message of the last failing cpg_dag_* call on this thread. */
+const char* cpg_dag_last_error(void);
 cpg_status cpg_load_dag(cpg_handle* h, const cpg_dag* d);
 void cpg_dag_free(cpg_dag* d);
 

@@ -619,6 +619,7 @@ def run_ingest(args):
     import tempfile
     import cpg_b200
     import cases
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     c = cases.CASES[WORKLOAD]
     with tempfile.TemporaryDirectory() as tmp:

@@ -302,14 +302,19 @@ def generate(params: GenParams, text_path: str | None = None,
         lib.cpg_dag_free(h)
 
 
-def read_text(path: str, ignore_wgts: bool = False) -> Dag:
+def read_text(path: str, ignore_wgts: bool = False, csr_bin_path: str | None = None) -> Dag:
     """Parse a graph in the reference's text format on the host threads
-    (the parsing half of CpGen::read_input, gpucpg.cu:453-548)."""
+    (the parsing half of CpGen::read_input, gpucpg.cu:453-548); optionally
+    also write it as a binary CSR file."""
     h = C.c_void_p()
     st = lib.cpg_dag_read_text(path.encode(), int(ignore_wgts), C.byref(h))
     if st != CPG_OK:
         raise CpgError(st, lib.cpg_dag_last_error().decode())
     try:
+        if csr_bin_path is not None:
+            st = lib.cpg_dag_write_csr_bin(h, csr_bin_path.encode())
+            if st != CPG_OK:
+                raise CpgError(st, lib.cpg_dag_last_error().decode())
         return _dag_from_handle(h)
     finally:
         lib.cpg_dag_free(h)

@@ -378,9 +378,12 @@ Status upload_graph(cpg_handle* h, int32_t n, int32_t m, const int32_t* adjp,
 
 Status load_edgelist(cpg_handle* h, const EdgeList& el) {
   HostGraph g;
-  Status st = edges_to_csr(el, g, h->err);
+  bool grouped = false;
+  Status st = edges_to_csr(el, g, h->err, &grouped);
   if (st != CPG_OK) return st;
-  return upload_graph(h, g.n, g.m, g.adjp.data(), g.adj.data(), g.w.data());
+  // a list grouped by tail is its own adjacency
+  return grouped ? upload_graph(h, g.n, g.m, g.adjp.data(), el.dst.data(), el.w.data())
+                 : upload_graph(h, g.n, g.m, g.adjp.data(), g.adj.data(), g.w.data());
 }
 
 SfxtParams sfxt_params(cpg_handle* h, int32_t start_level) {

@@ -27,15 +27,12 @@ struct HostGraph {
   int32_t n = 0, m = 0;
   std::vector<int32_t> adjp, adj;  // fan-out CSR, rows in file order
   std::vector<float> w;
-  std::vector<int32_t> iadjp, iadj;  // fan-in CSR
 };
 
 Status read_text_graph(const char* path, bool ignore_wgts, EdgeList& out,
                        std::string& err);
-Status edges_to_csr(const EdgeList& el, HostGraph& g, std::string& err);
-Status csr_to_graph(int32_t n, int32_t m, const int32_t* adjp,
-                    const int32_t* adjncy, const float* w, HostGraph& g,
-                    std::string& err);
+Status edges_to_csr(const EdgeList& el, HostGraph& g, std::string& err,
+                    bool* grouped = nullptr);
 Status generate_dag(const cpg_gen_params& p, EdgeList& out, std::string& err);
 Status write_text_graph(const EdgeList& el, const char* path, std::string& err);
 Status write_csr_bin(int32_t n, int32_t m, const int32_t* adjp, const int32_t* adj,

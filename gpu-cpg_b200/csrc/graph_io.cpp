@@ -342,72 +342,99 @@ Status read_text_graph(const char* path, bool ignore_wgts, EdgeList& out,
   return CPG_OK;
 }
 
-Status edges_to_csr(const EdgeList& el, HostGraph& g, std::string& err) {
+// Fan-out CSR of an edge list; each row keeps the list's order (the
+// reference's unordered_map of vectors, gpucpg.cu:500-541).  Runs on the host
+// threads.  A list already grouped by tail (a text file written row by row) is
+// taken as it is: only the offsets are computed and, when `grouped` is given,
+// the heads and delays are left in the list for the caller to use.  Otherwise
+// each thread counts the tails of its contiguous slice, per-thread row offsets
+// follow from the counts, and each thread scatters its slice in order, so
+// every row stays in list order.
+Status edges_to_csr(const EdgeList& el, HostGraph& g, std::string& err, bool* grouped) {
   const int64_t n = el.n;
   const int64_t m = static_cast<int64_t>(el.src.size());
   if (m > INT32_MAX - 1) {
     err = "too many edges for 32-bit CSR offsets";
     return CPG_ERR_INVALID;
   }
+  if (grouped) *grouped = false;
   g.n = el.n;
   g.m = static_cast<int32_t>(m);
-  g.adjp.assign(n + 1, 0);
-  g.iadjp.assign(n + 1, 0);
+  int threads = io_threads(m * 12);
+  const int32_t* src = el.src.data();
+  const int32_t* dst = el.dst.data();
+  int64_t bad = INT64_MAX;
+  int unsorted = 0;
+#pragma omp parallel for num_threads(threads) reduction(min : bad) reduction(| : unsorted)
   for (int64_t e = 0; e < m; ++e) {
-    if (el.src[e] < 0 || el.src[e] >= n || el.dst[e] < 0 || el.dst[e] >= n) {
-      err = "edge endpoint out of range";
-      return CPG_ERR_INVALID;
+    if (src[e] < 0 || src[e] >= n || dst[e] < 0 || dst[e] >= n) bad = std::min(bad, e);
+    if (e > 0 && src[e] < src[e - 1]) unsorted = 1;
+  }
+  if (bad != INT64_MAX) {
+    err = "edge endpoint out of range at edge " + std::to_string(bad);
+    return CPG_ERR_INVALID;
+  }
+  g.adjp.assign(static_cast<size_t>(n) + 1, 0);
+  int32_t* adjp = g.adjp.data();
+  if (!unsorted) {
+    // row ends where the tail changes; rows with no edges take the next end
+#pragma omp parallel for num_threads(threads)
+    for (int64_t e = 0; e < m; ++e)
+      if (e == m - 1 || src[e] != src[e + 1]) adjp[src[e] + 1] = static_cast<int32_t>(e + 1);
+    for (int64_t v = 0; v < n; ++v) adjp[v + 1] = std::max(adjp[v + 1], adjp[v]);
+    if (grouped) {
+      *grouped = true;
+      g.adj.clear();
+      g.w.clear();
+    } else {
+      g.adj = el.dst;
+      g.w = el.w;
     }
-    g.adjp[el.src[e] + 1]++;
-    g.iadjp[el.dst[e] + 1]++;
+    return CPG_OK;
   }
+  // per-thread counts: at most 2^28 counters in all
+  if (n > 0) threads = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(threads, (int64_t{1} << 28) / n)));
+  std::vector<int32_t> cnt(static_cast<size_t>(threads) * static_cast<size_t>(n));
+  auto slice = [&](int t, int64_t& b, int64_t& e) {
+    b = m * t / threads;
+    e = m * (t + 1) / threads;
+  };
+#pragma omp parallel for num_threads(threads) schedule(static, 1)
+  for (int t = 0; t < threads; ++t) {
+    int32_t* c = cnt.data() + static_cast<size_t>(t) * n;
+    std::fill(c, c + n, 0);
+    int64_t b, e;
+    slice(t, b, e);
+    for (int64_t x = b; x < e; ++x) ++c[src[x]];
+  }
+  // cnt[t][v] becomes thread t's offset inside row v; adjp[v + 1] the degree
+#pragma omp parallel for num_threads(threads) schedule(static)
   for (int64_t v = 0; v < n; ++v) {
-    g.adjp[v + 1] += g.adjp[v];
-    g.iadjp[v + 1] += g.iadjp[v];
+    int32_t run = 0;
+    for (int t = 0; t < threads; ++t) {
+      int32_t& c = cnt[static_cast<size_t>(t) * n + v];
+      const int32_t k = c;
+      c = run;
+      run += k;
+    }
+    adjp[v + 1] = run;
   }
-  g.adj.resize(m);
-  g.w.resize(m);
-  g.iadj.resize(m);
-  std::vector<int32_t> fill(n, 0);
-  for (int64_t e = 0; e < m; ++e) {
-    int32_t s = el.src[e];
-    int32_t p = g.adjp[s] + fill[s]++;
-    g.adj[p] = el.dst[e];
-    g.w[p] = el.w[e];
-  }
-  std::fill(fill.begin(), fill.end(), 0);
-  for (int64_t e = 0; e < m; ++e) {
-    int32_t d = el.dst[e];
-    int32_t p = g.iadjp[d] + fill[d]++;
-    g.iadj[p] = el.src[e];
+  for (int64_t v = 0; v < n; ++v) adjp[v + 1] += adjp[v];
+  g.adj.resize(static_cast<size_t>(m));
+  g.w.resize(static_cast<size_t>(m));
+#pragma omp parallel for num_threads(threads) schedule(static, 1)
+  for (int t = 0; t < threads; ++t) {
+    int32_t* c = cnt.data() + static_cast<size_t>(t) * n;
+    int64_t b, e;
+    slice(t, b, e);
+    for (int64_t x = b; x < e; ++x) {
+      const int32_t v = src[x];
+      const int32_t p = adjp[v] + c[v]++;
+      g.adj[p] = dst[x];
+      g.w[p] = el.w[x];
+    }
   }
   return CPG_OK;
-}
-
-Status csr_to_graph(int32_t n, int32_t m, const int32_t* adjp,
-                    const int32_t* adjncy, const float* w, HostGraph& g,
-                    std::string& err) {
-  if (n < 0 || m < 0 || !adjp || (m > 0 && (!adjncy || !w))) {
-    err = "null CSR buffer";
-    return CPG_ERR_INVALID;
-  }
-  if (adjp[0] != 0 || adjp[n] != m) {
-    err = "CSR offsets must start at 0 and end at m";
-    return CPG_ERR_INVALID;
-  }
-  EdgeList el;
-  el.n = n;
-  el.src.resize(m);
-  el.dst.assign(adjncy, adjncy + m);
-  el.w.assign(w, w + m);
-  for (int32_t v = 0; v < n; ++v) {
-    if (adjp[v] > adjp[v + 1]) {
-      err = "CSR offsets must be non-decreasing";
-      return CPG_ERR_INVALID;
-    }
-    for (int32_t e = adjp[v]; e < adjp[v + 1]; ++e) el.src[e] = v;
-  }
-  return edges_to_csr(el, g, err);
 }
 
 // ------------------------------------------------------------------ generator
@@ -606,8 +633,6 @@ Status read_csr_bin(const char* path, HostGraph& g, std::string& err) {
   g.adjp.resize(static_cast<size_t>(n) + 1);
   g.adj.resize(static_cast<size_t>(m));
   g.w.resize(static_cast<size_t>(m));
-  g.iadjp.clear();
-  g.iadj.clear();
   const long off_adj = 8 + 4 * (n + 1), off_w = off_adj + 4 * m;
   if (!read_range(path, 8, reinterpret_cast<char*>(g.adjp.data()), 4 * (n + 1), threads) ||
       (m > 0 && (!read_range(path, off_adj, reinterpret_cast<char*>(g.adj.data()), 4 * m, threads) ||

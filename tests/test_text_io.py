@@ -245,3 +245,20 @@ def test_csr_bin_empty_graph(tmp_path):
     _bin(path, 0, [0], [], [])
     d = cpg_b200.read_csr_bin(path)
     assert d.n == 0 and d.m == 0
+
+
+@pytest.mark.parametrize("m", [5_000, 400_000])
+def test_csr_of_unordered_edge_list_keeps_list_order(tmp_path, m):
+    # edges in random order (and repeated pairs): every row keeps the list's
+    # order; the larger list is built on several threads
+    rng = np.random.default_rng(m)
+    n = 3_000
+    src = rng.integers(0, n, m).astype(np.int32)
+    dst = rng.integers(0, n, m).astype(np.int32)
+    w = np.arange(m, dtype=np.float32)  # the delay records the list position
+    path, binp, want = str(tmp_path / "g.txt"), str(tmp_path / "g.bin"), str(tmp_path / "w.bin")
+    d = cpg_b200.Dag(n, src, dst, w)
+    cpg_b200.write_text(d, path)
+    cpg_b200.read_text(path, csr_bin_path=binp)
+    cpg_b200.write_csr_bin(d, want)
+    assert open(binp, "rb").read() == open(want, "rb").read()

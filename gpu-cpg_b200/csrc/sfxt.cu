@@ -427,7 +427,7 @@ __device__ void heap_insert(const SfxtParams& p, int v, unsigned long long* chun
   heap_store<kPublish>(p, v, static_cast<int>(a), static_cast<int>(pos));
 }
 
-// BVSS form of the Kahn step.// BVSS form of the Kahn step.  A vertex that joins level L sets its bit in
+// BVSS form of the Kahn step.  A vertex that joins level L sets its bit in
 // the level-parity frontier bitmap fbits[L & 1] and, first in its interval of
 // 8, appends the interval to act_list.  Pulling level L, one warp per active
 // interval counts for every slice (row u, mask of u's heads in the interval)

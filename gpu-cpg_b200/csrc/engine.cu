@@ -261,11 +261,10 @@ __device__ void select_hist(const EngineParams& p, unsigned long long n_paths,
   }
 }
 
-// One warp per selecting query: find the bin holding the krem-th key.
-__device__ void select_pick(const EngineParams& p, int shift, int bits) {
+// One warp per selecting query (warps gw, gw + nw, ...): find the bin
+// holding the krem-th key.
+__device__ void select_pick(const EngineParams& p, int shift, int bits, int gw, int nw) {
   const int lane = threadIdx.x & 31;
-  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nw = (gridDim.x * blockDim.x) >> 5;
   const int bins = 1 << bits;
   const int per = bins / 32;
   for (int qi = gw; qi < p.nq; qi += nw) {
@@ -301,13 +300,65 @@ __device__ void select_pick(const EngineParams& p, int shift, int bits) {
   }
 }
 
+// D. The split and acceptance limit of every selecting query (threads t0,
+// t0 + nt, ...), and the cursors the promotion starts from.
+__device__ void set_limits(const EngineParams& p, unsigned t0, unsigned nt, bool reset) {
+  for (unsigned qi = t0; qi < static_cast<unsigned>(p.nq); qi += nt) {
+    EngineQuery& Q = p.q[qi];
+    if (Q.mode == 0) continue;
+    const float t = key_float(Q.prefix);
+    Q.t = t;
+    if (Q.mode == 2) {
+      const float a = fmaxf(fmaxf(fabsf(t), Q.root_abs), 1.0f);
+      Q.lim = t + a * 0x1p-16f;
+      Q.tie = t;
+    } else {
+      // accept strictly below the split when anything pending is cheaper
+      // than it (ksel - krem items are), so a tie group at the split waits
+      Q.lim = Q.ksel > Q.krem ? float_below(t) : t;
+      Q.tie = __int_as_float(0x7fc00000);  // NaN: expand every path
+    }
+  }
+  if (reset) {
+    p.ctr->frontier[0] = 0;
+    p.ctr->frontier[1] = 0;
+    p.ctr->frontier[2] = 0;
+    p.ctr->pend_out = 0;
+  }
+}
+
+// The per-query radix select, then (with_limits) the split and limits.
+// With at most one query per warp of a block, the last block to finish a
+// histogram pass picks the bins itself before releasing the barrier, so a
+// pass costs one grid barrier instead of two (and the limits none).
 __device__ bool run_select(const EngineParams& p, unsigned long long n_paths,
-                           const Item* pend, unsigned long long n_pend) {
+                           const Item* pend, unsigned long long n_pend, bool with_limits) {
+  const bool fused = p.nq <= kEngWarps;
   for (int pass = 0; pass < p.sel_passes; ++pass) {
-    select_hist(p, n_paths, pend, n_pend, p.sel_shift[pass], p.sel_bits[pass]);
-    if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit)) return false;
-    select_pick(p, p.sel_shift[pass], p.sel_bits[pass]);
-    if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit)) return false;
+    const int shift = p.sel_shift[pass], bits = p.sel_bits[pass];
+    const bool last = pass == p.sel_passes - 1;
+    select_hist(p, n_paths, pend, n_pend, shift, bits);
+    if (fused) {
+      if (!grid_sync_last(&p.ctr->bar, &p.ctr->err, p.spin_limit, [&]() {
+            select_pick(p, shift, bits, static_cast<int>(threadIdx.x >> 5),
+                        static_cast<int>(blockDim.x >> 5));
+            if (last && with_limits) {
+              __syncthreads();
+              set_limits(p, threadIdx.x, blockDim.x, threadIdx.x == 0);
+            }
+          }))
+        return false;
+    } else {
+      if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit)) return false;
+      select_pick(p, shift, bits, static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 5),
+                  static_cast<int>((gridDim.x * blockDim.x) >> 5));
+      if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit)) return false;
+      if (last && with_limits) {
+        set_limits(p, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x,
+                   blockIdx.x == 0 && threadIdx.x == 0);
+        if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit)) return false;
+      }
+    }
   }
   return true;
 }
@@ -591,6 +642,84 @@ __device__ bool lsd_pass(const EngineParams& p, unsigned long long n, int src,
   return grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit);
 }
 
+// B. The next phase of one query: its mode and the rank its select aims at.
+// Returns true if the query takes part in the phase.
+__device__ bool decide_query(const EngineParams& p, EngineQuery& Q) {
+  Q.mode = 0;
+  if (Q.done) return false;
+  Q.prefix = 0;
+  // Every path costing <= the last phase's limit is accepted, so once
+  // K non-zero paths are, the K-th of them is the answer's K-th cost and
+  // the final phase only sweeps items within the rounding margin.
+  if (Q.paths_nz >= static_cast<unsigned long long>(Q.k)) {
+    Q.mode = 2;                       // final: the k-th of paths+pending
+    Q.krem = static_cast<unsigned long long>(Q.k);
+    Q.ksel = Q.krem;
+    atomicOr(&p.ctr->sel_paths, 1);
+  } else if (Q.pend_n > 0) {
+    Q.mode = 1;                       // grow by count
+    // promote ~4x the accepted count, but never more than half the
+    // pile: every path below the split is accepted with its whole
+    // closure, and the upper half of the pile reaches costs whose
+    // closure is exponentially large (measured: a 3/4 cap accepted 77x
+    // the paths needed)
+    unsigned long long j = 4 * (Q.paths_nz + 1);
+    // Near K, aim at K: every promoted item is accepted with its closure
+    // below the split, and the last growth phase showed how many paths
+    // one promoted item brings.  Promote the missing paths over that
+    // ratio (with 20% to spare), so the phase that reaches K overshoots
+    // little; falling short costs one more phase, which is only worth
+    // risking when the overshoot would be large (an extra phase costs
+    // about as much as closing ~1e5 more paths).
+    if (p.grow_cap_k && static_cast<unsigned long long>(Q.k) - Q.paths_nz >= (1ull << 17)) {
+      const unsigned long long miss = static_cast<unsigned long long>(Q.k) - Q.paths_nz;
+      unsigned long long aim = miss;
+      if (Q.last_j > 0 && Q.paths_nz > Q.acc_prev) {
+        const double ratio = static_cast<double>(Q.paths_nz - Q.acc_prev) /
+                             static_cast<double>(Q.last_j);
+        if (ratio > 1.0) aim = static_cast<unsigned long long>(1.2 * miss / ratio) + 64;
+      }
+      if (j > aim) j = aim;
+    }
+    if (j < 64) j = 64;
+    const unsigned long long half = (Q.pend_n + 1) / 2;
+    if (j > half) j = half;
+    Q.acc_prev = Q.paths_nz;
+    Q.last_j = j;
+    Q.krem = j;
+    Q.ksel = j;
+  } else {
+    Q.done = 1;                       // every path enumerated
+    return false;
+  }
+  ++Q.phases;
+  return true;
+}
+
+// The bookkeeping between two phases, done by the last block to reach the
+// grid barrier after the closure (or after seeding, finish == false): the
+// finished phase's counts become the pending pile's, and every query's next
+// phase is decided.  ctr->active then holds the number of running queries.
+__device__ void next_phase(const EngineParams& p, int phase, bool finish) {
+  if (threadIdx.x == 0) {
+    if (finish) p.ctr->phases = phase + 1;
+    p.ctr->active = 0;
+    p.ctr->sel_paths = 0;
+  }
+  __syncthreads();
+  for (int qi = threadIdx.x; qi < p.nq; qi += blockDim.x) {
+    EngineQuery& Q = p.q[qi];
+    if (finish) {
+      // G. final-mode queries are answered; counts restart
+      if (Q.mode == 2) Q.done = 1;
+      Q.pend_n = Q.pend_next_n;
+      Q.pend_nz = Q.pend_next_nz;
+      Q.pend_next_n = Q.pend_next_nz = 0;
+    }
+    if (decide_query(p, Q)) atomicAdd(&p.ctr->active, 1);
+  }
+}
+
 // ------------------------------------------------------------------ kernel
 __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
   const unsigned long long tid =
@@ -603,7 +732,9 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
   if (blockIdx.x == 0 && threadIdx.x == 0) t_last = gtime();
   // seed roots (pending pile 0)
   for (int qi = gw; qi < p.nq; qi += nw) seed_query(p, qi);
-  ENG_SYNC();
+  if (!grid_sync_last(&p.ctr->bar, &p.ctr->err, p.spin_limit,
+                      [&]() { next_phase(p, 0, false); }))
+    return;
   STAMP(0);
   int pin = 0;
   unsigned long long n_pend = *reinterpret_cast<volatile unsigned long long*>(&p.ctr->pend_out);
@@ -613,90 +744,10 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
     const Item* pend = p.pend[pin];
     Item* pend_next = p.pend[pin ^ 1];
     // (per-query counts are kept current by seeding, promotion and closure)
-    // B. per-query decision
-    for (unsigned long long qi = tid; qi < static_cast<unsigned long long>(p.nq); qi += nth) {
-      EngineQuery& Q = p.q[qi];
-      Q.mode = 0;
-      if (Q.done) continue;
-      Q.prefix = 0;
-      // Every path costing <= the last phase's limit is accepted, so once
-      // K non-zero paths are, the K-th of them is the answer's K-th cost and
-      // the final phase only sweeps items within the rounding margin.
-      if (Q.paths_nz >= static_cast<unsigned long long>(Q.k)) {
-        Q.mode = 2;                       // final: the k-th of paths+pending
-        Q.krem = static_cast<unsigned long long>(Q.k);
-        Q.ksel = Q.krem;
-        atomicOr(&p.ctr->sel_paths, 1);
-      } else if (Q.pend_n > 0) {
-        Q.mode = 1;                       // grow by count
-        // promote ~4x the accepted count, but never more than half the
-        // pile: every path below the split is accepted with its whole
-        // closure, and the upper half of the pile reaches costs whose
-        // closure is exponentially large (measured: a 3/4 cap accepted 77x
-        // the paths needed)
-        unsigned long long j = 4 * (Q.paths_nz + 1);
-        // Near K, aim at K: every promoted item is accepted with its closure
-        // below the split, and the last growth phase showed how many paths
-        // one promoted item brings.  Promote the missing paths over that
-        // ratio (with 20% to spare), so the phase that reaches K overshoots
-        // little; falling short costs one more phase, which is only worth
-        // risking when the overshoot would be large (an extra phase costs
-        // about as much as closing ~1e5 more paths).
-        if (p.grow_cap_k && static_cast<unsigned long long>(Q.k) - Q.paths_nz >= (1ull << 17)) {
-          const unsigned long long miss = static_cast<unsigned long long>(Q.k) - Q.paths_nz;
-          unsigned long long aim = miss;
-          if (Q.last_j > 0 && Q.paths_nz > Q.acc_prev) {
-            const double ratio = static_cast<double>(Q.paths_nz - Q.acc_prev) /
-                                 static_cast<double>(Q.last_j);
-            if (ratio > 1.0) aim = static_cast<unsigned long long>(1.2 * miss / ratio) + 64;
-          }
-          if (j > aim) j = aim;
-        }
-        if (j < 64) j = 64;
-        const unsigned long long half = (Q.pend_n + 1) / 2;
-        if (j > half) j = half;
-        Q.acc_prev = Q.paths_nz;
-        Q.last_j = j;
-        Q.krem = j;
-        Q.ksel = j;
-      } else {
-        Q.done = 1;                       // every path enumerated
-        continue;
-      }
-      ++Q.phases;
-      atomicAdd(&p.ctr->active, 1);
-    }
-    ENG_SYNC();
-    STAMP(1);
     if (*reinterpret_cast<volatile int*>(&p.ctr->active) == 0) break;
-    // C. per-query radix select
-    if (!run_select(p, n_paths, pend, n_pend)) return;
+    // C + D. per-query radix select, split and acceptance limit
+    if (!run_select(p, n_paths, pend, n_pend, true)) return;
     STAMP(2);
-    // D. split and acceptance limit
-    for (unsigned long long qi = tid; qi < static_cast<unsigned long long>(p.nq); qi += nth) {
-      EngineQuery& Q = p.q[qi];
-      if (Q.mode == 0) continue;
-      const float t = key_float(Q.prefix);
-      Q.t = t;
-      if (Q.mode == 2) {
-        const float a = fmaxf(fmaxf(fabsf(t), Q.root_abs), 1.0f);
-        Q.lim = t + a * 0x1p-16f;
-        Q.tie = t;
-      } else {
-        // accept strictly below the split when anything pending is cheaper
-        // than it (ksel - krem items are), so a tie group at the split waits
-        Q.lim = Q.ksel > Q.krem ? float_below(t) : t;
-        Q.tie = __int_as_float(0x7fc00000);  // NaN: expand every path
-      }
-    }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-      p.ctr->frontier[0] = 0;
-      p.ctr->frontier[1] = 0;
-      p.ctr->frontier[2] = 0;
-      p.ctr->pend_out = 0;
-    }
-    ENG_SYNC();
-    STAMP(1);
     // E. promote pending items under their query's limit
     {
       const unsigned long long pad = (n_pend + 31) & ~31ull;
@@ -746,20 +797,10 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
     // F. closure
     if (!run_closure(p, pend_next)) return;
     STAMP(4);
-    // G. final-mode queries are answered; counts restart
-    for (unsigned long long qi = tid; qi < static_cast<unsigned long long>(p.nq); qi += nth) {
-      EngineQuery& Q = p.q[qi];
-      if (Q.mode == 2) Q.done = 1;
-      Q.pend_n = Q.pend_next_n;
-      Q.pend_nz = Q.pend_next_nz;
-      Q.pend_next_n = Q.pend_next_nz = 0;
-    }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-      p.ctr->phases = phase + 1;
-      p.ctr->active = 0;
-      p.ctr->sel_paths = 0;
-    }
-    ENG_SYNC();
+    // G + B. counts restart, the next phase is decided
+    if (!grid_sync_last(&p.ctr->bar, &p.ctr->err, p.spin_limit,
+                        [&]() { next_phase(p, phase, true); }))
+      return;
     STAMP(1);
     n_paths = *reinterpret_cast<volatile unsigned long long*>(&p.ctr->paths);
     n_pend = *reinterpret_cast<volatile unsigned long long*>(&p.ctr->pend_out);
@@ -793,7 +834,7 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
     }
     p.ctr->out_total = acc;
   }
-  if (!run_select(p, n_paths, nullptr, 0)) return;
+  if (!run_select(p, n_paths, nullptr, 0, false)) return;
   STAMP(5);
   const unsigned long long n_out = *reinterpret_cast<volatile unsigned long long*>(&p.ctr->out_total);
   if (n_out > p.out_cap) {

@@ -57,48 +57,6 @@ __device__ __forceinline__ bool grid_sync(GridBarrier* b, int* err,
   return *reinterpret_cast<volatile int*>(err) == kDevOk;
 }
 
-// grid_sync whose last block to arrive runs f() with all its threads before
-// it releases the others: work that one block can do on what every block
-// wrote before the barrier, without a second barrier for its results.  Same
-// bounded wait and return value as grid_sync.
-template <typename F>
-__device__ __forceinline__ bool grid_sync_last(GridBarrier* b, int* err, unsigned int limit,
-                                               F&& f) {
-  __shared__ int s_last;
-  __syncthreads();
-  unsigned int g = 0;
-  if (threadIdx.x == 0) {
-    g = *reinterpret_cast<volatile unsigned int*>(&b->gen);
-    __threadfence();
-    s_last = atomicAdd(&b->count, 1u) == gridDim.x - 1;
-  }
-  __syncthreads();
-  if (s_last) {
-    __threadfence();  // the other blocks' writes before their arrival
-    f();
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      atomicExch(&b->count, 0u);
-      __threadfence();
-      atomicAdd(&b->gen, 1u);
-    }
-  } else if (threadIdx.x == 0) {
-    volatile unsigned int* vgen = &b->gen;
-    unsigned int it = 0;
-    while (*vgen == g) {
-      if (++it > limit) {
-        atomicCAS(err, kDevOk, kDevTimeout);
-        break;
-      }
-      __nanosleep(64);
-    }
-    __threadfence();
-  }
-  __syncthreads();
-  return *reinterpret_cast<volatile int*>(err) == kDevOk;
-}
-
 // Warp-aggregated append: one atomic per warp.  Every lane of the warp must
 // call it; returns the slot of this lane (meaningful only where pred).
 template <typename T>

@@ -50,9 +50,70 @@ __device__ __forceinline__ unsigned long long gtime() {
   return t;
 }
 
-#define ENG_SYNC()                                                   \
-  do {                                                               \
-    if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit)) return;  \
+// Grid barriers of the engine.  The arrival counter only grows, so the
+// barrier a block arrives at is told by the count it finds: arrivals
+// n * G .. n * G + G - 1 (G blocks) belong to the n-th barrier of the launch,
+// which is passed once the counter reads (n + 1) * G.  The last block to
+// arrive has nothing to reset and the others leave on the first poll that
+// sees its arrival.  eng_sync_last lets that last block run f() first and
+// then publish the same target in a second word the others wait on.  Waits
+// are bounded (kDevTimeout); both return false once any block has recorded
+// an error.
+__device__ __forceinline__ bool bar_wait(const EngineParams& p, const unsigned int* word,
+                                         unsigned int target) {
+  const volatile unsigned int* w = word;
+  unsigned int it = 0;
+  while (static_cast<int>(*w - target) < 0) {
+    if (++it > p.spin_limit) {
+      atomicCAS(&p.ctr->err, kDevOk, kDevTimeout);
+      return false;
+    }
+    __nanosleep(32);
+  }
+  return true;
+}
+
+__device__ __forceinline__ bool eng_sync(const EngineParams& p) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned int old = atomicAdd(&p.ctr->bar.count, 1u);
+    bar_wait(p, &p.ctr->bar.count, (old / gridDim.x + 1u) * gridDim.x);
+    __threadfence();
+  }
+  __syncthreads();
+  return *reinterpret_cast<volatile int*>(&p.ctr->err) == kDevOk;
+}
+
+template <typename F>
+__device__ __forceinline__ bool eng_sync_last(const EngineParams& p, F&& f) {
+  __shared__ unsigned int s_target;
+  __shared__ int s_last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned int old = atomicAdd(&p.ctr->bar.count, 1u);
+    s_target = (old / gridDim.x + 1u) * gridDim.x;
+    s_last = old + 1u == s_target;
+  }
+  __syncthreads();
+  if (s_last) {
+    __threadfence();  // the other blocks' writes before their arrival
+    f();
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) atomicMax(&p.ctr->bar.gen, s_target);
+  } else if (threadIdx.x == 0) {
+    bar_wait(p, &p.ctr->bar.gen, s_target);
+    __threadfence();
+  }
+  __syncthreads();
+  return *reinterpret_cast<volatile int*>(&p.ctr->err) == kDevOk;
+}
+
+#define ENG_SYNC()              \
+  do {                          \
+    if (!eng_sync(p)) return;   \
   } while (0)
 
 __device__ __forceinline__ unsigned q_of(const Item& it) {
@@ -339,7 +400,7 @@ __device__ bool run_select(const EngineParams& p, unsigned long long n_paths,
     const bool last = pass == p.sel_passes - 1;
     select_hist(p, n_paths, pend, n_pend, shift, bits);
     if (fused) {
-      if (!grid_sync_last(&p.ctr->bar, &p.ctr->err, p.spin_limit, [&]() {
+      if (!eng_sync_last(p, [&]() {
             select_pick(p, shift, bits, static_cast<int>(threadIdx.x >> 5),
                         static_cast<int>(blockDim.x >> 5));
             if (last && with_limits) {
@@ -349,14 +410,14 @@ __device__ bool run_select(const EngineParams& p, unsigned long long n_paths,
           }))
         return false;
     } else {
-      if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit)) return false;
+      if (!eng_sync(p)) return false;
       select_pick(p, shift, bits, static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 5),
                   static_cast<int>((gridDim.x * blockDim.x) >> 5));
-      if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit)) return false;
+      if (!eng_sync(p)) return false;
       if (last && with_limits) {
         set_limits(p, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x,
                    blockIdx.x == 0 && threadIdx.x == 0);
-        if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit)) return false;
+        if (!eng_sync(p)) return false;
       }
     }
   }
@@ -535,7 +596,7 @@ __device__ bool run_closure(const EngineParams& p, Item* pend_out) {
       qadd(p.q, QOFF(pend_next_nz), acc_pnz != 0, 0u, acc_pnz);
       acc_nz = acc_pn = acc_pnz = 0;
     }
-    if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit)) return false;
+    if (!eng_sync(p)) return false;
     ++r;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) p.ctr->rounds += r;
@@ -569,7 +630,7 @@ __device__ bool lsd_pass(const EngineParams& p, unsigned long long n, int src,
     atomicAdd(&running[digit_of(i)], 1u);
   __syncthreads();
   for (int d = threadIdx.x; d < 256; d += blockDim.x) p.sort_hist[d * G + blockIdx.x] = running[d];
-  if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit)) return false;
+  if (!eng_sync(p)) return false;
   // 2. one warp per digit: exclusive scan across tiles
   {
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -590,7 +651,7 @@ __device__ bool lsd_pass(const EngineParams& p, unsigned long long n, int src,
       if (lane == 0) p.digit_tot[d] = carry;
     }
   }
-  if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit)) return false;
+  if (!eng_sync(p)) return false;
   // 3. digit bases, then a stable scatter of the tile
   if (threadIdx.x == 0) {
     unsigned acc = 0;
@@ -639,7 +700,7 @@ __device__ bool lsd_pass(const EngineParams& p, unsigned long long n, int src,
     }
     __syncthreads();
   }
-  return grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit);
+  return eng_sync(p);
 }
 
 // B. The next phase of one query: its mode and the rank its select aims at.
@@ -732,8 +793,7 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
   if (blockIdx.x == 0 && threadIdx.x == 0) t_last = gtime();
   // seed roots (pending pile 0)
   for (int qi = gw; qi < p.nq; qi += nw) seed_query(p, qi);
-  if (!grid_sync_last(&p.ctr->bar, &p.ctr->err, p.spin_limit,
-                      [&]() { next_phase(p, 0, false); }))
+  if (!eng_sync_last(p, [&]() { next_phase(p, 0, false); }))
     return;
   STAMP(0);
   int pin = 0;
@@ -798,8 +858,7 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
     if (!run_closure(p, pend_next)) return;
     STAMP(4);
     // G + B. counts restart, the next phase is decided
-    if (!grid_sync_last(&p.ctr->bar, &p.ctr->err, p.spin_limit,
-                        [&]() { next_phase(p, phase, true); }))
+    if (!eng_sync_last(p, [&]() { next_phase(p, phase, true); }))
       return;
     STAMP(1);
     n_paths = *reinterpret_cast<volatile unsigned long long*>(&p.ctr->paths);

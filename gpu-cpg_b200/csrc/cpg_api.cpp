@@ -74,7 +74,7 @@ struct cpg_handle {
   bool h_sfxt_cached = false;
   bool h_levels_cached = false;  // levels depend on the graph, not on delays
   DevMem d_order, d_lvlp, d_level_of, d_dist, d_succ, d_dev_cnt, d_dev,
-      d_ht_root, d_ht_size, d_hnodes, d_pool_mark, d_deps, d_sctr;
+      d_ht_root, d_ht_size, d_hnodes, d_pool_mark, d_deps, d_sctr, d_best;
   unsigned long long hnode_cap = 0;
 
   // query
@@ -269,7 +269,8 @@ Status upload_graph(cpg_handle* h, int32_t n, int32_t m, const int32_t* adjp,
   CK(ensure(h->d_dist, nn * 4), "alloc dist");
   CK(ensure(h->d_succ, nn * 4), "alloc succ");
   CK(ensure(h->d_dev_cnt, nn * 4), "alloc dev_cnt");
-  CK(ensure(h->d_dev, mm * sizeof(DevSidetrack)), "alloc deviations");
+  CK(ensure(h->d_dev, (mm + kDevPad) * sizeof(DevSidetrack)), "alloc deviations");
+  CK(ensure(h->d_best, nn * sizeof(DevSidetrack) + 16), "alloc deviations");
   CK(ensure(h->d_ht_root, nn * 4), "alloc ht_root");
   CK(ensure(h->d_ht_size, nn * 4), "alloc ht_size");
   CK(ensure(h->d_pool_mark, (nn + 2) * 8), "alloc pool_mark");
@@ -400,6 +401,7 @@ SfxtParams sfxt_params(cpg_handle* h, int32_t start_level) {
   p.succ = P<int32_t>(h->d_succ);
   p.dev_cnt = P<int32_t>(h->d_dev_cnt);
   p.dev = P<DevSidetrack>(h->d_dev);
+  p.best = P<DevSidetrack>(h->d_best);
   p.ht_root = P<int32_t>(h->d_ht_root);
   p.ht_size = P<int32_t>(h->d_ht_size);
   p.hnodes = P<HeapNode>(h->d_hnodes);
@@ -1071,7 +1073,7 @@ cpg_status cpg_destroy(cpg_handle* h) {
   DevMem* all[] = {&h->d_adjp, &h->d_edges, &h->d_iadjp, &h->d_iadj, &h->d_srcs,
                    &h->d_big_off, &h->d_big_tmp, &h->d_big_rows, &h->d_order, &h->d_lvlp,
                    &h->d_level_of, &h->d_dist, &h->d_succ, &h->d_dev_cnt,
-                   &h->d_dev, &h->d_ht_root, &h->d_ht_size, &h->d_hnodes,
+                   &h->d_dev, &h->d_best, &h->d_ht_root, &h->d_ht_size, &h->d_hnodes,
                    &h->d_pool_mark, &h->d_deps, &h->d_sctr, &h->d_pcost,
                    &h->d_pparent, &h->d_pfrom, &h->d_pto, &h->d_plevel,
                    &h->d_front0, &h->d_front1, &h->d_pend0, &h->d_pend1,

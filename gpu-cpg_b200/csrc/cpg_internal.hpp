@@ -58,15 +58,27 @@ struct alignas(16) DevSidetrack {
 };
 
 // Node of the persistent chain heap: the heap of vertex v holds, for every
-// vertex u on v's suffix chain that has deviations, u's cheapest deviation
-// key.  The heap of v shares every node but one root-to-leaf path with the
-// heap of succ[v].
-struct alignas(16) HeapNode {
+// vertex u on v's suffix chain that has deviations, u's cheapest deviation.
+// The heap of v shares every node but one root-to-leaf path with the heap of
+// succ[v].  A node carries its element's whole record (the start of u's
+// sorted deviation row, that deviation's head, delay and head distance, and
+// u's distance), so a path search prices the element, and finds its row,
+// from the node alone.  Heap order is (deviation_key of the record, vtx).
+struct alignas(32) HeapNode {
   int32_t vtx;
   int32_t left;
   int32_t right;
-  float key;
+  int32_t row;        // adjp[vtx]
+  int32_t head;       // the cheapest deviation (entry 0 of the sorted row)
+  float w;
+  int32_t dist_head;
+  int32_t dist_v;     // dist[vtx]
 };
+
+// Deviation rows are padded past the last edge by this many entries, so a
+// search may load entry j of a row before checking j against the row's count
+// (j <= 2 * count + 2 < 2 * the longest row).
+constexpr int kDevPad = 2 * 16384 + 64;
 
 // A path-graph item: the path "parent + the j-th deviation of vertex
 // heap[node].vtx", or, when node <= -2, the root path that starts at source
@@ -125,6 +137,7 @@ struct SfxtParams {
   int32_t* succ;
   int32_t* dev_cnt;
   DevSidetrack* dev;
+  DevSidetrack* best;    // per vertex: its cheapest deviation (the heap element)
   int32_t* ht_root;
   int32_t* ht_size;
   HeapNode* hnodes;

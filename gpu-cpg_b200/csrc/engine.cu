@@ -502,6 +502,11 @@ __device__ bool run_closure(const EngineParams& p, Item* pend_out) {
       hn.vtx = -1;
       hn.left = -1;
       hn.right = -1;
+      hn.row = 0;
+      hn.head = -1;
+      hn.w = 0.f;
+      hn.dist_head = 0;
+      hn.dist_v = 0;
       float lim = 0.f, tie = 0.f;
       if (valid) {
         lim = single ? lim0 : __ldcg(&p.q[q].lim);
@@ -512,8 +517,7 @@ __device__ bool run_closure(const EngineParams& p, Item* pend_out) {
         } else {
           hn = load_node(p.g.hnodes, it.node);
           from = hn.vtx;
-          const DevSidetrack d = load_dev(p.g.dev, __ldg(p.g.adjp + from) + jj);
-          to = d.head;
+          to = dev_head(p.g, hn, jj);
           level = __ldcg(p.ps.level + it.parent) + 1;
         }
         if (qp < p.ps.cap) {
@@ -539,13 +543,15 @@ __device__ bool run_closure(const EngineParams& p, Item* pend_out) {
       const int cross = expand ? __ldg(p.g.ht_root + to) : -1;
       float cc[5];
       unsigned exm = 0;
-      if (sib && make_candidate(p.g, jj == 0 ? hn.left : it.node, jj == 0 ? 0 : 2 * jj + 1,
-                                pcost, cc[0])) exm |= 1u;
-      if (sib && make_candidate(p.g, jj == 0 ? hn.right : it.node, jj == 0 ? 0 : 2 * jj + 2,
-                                pcost, cc[1])) exm |= 2u;
-      if (sib && jj == 0 && make_candidate(p.g, it.node, 1, pcost, cc[2])) exm |= 4u;
-      if (sib && jj == 0 && make_candidate(p.g, it.node, 2, pcost, cc[3])) exm |= 8u;
-      if (expand && make_candidate(p.g, cross, 0, it.cost, cc[4])) exm |= 16u;
+      // (the item's own node carries its row start, and every node the
+      // record of its element, so no child costs more than one more load)
+      if (sib && (jj == 0 ? cand_top(p.g, hn.left, pcost, cc[0])
+                          : cand_row(p.g, hn, 2 * jj + 1, pcost, cc[0]))) exm |= 1u;
+      if (sib && (jj == 0 ? cand_top(p.g, hn.right, pcost, cc[1])
+                          : cand_row(p.g, hn, 2 * jj + 2, pcost, cc[1]))) exm |= 2u;
+      if (sib && jj == 0 && cand_row(p.g, hn, 1, pcost, cc[2])) exm |= 4u;
+      if (sib && jj == 0 && cand_row(p.g, hn, 2, pcost, cc[3])) exm |= 8u;
+      if (expand && cand_top(p.g, cross, it.cost, cc[4])) exm |= 16u;
       unsigned tm = 0, dm = 0, dnz = 0;
 #pragma unroll
       for (int k = 0; k < 5; ++k) {

@@ -87,6 +87,11 @@ closure_kernel(ClosureParams p) {
       hn.vtx = -1;
       hn.left = -1;
       hn.right = -1;
+      hn.row = 0;
+      hn.head = -1;
+      hn.w = 0.f;
+      hn.dist_head = 0;
+      hn.dist_v = 0;
       if (valid) {
         int from = -1, level = 0;
         if (it.node <= -2) {
@@ -94,8 +99,7 @@ closure_kernel(ClosureParams p) {
         } else {
           hn = load_node(p.g.hnodes, it.node);
           from = hn.vtx;
-          const DevSidetrack d = load_dev(p.g.dev, __ldg(p.g.adjp + from) + it.j);
-          to = d.head;
+          to = dev_head(p.g, hn, it.j);
           level = __ldcg(p.ps.level + it.parent) + 1;
         }
         if (q < p.ps.cap) {
@@ -123,18 +127,20 @@ closure_kernel(ClosureParams p) {
         // first child: chain-heap left (j == 0) or list child 2j+1
         c.node = it.j == 0 ? hn.left : it.node;
         c.j = it.j == 0 ? 0 : 2 * it.j + 1;
-        ex = sib && make_candidate(p.g, c.node, c.j, pcost, c.cost);
+        ex = sib && (it.j == 0 ? cand_top(p.g, c.node, pcost, c.cost)
+                               : cand_row(p.g, hn, c.j, pcost, c.cost));
         route(p, out, out_cnt, ex, c);
         c.node = it.j == 0 ? hn.right : it.node;
         c.j = it.j == 0 ? 0 : 2 * it.j + 2;
-        ex = sib && make_candidate(p.g, c.node, c.j, pcost, c.cost);
+        ex = sib && (it.j == 0 ? cand_top(p.g, c.node, pcost, c.cost)
+                               : cand_row(p.g, hn, c.j, pcost, c.cost));
         route(p, out, out_cnt, ex, c);
         c.node = it.node;
         c.j = 1;
-        ex = sib && it.j == 0 && make_candidate(p.g, c.node, c.j, pcost, c.cost);
+        ex = sib && it.j == 0 && cand_row(p.g, hn, c.j, pcost, c.cost);
         route(p, out, out_cnt, ex, c);
         c.j = 2;
-        ex = sib && it.j == 0 && make_candidate(p.g, c.node, c.j, pcost, c.cost);
+        ex = sib && it.j == 0 && cand_row(p.g, hn, c.j, pcost, c.cost);
         route(p, out, out_cnt, ex, c);
       }
       // cross: the cheapest deviation on the new path's own suffix chain
@@ -143,7 +149,7 @@ closure_kernel(ClosureParams p) {
         c.parent = static_cast<int>(q);
         c.node = expand ? __ldg(p.g.ht_root + to) : -1;
         c.j = 0;
-        const bool ex = expand && make_candidate(p.g, c.node, 0, it.cost, c.cost);
+        const bool ex = expand && cand_top(p.g, c.node, it.cost, c.cost);
         route(p, out, out_cnt, ex, c);
       }
     }

@@ -31,12 +31,17 @@ __device__ __forceinline__ float child_cost(int division, float slack, int dn,
 }
 
 __device__ __forceinline__ HeapNode load_node(const HeapNode* h, int i) {
-  const int4 r = __ldg(reinterpret_cast<const int4*>(h + i));
+  const int4 a = __ldg(reinterpret_cast<const int4*>(h + i));
+  const int4 b = __ldg(reinterpret_cast<const int4*>(h + i) + 1);
   HeapNode n;
-  n.vtx = r.x;
-  n.left = r.y;
-  n.right = r.z;
-  n.key = __int_as_float(r.w);
+  n.vtx = a.x;
+  n.left = a.y;
+  n.right = a.z;
+  n.row = a.w;
+  n.head = b.x;
+  n.w = __int_as_float(b.y);
+  n.dist_head = b.z;
+  n.dist_v = b.w;
   return n;
 }
 
@@ -50,19 +55,42 @@ __device__ __forceinline__ DevSidetrack load_dev(const DevSidetrack* d, int i) {
   return s;
 }
 
-// Candidate (parent path, heap node, index j): fills its cost.  Returns false
-// if the candidate does not exist.
-__device__ __forceinline__ bool make_candidate(const PfxtGraph& g, int node,
-                                               int j, float parent_cost,
-                                               float& cost) {
+// Candidate (node, 0): the cheapest deviation of the node's vertex, priced
+// from the record the node carries.  False if there is no node.
+__device__ __forceinline__ bool cand_top(const PfxtGraph& g, int node, float parent_cost,
+                                         float& cost) {
   if (node < 0) return false;
-  const HeapNode hn = load_node(g.hnodes, node);
-  const int v = hn.vtx;
-  if (j >= __ldg(g.dev_cnt + v)) return false;
-  const DevSidetrack d = load_dev(g.dev, __ldg(g.adjp + v) + j);
-  cost = child_cost(g.division, parent_cost, d.dist_head, d.w, __ldg(g.dist + v));
+  const HeapNode n = load_node(g.hnodes, node);
+  cost = child_cost(g.division, parent_cost, n.dist_head, n.w, n.dist_v);
   return true;
 }
 
+// Candidate (entry j >= 1 of the sorted row of hn's vertex).  The entry and
+// the row's count are requested together (rows are padded, so the entry's
+// load stays inside the allocation for any j a search asks); false if j is
+// past the count.
+__device__ __forceinline__ bool cand_row(const PfxtGraph& g, const HeapNode& hn, int j,
+                                         float parent_cost, float& cost) {
+  const int cnt = __ldg(g.dev_cnt + hn.vtx);
+  const DevSidetrack d = load_dev(g.dev, hn.row + j);
+  if (j >= cnt) return false;
+  cost = child_cost(g.division, parent_cost, d.dist_head, d.w, hn.dist_v);
+  return true;
+}
+
+// Candidate (parent path, heap node, index j): fills its cost.  Returns false
+// if the candidate does not exist.
+__device__ __forceinline__ bool make_candidate(const PfxtGraph& g, int node, int j,
+                                               float parent_cost, float& cost) {
+  if (node < 0) return false;
+  if (j == 0) return cand_top(g, node, parent_cost, cost);
+  return cand_row(g, load_node(g.hnodes, node), j, parent_cost, cost);
+}
+
+// Head of entry j of the sorted row of hn's vertex: the last edge of the
+// path that takes that deviation.
+__device__ __forceinline__ int dev_head(const PfxtGraph& g, const HeapNode& hn, int j) {
+  return j == 0 ? hn.head : load_dev(g.dev, hn.row + j).head;
+}
 
 }  // namespace cpg

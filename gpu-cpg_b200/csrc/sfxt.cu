@@ -54,6 +54,50 @@ __device__ __forceinline__ unsigned long long sort_word(float key, int idx) {
          static_cast<unsigned>(idx);
 }
 
+// The cheapest deviation of a row too long to sort in registers, tracked per
+// lane while the row is built: the least (key, edge position) word and its
+// record.  best_reduce gives every lane the row's first entry once sorted.
+struct BestDev {
+  unsigned long long word;
+  DevSidetrack rec;
+};
+
+__device__ __forceinline__ BestDev best_none() {
+  BestDev b;
+  b.word = ~0ull;
+  b.rec.head = -1;
+  b.rec.w = 0.f;
+  b.rec.dist_head = 0;
+  b.rec.key = 0.f;
+  return b;
+}
+
+__device__ __forceinline__ void best_take(BestDev& b, bool valid, const DevSidetrack& rec,
+                                          int pos) {
+  const unsigned long long x = sort_word(rec.key, pos);
+  if (valid && x < b.word) {
+    b.word = x;
+    b.rec = rec;
+  }
+}
+
+__device__ __forceinline__ DevSidetrack best_reduce(const BestDev& b) {
+  unsigned long long m = b.word;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long y = __shfl_xor_sync(0xffffffffu, m, o);
+    m = y < m ? y : m;
+  }
+  const unsigned own = __ballot_sync(0xffffffffu, b.word == m);
+  const int src = __ffs(own) - 1;
+  DevSidetrack r;
+  r.head = __shfl_sync(0xffffffffu, b.rec.head, src);
+  r.w = __shfl_sync(0xffffffffu, b.rec.w, src);
+  r.dist_head = __shfl_sync(0xffffffffu, b.rec.dist_head, src);
+  r.key = __shfl_sync(0xffffffffu, b.rec.key, src);
+  return r;
+}
+
 // Bitonic sort of one word per lane across the warp, ascending by lane.
 __device__ __forceinline__ unsigned long long warp_sort32(unsigned long long x) {
   const int lane = threadIdx.x & 31;
@@ -73,9 +117,9 @@ __device__ __forceinline__ unsigned long long warp_sort32(unsigned long long x) 
 // A row of at most 32 edges (one per lane) is sorted in registers and
 // written once, in order (write_row64 does the same up to 64 edges); longer
 // rows are written in edge order and sorted by sort_rows_kernel.  Returns the
-// number of deviations written.
+// number of deviations written; lane 0's top is the first of them.
 __device__ __forceinline__ int write_short_row(const SfxtParams& p, int rb, bool valid,
-                                               const DevSidetrack& rec, float& kmin) {
+                                               const DevSidetrack& rec, DevSidetrack& top) {
   const int lane = threadIdx.x & 31;
   const unsigned bal = __ballot_sync(0xffffffffu, valid);
   const unsigned long long x = warp_sort32(valid ? sort_word(rec.key, lane) : ~0ull);
@@ -87,7 +131,7 @@ __device__ __forceinline__ int write_short_row(const SfxtParams& p, int rb, bool
   o.key = __shfl_sync(0xffffffffu, rec.key, src);
   const int cnt = __popc(bal);
   if (lane < cnt) p.dev[rb + lane] = o;
-  if (valid) kmin = fminf(kmin, rec.key);
+  top = o;
   return cnt;
 }
 
@@ -97,7 +141,7 @@ __device__ __forceinline__ int write_short_row(const SfxtParams& p, int rb, bool
 // chunk it came from.
 __device__ __forceinline__ int write_row64(const SfxtParams& p, int rb, bool v0,
                                            const DevSidetrack& r0, bool v1,
-                                           const DevSidetrack& r1, float& kmin) {
+                                           const DevSidetrack& r1, DevSidetrack& top) {
   const int lane = threadIdx.x & 31;
   const unsigned b0 = __ballot_sync(0xffffffffu, v0);
   const unsigned b1 = __ballot_sync(0xffffffffu, v1);
@@ -141,9 +185,8 @@ __device__ __forceinline__ int write_row64(const SfxtParams& p, int rb, bool v0,
     o.key = hi ? k1 : k0;
     const int i = 32 * c + lane;
     if (i < cnt) p.dev[rb + i] = o;
+    if (c == 0) top = o;
   }
-  if (v0) kmin = fminf(kmin, r0.key);
-  if (v1) kmin = fminf(kmin, r1.key);
   return cnt;
 }
 
@@ -163,7 +206,8 @@ __device__ int build_vertex(const SfxtParams& p, int v, int lvl, bool do_kahn) {
   int best = INT_MAX;
   int s = -1;
   int cnt = 0;
-  float kmin = __int_as_float(0x7f800000);  // +inf
+  DevSidetrack top;  // the cheapest deviation (lane 0's copy is used)
+  top.head = -1;
   if (re - rb <= kRegChunks * 32) {
     // the whole row in registers: every edge word, then every head distance,
     // is requested before any is used, so a long row costs about two memory
@@ -208,7 +252,7 @@ __device__ int build_vertex(const SfxtParams& p, int v, int lvl, bool do_kahn) {
       rec.w = ed[0].w;
       rec.dist_head = dh[0];
       rec.key = deviation_key(dh[0], best, ed[0].w);
-      cnt = write_short_row(p, rb, valid, rec, kmin);
+      cnt = write_short_row(p, rb, valid, rec, top);
     } else if (re - rb <= 64) {
       DevSidetrack r[2];
       bool v[2];
@@ -220,23 +264,26 @@ __device__ int build_vertex(const SfxtParams& p, int v, int lvl, bool do_kahn) {
         r[c].dist_head = dh[c];
         r[c].key = deviation_key(dh[c], best, ed[c].w);
       }
-      cnt = write_row64(p, rb, v[0], r[0], v[1], r[1], kmin);
-    } else
+      cnt = write_row64(p, rb, v[0], r[0], v[1], r[1], top);
+    } else {
+      BestDev bd = best_none();
 #pragma unroll
-    for (int c = 0; c < kRegChunks; ++c) {
-      if (rb + c * 32 >= re) break;
-      const bool valid = ed[c].head >= 0 && ed[c].head != s && dh[c] != INT_MAX;
-      const unsigned bal = __ballot_sync(0xffffffffu, valid);
-      if (valid) {
-        DevSidetrack rec;
-        rec.head = ed[c].head;
-        rec.w = ed[c].w;
-        rec.dist_head = dh[c];
-        rec.key = deviation_key(dh[c], best, ed[c].w);
-        p.dev[rb + cnt + __popc(bal & lanemask_lt())] = rec;
-        kmin = fminf(kmin, rec.key);
+      for (int c = 0; c < kRegChunks; ++c) {
+        if (rb + c * 32 >= re) break;
+        const bool valid = ed[c].head >= 0 && ed[c].head != s && dh[c] != INT_MAX;
+        const unsigned bal = __ballot_sync(0xffffffffu, valid);
+        if (valid) {
+          DevSidetrack rec;
+          rec.head = ed[c].head;
+          rec.w = ed[c].w;
+          rec.dist_head = dh[c];
+          rec.key = deviation_key(dh[c], best, ed[c].w);
+          p.dev[rb + cnt + __popc(bal & lanemask_lt())] = rec;
+          best_take(bd, true, rec, c * 32 + lane);
+        }
+        cnt += __popc(bal);
       }
-      cnt += __popc(bal);
+      top = best_reduce(bd);
     }
   } else {
     // long rows (a super-source, say): chunk by chunk
@@ -259,6 +306,7 @@ __device__ int build_vertex(const SfxtParams& p, int v, int lvl, bool do_kahn) {
       }
       s = warp_max_i(s);
     }
+    BestDev bd = best_none();
     for (int base = rb; base < re; base += 32) {
       const int e = base + lane;
       bool valid = false;
@@ -273,14 +321,12 @@ __device__ int build_vertex(const SfxtParams& p, int v, int lvl, bool do_kahn) {
         rec.key = deviation_key(dh, best, ed.w);
       }
       const unsigned bal = __ballot_sync(0xffffffffu, valid);
-      if (valid) {
-        p.dev[rb + cnt + __popc(bal & lanemask_lt())] = rec;
-        kmin = fminf(kmin, rec.key);
-      }
+      if (valid) p.dev[rb + cnt + __popc(bal & lanemask_lt())] = rec;
+      best_take(bd, valid, rec, e - rb);
       cnt += __popc(bal);
     }
+    top = best_reduce(bd);
   }
-  for (int o = 16; o > 0; o >>= 1) kmin = fminf(kmin, __shfl_xor_sync(0xffffffffu, kmin, o));
 
   if (lane == 0) {
     p.dist[v] = best;
@@ -288,10 +334,8 @@ __device__ int build_vertex(const SfxtParams& p, int v, int lvl, bool do_kahn) {
     p.dev_cnt[v] = cnt;
     if (re - rb > 64 && cnt > 1 && cnt <= kSmemRow)  // left for sort_rows_kernel
       p.long_rows[atomicAdd(&p.ctr->n_long, 1)] = v;
-    // v's fan-outs are all processed, so its dependency counter is free: it
-    // carries the cheapest deviation key to the chain-heap insert, which runs
-    // one level later, off this level's critical path
-    p.deps[v] = __float_as_int(kmin);
+    // the chain-heap insert, one level later, takes v's cheapest deviation
+    if (cnt > 0) p.best[v] = top;
     if (kLevel) p.level_of[v] = lvl;
   }
 
@@ -370,6 +414,48 @@ __device__ __forceinline__ unsigned long long heap_alloc(const SfxtParams& p, un
   return a;
 }
 
+// The element a chain-heap node carries: everything but the child links.
+struct HeapElem {
+  int32_t vtx, row, head;
+  float w;
+  int32_t dist_head, dist_v;
+  float key;  // deviation_key of the record: the heap order, with vtx
+};
+
+__device__ __forceinline__ HeapNode load_heap_node(const HeapNode* h, int i) {
+  const int4 a = __ldcg(reinterpret_cast<const int4*>(h + i));
+  const int4 b = __ldcg(reinterpret_cast<const int4*>(h + i) + 1);
+  HeapNode n;
+  n.vtx = a.x;
+  n.left = a.y;
+  n.right = a.z;
+  n.row = a.w;
+  n.head = b.x;
+  n.w = __int_as_float(b.y);
+  n.dist_head = b.z;
+  n.dist_v = b.w;
+  return n;
+}
+
+__device__ __forceinline__ HeapElem elem_of(const HeapNode& n) {
+  HeapElem e;
+  e.vtx = n.vtx;
+  e.row = n.row;
+  e.head = n.head;
+  e.w = n.w;
+  e.dist_head = n.dist_head;
+  e.dist_v = n.dist_v;
+  e.key = deviation_key(n.dist_head, n.dist_v, n.w);
+  return e;
+}
+
+__device__ __forceinline__ void store_heap_node(HeapNode* at, const HeapElem& e, int left,
+                                                int right) {
+  int4* q = reinterpret_cast<int4*>(at);
+  q[0] = make_int4(e.vtx, left, right, e.row);
+  q[1] = make_int4(e.head, __float_as_int(e.w), e.dist_head, e.dist_v);
+}
+
 template <bool kPublish = false>
 __device__ void heap_insert(const SfxtParams& p, int v, unsigned long long* chunk = nullptr) {
   const int s = __ldcg(p.succ + v);
@@ -380,7 +466,18 @@ __device__ void heap_insert(const SfxtParams& p, int v, unsigned long long* chun
     heap_store<kPublish>(p, v, base_root, base_size);
     return;
   }
-  const float kmin = __int_as_float(__ldcg(p.deps + v));
+  // v's element: its cheapest deviation, as the build left it
+  HeapElem ce;
+  {
+    const int4 b = __ldcg(reinterpret_cast<const int4*>(p.best + v));
+    ce.vtx = v;
+    ce.row = __ldg(p.adjp + v);
+    ce.head = b.x;
+    ce.w = __int_as_float(b.y);
+    ce.dist_head = b.z;
+    ce.key = __int_as_float(b.w);
+    ce.dist_v = __ldcg(p.dist + v);
+  }
   const unsigned pos = static_cast<unsigned>(base_size) + 1u;
   const int depth = 31 - __clz(pos);
   const unsigned long long a = heap_alloc(p, static_cast<unsigned>(depth + 1), chunk);
@@ -389,41 +486,19 @@ __device__ void heap_insert(const SfxtParams& p, int v, unsigned long long* chun
     heap_store<kPublish>(p, v, -1, 0);
     return;
   }
-  int cv = v;
-  float ck = kmin;
   int cur = base_root;
   for (int d = depth - 1; d >= 0; --d) {
-    HeapNode old;
-    {
-      const int4 raw = __ldcg(reinterpret_cast<const int4*>(p.hnodes + cur));
-      old.vtx = raw.x;
-      old.left = raw.y;
-      old.right = raw.z;
-      old.key = __int_as_float(raw.w);
-    }
+    const HeapNode old = load_heap_node(p.hnodes, cur);
+    const HeapElem oe = elem_of(old);
     const int bit = (pos >> d) & 1u;
-    HeapNode nn;
-    if (heap_less(cv, ck, old.vtx, old.key)) {
-      nn.vtx = cv;
-      nn.key = ck;
-      cv = old.vtx;
-      ck = old.key;
-    } else {
-      nn.vtx = old.vtx;
-      nn.key = old.key;
-    }
     const int next = static_cast<int>(a) + (depth - d);
-    nn.left = bit ? old.left : next;
-    nn.right = bit ? next : old.right;
-    p.hnodes[a + (depth - 1 - d)] = nn;
+    const bool carry_down = heap_less(ce.vtx, ce.key, oe.vtx, oe.key);
+    store_heap_node(p.hnodes + a + (depth - 1 - d), carry_down ? ce : oe,
+                    bit ? old.left : next, bit ? next : old.right);
+    if (carry_down) ce = oe;
     cur = bit ? old.right : old.left;
   }
-  HeapNode leaf;
-  leaf.vtx = cv;
-  leaf.key = ck;
-  leaf.left = -1;
-  leaf.right = -1;
-  p.hnodes[a + depth] = leaf;
+  store_heap_node(p.hnodes + a + depth, ce, -1, -1);
   heap_store<kPublish>(p, v, static_cast<int>(a), static_cast<int>(pos));
 }
 
@@ -660,7 +735,8 @@ __device__ int build_vertex_polled(const SfxtParams& p, int v) {
   int s = -1;
   int cnt = 0;
   int lmax = -1;
-  float kmin = __int_as_float(0x7f800000);  // +inf
+  DevSidetrack top;  // the cheapest deviation (lane 0's copy is used)
+  top.head = -1;
   constexpr unsigned long long kNone = ~0ull;
   if (re - rb <= kRegChunks * 32) {
     DevEdge ed[kRegChunks];
@@ -730,7 +806,7 @@ __device__ int build_vertex_polled(const SfxtParams& p, int v) {
       rec.w = ed[0].w;
       rec.dist_head = dh[0];
       rec.key = deviation_key(dh[0], best, ed[0].w);
-      cnt = write_short_row(p, rb, valid, rec, kmin);
+      cnt = write_short_row(p, rb, valid, rec, top);
     } else if (re - rb <= 64) {
       DevSidetrack r[2];
       bool v[2];
@@ -742,23 +818,26 @@ __device__ int build_vertex_polled(const SfxtParams& p, int v) {
         r[c].dist_head = dh[c];
         r[c].key = deviation_key(dh[c], best, ed[c].w);
       }
-      cnt = write_row64(p, rb, v[0], r[0], v[1], r[1], kmin);
-    } else
+      cnt = write_row64(p, rb, v[0], r[0], v[1], r[1], top);
+    } else {
+      BestDev bd = best_none();
 #pragma unroll
-    for (int c = 0; c < kRegChunks; ++c) {
-      if (rb + c * 32 >= re) break;
-      const bool valid = ed[c].head >= 0 && ed[c].head != s && dh[c] != INT_MAX;
-      const unsigned bal = __ballot_sync(0xffffffffu, valid);
-      if (valid) {
-        DevSidetrack rec;
-        rec.head = ed[c].head;
-        rec.w = ed[c].w;
-        rec.dist_head = dh[c];
-        rec.key = deviation_key(dh[c], best, ed[c].w);
-        p.dev[rb + cnt + __popc(bal & lanemask_lt())] = rec;
-        kmin = fminf(kmin, rec.key);
+      for (int c = 0; c < kRegChunks; ++c) {
+        if (rb + c * 32 >= re) break;
+        const bool valid = ed[c].head >= 0 && ed[c].head != s && dh[c] != INT_MAX;
+        const unsigned bal = __ballot_sync(0xffffffffu, valid);
+        if (valid) {
+          DevSidetrack rec;
+          rec.head = ed[c].head;
+          rec.w = ed[c].w;
+          rec.dist_head = dh[c];
+          rec.key = deviation_key(dh[c], best, ed[c].w);
+          p.dev[rb + cnt + __popc(bal & lanemask_lt())] = rec;
+          best_take(bd, true, rec, c * 32 + lane);
+        }
+        cnt += __popc(bal);
       }
-      cnt += __popc(bal);
+      top = best_reduce(bd);
     }
     lmax = lvl;
   } else {
@@ -793,6 +872,7 @@ __device__ int build_vertex_polled(const SfxtParams& p, int v) {
       if (cand_dist(dist_of(ed.head), ed.w) == best) s = max(s, ed.head);
     }
     s = warp_max_i(s);
+    BestDev bd = best_none();
     for (int base = rb; base < re; base += 32) {
       const int e = base + lane;
       bool valid = false;
@@ -807,22 +887,20 @@ __device__ int build_vertex_polled(const SfxtParams& p, int v) {
         rec.key = deviation_key(dh, best, ed.w);
       }
       const unsigned bal = __ballot_sync(0xffffffffu, valid);
-      if (valid) {
-        p.dev[rb + cnt + __popc(bal & lanemask_lt())] = rec;
-        kmin = fminf(kmin, rec.key);
-      }
+      if (valid) p.dev[rb + cnt + __popc(bal & lanemask_lt())] = rec;
+      best_take(bd, valid, rec, e - rb);
       cnt += __popc(bal);
     }
+    top = best_reduce(bd);
     lmax = lvl;
   }
-  for (int o = 16; o > 0; o >>= 1) kmin = fminf(kmin, __shfl_xor_sync(0xffffffffu, kmin, o));
   if (lane == 0) {
     p.dist[v] = best;
     p.succ[v] = s;
     p.dev_cnt[v] = cnt;
     if (re - rb > 64 && cnt > 1 && cnt <= kSmemRow)  // left for sort_rows_kernel
       p.long_rows[atomicAdd(&p.ctr->n_long, 1)] = v;
-    p.deps[v] = __float_as_int(kmin);
+    if (cnt > 0) p.best[v] = top;
     p.level_of[v] = lmax;
     // the word carries everything a tail's build reads of v, so it needs
     // no fence before it

@@ -41,7 +41,7 @@ METRIC = "K-paths/sec"
 # DRAM bytes (read + write) per launch of the dominant kernels on this
 # workload, from the ncu captures summarised in profiles/ (the suffix-tree
 # build does not depend on K; the engine's figure is the K = 1e6 capture).
-KERNEL_TRAFFIC = {"sfxt_dataflow_kernel": 1_247_385_344, "engine_kernel": 321_948_672}
+KERNEL_TRAFFIC = {"sfxt_dataflow_kernel": 1_541_029_120, "engine_kernel": 284_772_352}
 
 
 def peaks():

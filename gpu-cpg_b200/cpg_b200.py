@@ -102,7 +102,8 @@ class ServerStats(C.Structure):
         ("p99_ms", C.c_double), ("mean_ms", C.c_double), ("max_ms", C.c_double),
         ("wall_s", C.c_double), ("paths_per_s", C.c_double), ("launches", C.c_int64),
         ("sfxt_rebuilds", C.c_int64), ("busy_ms", C.c_double), ("max_batch_seen", C.c_int32),
-        ("reserved", C.c_int32), ("sfxt_ms", C.c_double),
+        ("reserved", C.c_int32), ("sfxt_ms", C.c_double), ("retries", C.c_int64),
+        ("pool_rebuilds", C.c_int64), ("max_step_ms", C.c_double),
     ]
 
 

@@ -85,6 +85,10 @@ struct cpg_handle {
       d_ehist, d_esort, d_equery, d_ectr;
   size_t sorted_vals_off = 0;  // where the sorted path indices start in d_vals
   int64_t n_result = 0;
+  int64_t pool_rebuilds = 0;  // full suffix-tree rebuilds after the heap pool filled
+  // engine counters of the last launch that overflowed (valid while set)
+  bool overflow_known = false;
+  unsigned long long overflow_paths = 0, overflow_pend = 0;
   unsigned long long n_paths = 0;
   bool result_valid = false;
 
@@ -133,6 +137,17 @@ cudaError_t ensure(DevMem& b, size_t bytes) {
   cudaError_t e = cudaMalloc(&b.p, bytes);
   if (e == cudaSuccess) b.bytes = bytes;
   return e;
+}
+
+// ensure() for per-query buffers, whose size follows K and the batch: grows
+// to at least twice the old size, so a stream of growing queries reallocates
+// (and, with cudaFree, waits for the device) only a logarithmic number of times.
+cudaError_t ensure_grow(DevMem& b, size_t bytes) {
+  if (b.bytes >= bytes) return cudaSuccess;
+  const size_t want = b.bytes ? std::max(bytes, 2 * b.bytes) : bytes;
+  if (ensure(b, want) == cudaSuccess) return cudaSuccess;
+  cudaGetLastError();
+  return ensure(b, bytes);  // the doubled size did not fit: the size asked for
 }
 
 void release(DevMem& b) {
@@ -526,6 +541,7 @@ Status run_sfxt(cpg_handle* h, int32_t start_level) {
       // chain heaps outgrew their pool.  Incremental builds append to the
       // pool, so first rebuild from scratch (which compacts it); grow only
       // if a full build overflows.
+      h->pool_rebuilds += 1;
       if (start_level == 0) {
         st = grow_heap_pool(h);
         if (st != CPG_OK) return st;
@@ -614,6 +630,32 @@ float margin_of(float t, float root_abs) {
 }
 
 
+// Capacities for the rerun after an engine launch overflowed.  The launch's
+// counters kept counting past the ends, so a path store or pending pile that
+// overflowed grows to 1.5x what it was asked to hold (at least twice its
+// size); when neither did (the frontier or another buffer did), or the
+// counters are unknown, every pile grows 4x.  Growing only what overflowed
+// keeps the reallocation, which waits for the device, small.
+void grow_caps(cpg_handle* h) {
+  bool grown = false;
+  if (h->overflow_known) {
+    if (h->overflow_paths > h->cap_paths) {
+      h->cap_paths = std::max(2 * h->cap_paths, h->overflow_paths + h->overflow_paths / 2);
+      grown = true;
+    }
+    if (h->overflow_pend > h->cap_pend) {
+      h->cap_pend = std::max(2 * h->cap_pend, h->overflow_pend + h->overflow_pend / 2);
+      grown = true;
+    }
+  }
+  if (!grown) {
+    h->cap_paths *= 4;
+    h->cap_front *= 4;
+    h->cap_pend *= 4;
+  }
+  h->overflow_known = false;
+}
+
 Status alloc_query(cpg_handle* h, unsigned long long k) {
   const size_t cp = h->cap_paths, cf = h->cap_front, cpd = h->cap_pend;
   const size_t need =
@@ -623,26 +665,26 @@ Status alloc_query(cpg_handle* h, unsigned long long k) {
       static_cast<int64_t>(need) > h->opts.hbm_budget_bytes)
     return fail(h, CPG_ERR_CAPACITY, "query needs more device memory than hbm_budget_bytes");
   h->stats.bytes_reserved = static_cast<int64_t>(need);
-  CK(ensure(h->d_pcost, cp * 4), "alloc paths");
-  CK(ensure(h->d_pparent, cp * 4), "alloc paths");
-  CK(ensure(h->d_pfrom, cp * 4), "alloc paths");
-  CK(ensure(h->d_pto, cp * 4), "alloc paths");
-  CK(ensure(h->d_plevel, cp * 4), "alloc paths");
-  CK(ensure(h->d_front0, cf * sizeof(Item)), "alloc frontier");
-  CK(ensure(h->d_front1, cf * sizeof(Item)), "alloc frontier");
-  CK(ensure(h->d_pend0, cpd * sizeof(Item)), "alloc pending");
-  CK(ensure(h->d_pend1, cpd * sizeof(Item)), "alloc pending");
-  CK(ensure(h->d_pctr, sizeof(PfxtCounters)), "alloc counters");
-  CK(ensure(h->d_selstate, 64), "alloc select");
-  CK(ensure(h->d_selhist, 2048 * 4), "alloc select");
-  CK(ensure(h->d_counts, 64), "alloc counts");
-  CK(ensure(h->d_keys, 2 * k * 4), "alloc sort");
-  CK(ensure(h->d_vals, 2 * k * 4), "alloc sort");
-  CK(ensure(h->d_sorthist, 256 * ((k + 2047) / 2048) * 4), "alloc sort");
-  CK(ensure(h->d_cnt, 16), "alloc sort");
-  CK(ensure(h->d_rank, cp * 4), "alloc rank");
-  CK(ensure(h->d_out_cost, k * 4), "alloc output");
-  CK(ensure(h->d_out_nodes, k * sizeof(cpg_path_node)), "alloc output");
+  CK(ensure_grow(h->d_pcost, cp * 4), "alloc paths");
+  CK(ensure_grow(h->d_pparent, cp * 4), "alloc paths");
+  CK(ensure_grow(h->d_pfrom, cp * 4), "alloc paths");
+  CK(ensure_grow(h->d_pto, cp * 4), "alloc paths");
+  CK(ensure_grow(h->d_plevel, cp * 4), "alloc paths");
+  CK(ensure_grow(h->d_front0, cf * sizeof(Item)), "alloc frontier");
+  CK(ensure_grow(h->d_front1, cf * sizeof(Item)), "alloc frontier");
+  CK(ensure_grow(h->d_pend0, cpd * sizeof(Item)), "alloc pending");
+  CK(ensure_grow(h->d_pend1, cpd * sizeof(Item)), "alloc pending");
+  CK(ensure_grow(h->d_pctr, sizeof(PfxtCounters)), "alloc counters");
+  CK(ensure_grow(h->d_selstate, 64), "alloc select");
+  CK(ensure_grow(h->d_selhist, 2048 * 4), "alloc select");
+  CK(ensure_grow(h->d_counts, 64), "alloc counts");
+  CK(ensure_grow(h->d_keys, 2 * k * 4), "alloc sort");
+  CK(ensure_grow(h->d_vals, 2 * k * 4), "alloc sort");
+  CK(ensure_grow(h->d_sorthist, 256 * ((k + 2047) / 2048) * 4), "alloc sort");
+  CK(ensure_grow(h->d_cnt, 16), "alloc sort");
+  CK(ensure_grow(h->d_rank, cp * 4), "alloc rank");
+  CK(ensure_grow(h->d_out_cost, k * 4), "alloc output");
+  CK(ensure_grow(h->d_out_nodes, k * sizeof(cpg_path_node)), "alloc output");
   CK(cudaMemsetAsync(h->d_selhist.p, 0, 2048 * 4, h->stream), "memset hist");
   return CPG_OK;
 }
@@ -852,12 +894,12 @@ Status engine_prepare(cpg_handle* h, const std::vector<EngineQuery>& qs,
   int grid = 0;
   CK(engine_grid(h->device, h->engine_grid_limit, &grid), "engine occupancy");
   const size_t nq = qs.size();
-  CK(ensure(h->d_pq, h->cap_paths * 4), "alloc paths");
-  CK(ensure(h->d_qids, 2 * k_total * 4), "alloc sort");
-  CK(ensure(h->d_ehist, nq * static_cast<size_t>(kSelBins) * 4), "alloc select");
-  CK(ensure(h->d_esort, (256 * static_cast<size_t>(grid) + 256) * 4), "alloc sort");
-  CK(ensure(h->d_equery, nq * sizeof(EngineQuery)), "alloc queries");
-  CK(ensure(h->d_ectr, sizeof(EngineCounters)), "alloc counters");
+  CK(ensure_grow(h->d_pq, h->cap_paths * 4), "alloc paths");
+  CK(ensure_grow(h->d_qids, 2 * k_total * 4), "alloc sort");
+  CK(ensure_grow(h->d_ehist, nq * static_cast<size_t>(kSelBins) * 4), "alloc select");
+  CK(ensure_grow(h->d_esort, (256 * static_cast<size_t>(grid) + 256) * 4), "alloc sort");
+  CK(ensure_grow(h->d_equery, nq * sizeof(EngineQuery)), "alloc queries");
+  CK(ensure_grow(h->d_ectr, sizeof(EngineCounters)), "alloc counters");
   CK(cudaMemcpyAsync(h->d_equery.p, qs.data(), nq * sizeof(EngineQuery),
                      cudaMemcpyHostToDevice, h->stream), "H2D queries");
   CK(cudaStreamSynchronize(h->stream), "H2D queries");
@@ -937,7 +979,12 @@ int engine_finish(cpg_handle* h, std::vector<EngineQuery>& qout, EngineCounters&
   std::memcpy(&c, hb, sizeof(c));
   if (c.err == kDevTimeout)
     return fail(h, CPG_ERR_TIMEOUT, "query engine: grid barrier wait ran out");
-  if (c.err == kDevCapacity) return kRetry;
+  if (c.err == kDevCapacity) {
+    h->overflow_known = true;
+    h->overflow_paths = c.paths;
+    h->overflow_pend = c.pend_out;
+    return kRetry;
+  }
   CK(cudaMemcpy(qout.data(), h->d_equery.p, nq * sizeof(EngineQuery), cudaMemcpyDeviceToHost),
      "D2H queries");
   h->stats.paths_accepted = static_cast<int64_t>(c.paths);
@@ -1294,9 +1341,7 @@ cpg_status cpg_report_paths(cpg_handle* h, int64_t k) {
       const size_t held = static_cast<size_t>(h->stats.bytes_reserved);
       const size_t next = 4 * held;
       if (next > held + free_b * 9 / 10) break;
-      h->cap_paths *= 4;
-      h->cap_front *= 4;
-      h->cap_pend *= 4;
+      grow_caps(h);
       continue;
     }
     return static_cast<cpg_status>(r);
@@ -1733,9 +1778,7 @@ cpg_status cpg_batch_run(cpg_batch* b, int32_t rebuild_sfxt) {
       cudaMemGetInfo(&free_b, &total_b);
       const size_t held = static_cast<size_t>(h->stats.bytes_reserved);
       if (4 * held > held + free_b * 9 / 10) break;
-      h->cap_paths *= 4;
-      h->cap_front *= 4;
-      h->cap_pend *= 4;
+      grow_caps(h);
       b->prepared = false;
       rebuild = true;
       continue;
@@ -1883,8 +1926,8 @@ struct cpg_server {
   bool running = false, stopping = false;
   // statistics
   std::vector<double> lat_ms;
-  int64_t paths = 0, launches = 0, rebuilds = 0;
-  double busy_ms = 0, sfxt_ms = 0, first_submit = -1, last_done = 0;
+  int64_t paths = 0, launches = 0, rebuilds = 0, retries = 0, pool_rebuilds = 0;
+  double busy_ms = 0, sfxt_ms = 0, first_submit = -1, last_done = 0, max_step_ms = 0;
   int32_t max_batch_seen = 0;
 };
 
@@ -1969,6 +2012,8 @@ void server_loop(cpg_server* sv) {
         sv->queue.erase(sv->queue.begin() + static_cast<std::ptrdiff_t>(i));
       }
     }
+    const double t_step = now_s();
+    const int64_t pool_before = h->pool_rebuilds;
     Status st = CPG_OK;
     bool updated = false;
     for (const ServerReq& r : batch) {
@@ -1985,9 +2030,8 @@ void server_loop(cpg_server* sv) {
     for (int attempt = 0; st == CPG_OK && attempt < 10; ++attempt) {
       const int r = server_launch(sv, batch, out);
       if (r == kRetry) {
-        h->cap_paths *= 4;
-        h->cap_front *= 4;
-        h->cap_pend *= 4;
+        grow_caps(h);
+        sv->retries += 1;
         continue;
       }
       st = static_cast<Status>(r);
@@ -1997,6 +2041,8 @@ void server_loop(cpg_server* sv) {
     {
       std::lock_guard<std::mutex> lk(sv->mu);
       sv->max_batch_seen = std::max<int32_t>(sv->max_batch_seen, static_cast<int32_t>(batch.size()));
+      sv->max_step_ms = std::max(sv->max_step_ms, (t - t_step) * 1e3);
+      sv->pool_rebuilds += h->pool_rebuilds - pool_before;
       for (size_t i = 0; i < batch.size(); ++i) {
         ServerResult& res = sv->results[batch[i].ticket];
         res.status = st;
@@ -2173,6 +2219,9 @@ cpg_status cpg_server_get_stats(const cpg_server* svc, cpg_server_stats* out) {
   out->busy_ms = sv->busy_ms;
   out->max_batch_seen = sv->max_batch_seen;
   out->sfxt_ms = sv->sfxt_ms;
+  out->retries = sv->retries;
+  out->pool_rebuilds = sv->pool_rebuilds;
+  out->max_step_ms = sv->max_step_ms;
   return CPG_OK;
 }
 

@@ -93,6 +93,8 @@ struct alignas(16) Item {
 struct GridBarrier {
   unsigned int count;
   unsigned int gen;
+  int err;        // the status word as the last block to arrive found it
+  int pad;
 };
 
 // Device error codes, written to a status word by kernels and mapped to
@@ -357,7 +359,7 @@ struct EngineCounters {
   alignas(128) int err;
   int active;
   int sel_paths;              // some query selects over accepted paths
-  int pad0;
+  int err_stage;              // 1 + the first stage (barriers passed) with an error; 0 none
   // append cursors, each on its own 128-byte line
   alignas(128) unsigned long long paths;
   alignas(128) unsigned long long frontier[3];

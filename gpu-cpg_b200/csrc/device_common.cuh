@@ -17,7 +17,11 @@ __device__ __forceinline__ unsigned lanemask_lt() {
 // Grid-wide barrier for cooperative (co-resident) launches.  The wait is
 // bounded: after `limit` polls the block records kDevTimeout in *err and
 // leaves the barrier, so a lost block can never hang the GPU.  Returns false
-// once any block has recorded an error.
+// once any block has recorded an error before arriving: the last block to
+// arrive copies *err into the barrier, and every block decides on that copy,
+// so a block that leaves late does not see an error another block records
+// after the barrier (it would return while the others wait for it at the
+// next one).
 //
 // If snap_src is given, the last block to arrive copies snap_src[0..snap_n)
 // to snap_dst before releasing the others: a counter that blocks keep
@@ -27,17 +31,21 @@ __device__ __forceinline__ bool grid_sync(GridBarrier* b, int* err,
                                           unsigned int limit,
                                           const int* snap_src = nullptr,
                                           int* snap_dst = nullptr, int snap_n = 1) {
+  __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     volatile unsigned int* vgen = &b->gen;
     const unsigned int g = *vgen;
     __threadfence();
     const unsigned int arrived = atomicAdd(&b->count, 1u);
+    bool timed_out = false;
     if (arrived == gridDim.x - 1) {
+      __threadfence();
       if (snap_src)
         for (int i = 0; i < snap_n; ++i)
           reinterpret_cast<volatile int*>(snap_dst)[i] =
               reinterpret_cast<const volatile int*>(snap_src)[i];
+      reinterpret_cast<volatile int*>(&b->err)[0] = reinterpret_cast<volatile int*>(err)[0];
       atomicExch(&b->count, 0u);
       __threadfence();
       atomicAdd(&b->gen, 1u);
@@ -46,15 +54,17 @@ __device__ __forceinline__ bool grid_sync(GridBarrier* b, int* err,
       while (*vgen == g) {
         if (++it > limit) {
           atomicCAS(err, kDevOk, kDevTimeout);
+          timed_out = true;
           break;
         }
         __nanosleep(64);
       }
     }
     __threadfence();
+    s_ok = !timed_out && reinterpret_cast<volatile int*>(&b->err)[0] == kDevOk;
   }
   __syncthreads();
-  return *reinterpret_cast<volatile int*>(err) == kDevOk;
+  return s_ok != 0;
 }
 
 // Warp-aggregated append: one atomic per warp.  Every lane of the warp must

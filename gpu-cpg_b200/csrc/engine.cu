@@ -57,20 +57,37 @@ __device__ __forceinline__ unsigned long long gtime() {
 // arrive has nothing to reset and the others leave on the first poll that
 // sees its arrival.  eng_sync_last lets that last block run f() first and
 // then publish the same target in a second word the others wait on.  Waits
-// are bounded (kDevTimeout); both return false once any block has recorded
-// an error.
-__device__ __forceinline__ bool bar_wait(const EngineParams& p, const unsigned int* word,
+// are bounded (kDevTimeout).
+//
+// Errors carry the stage they happened in (stage n is the work between
+// barriers n - 1 and n), and barrier n fails for every block exactly when a
+// stage up to n recorded one.  A block that leaves barrier n late must not
+// see an error that a faster block records in stage n + 1: it would return
+// while the others wait for it at barrier n + 1.
+__shared__ unsigned int s_stage;  // the stage this block is in
+
+__device__ __forceinline__ void eng_fail(const EngineParams& p, int code) {
+  atomicCAS(&p.ctr->err, kDevOk, code);
+  atomicCAS(reinterpret_cast<unsigned int*>(&p.ctr->err_stage), 0u, s_stage + 1u);
+}
+
+__device__ __forceinline__ void bar_wait(const EngineParams& p, const unsigned int* word,
                                          unsigned int target) {
   const volatile unsigned int* w = word;
   unsigned int it = 0;
   while (static_cast<int>(*w - target) < 0) {
     if (++it > p.spin_limit) {
-      atomicCAS(&p.ctr->err, kDevOk, kDevTimeout);
-      return false;
+      eng_fail(p, kDevTimeout);
+      return;
     }
     __nanosleep(32);
   }
-  return true;
+}
+
+// On leaving barrier n (s_stage == n + 1): false if stages 0..n failed.
+__device__ __forceinline__ bool eng_passed(const EngineParams& p) {
+  const unsigned int es = *reinterpret_cast<const volatile unsigned int*>(&p.ctr->err_stage);
+  return es == 0u || es > s_stage;
 }
 
 __device__ __forceinline__ bool eng_sync(const EngineParams& p) {
@@ -80,9 +97,10 @@ __device__ __forceinline__ bool eng_sync(const EngineParams& p) {
     const unsigned int old = atomicAdd(&p.ctr->bar.count, 1u);
     bar_wait(p, &p.ctr->bar.count, (old / gridDim.x + 1u) * gridDim.x);
     __threadfence();
+    s_stage = old / gridDim.x + 1u;
   }
   __syncthreads();
-  return *reinterpret_cast<volatile int*>(&p.ctr->err) == kDevOk;
+  return eng_passed(p);
 }
 
 template <typename F>
@@ -107,8 +125,9 @@ __device__ __forceinline__ bool eng_sync_last(const EngineParams& p, F&& f) {
     bar_wait(p, &p.ctr->bar.gen, s_target);
     __threadfence();
   }
+  if (threadIdx.x == 0) s_stage = s_target / gridDim.x;
   __syncthreads();
-  return *reinterpret_cast<volatile int*>(&p.ctr->err) == kDevOk;
+  return eng_passed(p);
 }
 
 #define ENG_SYNC()              \
@@ -241,7 +260,7 @@ __device__ void seed_query(const EngineParams& p, int qi) {
         it.j = pack_j(static_cast<unsigned>(qi), 0);
         p.pend[0][slot] = it;
       } else {
-        atomicCAS(&p.ctr->err, kDevOk, kDevCapacity);
+        eng_fail(p, kDevCapacity);
       }
     }
   }
@@ -452,12 +471,12 @@ __device__ __forceinline__ int route(const EngineParams& p, Item* out,
   const unsigned long long a = warp_append(out_cnt, take);
   if (take) {
     if (a < p.front_cap) out[a] = it;
-    else atomicCAS(&p.ctr->err, kDevOk, kDevCapacity);
+    else eng_fail(p, kDevCapacity);
   }
   const unsigned long long b = warp_append(&p.ctr->pend_out, defer);
   if (defer) {
     if (b < p.pend_cap) pend_out[b] = it;
-    else atomicCAS(&p.ctr->err, kDevOk, kDevCapacity);
+    else eng_fail(p, kDevCapacity);
   }
   return defer ? 1 : 0;
 }
@@ -477,7 +496,7 @@ __device__ bool run_closure(const EngineParams& p, Item* pend_out) {
     const unsigned long long n_cur = fc[r % 3];
     if (n_cur == 0) break;
     if (n_cur > p.front_cap) {
-      atomicCAS(&p.ctr->err, kDevOk, kDevCapacity);
+      eng_fail(p, kDevCapacity);
       return false;
     }
     const Item* in = p.front[r & 1];
@@ -529,7 +548,7 @@ __device__ bool run_closure(const EngineParams& p, Item* pend_out) {
           p.pq[qp] = static_cast<int>(q);
           stored = true;
         } else {
-          atomicCAS(&p.ctr->err, kDevOk, kDevCapacity);
+          eng_fail(p, kDevCapacity);
         }
       }
       if (single) acc_nz += stored && it.cost != 0.0f;
@@ -578,11 +597,11 @@ __device__ bool run_closure(const EngineParams& p, Item* pend_out) {
         c.j = pack_j(q, cj);
         if (tm & bit) {
           if (bt < p.front_cap) out[bt] = c;
-          else atomicCAS(&p.ctr->err, kDevOk, kDevCapacity);
+          else eng_fail(p, kDevCapacity);
           ++bt;
         } else {
           if (bd < p.pend_cap) pend_out[bd] = c;
-          else atomicCAS(&p.ctr->err, kDevOk, kDevCapacity);
+          else eng_fail(p, kDevCapacity);
           ++bd;
         }
       }
@@ -796,6 +815,7 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
   const int nw = static_cast<int>(nth >> 5);
 
   unsigned long long t_last = 0;
+  if (threadIdx.x == 0) s_stage = 0;
   if (blockIdx.x == 0 && threadIdx.x == 0) t_last = gtime();
   // seed roots (pending pile 0)
   for (int qi = gw; qi < p.nq; qi += nw) seed_query(p, qi);
@@ -838,12 +858,12 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
         const unsigned long long a = warp_append(&p.ctr->frontier[0], take);
         if (take) {
           if (a < p.front_cap) p.front[0][a] = it;
-          else atomicCAS(&p.ctr->err, kDevOk, kDevCapacity);
+          else eng_fail(p, kDevCapacity);
         }
         const unsigned long long b = warp_append(&p.ctr->pend_out, keep);
         if (keep) {
           if (b < p.pend_cap) pend_next[b] = it;
-          else atomicCAS(&p.ctr->err, kDevOk, kDevCapacity);
+          else eng_fail(p, kDevCapacity);
         }
         if (single) {
           acc_n += keep;
@@ -874,7 +894,7 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
 
   // ---------------------------------------------------------------- output
   if (n_paths > p.ps.cap) {
-    atomicCAS(&p.ctr->err, kDevOk, kDevCapacity);
+    eng_fail(p, kDevCapacity);
     return;
   }
   // H. per-query counts are current (kept up to date by the closures)
@@ -903,7 +923,7 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
   STAMP(5);
   const unsigned long long n_out = *reinterpret_cast<volatile unsigned long long*>(&p.ctr->out_total);
   if (n_out > p.out_cap) {
-    atomicCAS(&p.ctr->err, kDevOk, kDevCapacity);
+    eng_fail(p, kDevCapacity);
     return;
   }
   // J. compaction into per-query segments: keys below the k-th, then the

@@ -309,6 +309,9 @@ typedef struct {
   int32_t max_batch_seen;
   int32_t reserved;
   double sfxt_ms;             /* device time of the suffix-tree rebuilds */
+  int64_t retries;            /* launches rerun after a query buffer grew */
+  int64_t pool_rebuilds;      /* full suffix-tree rebuilds after the heap pool filled */
+  double max_step_ms;         /* longest loop step: updates, rebuild, launch, results */
 } cpg_server_stats;
 
 void cpg_server_options_init(cpg_server_options* o);

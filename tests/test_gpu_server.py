@@ -103,6 +103,11 @@ def test_server_many_updates_rebuild_only_changed_graphs():
         qs.append((g, 500, (e, rng.uniform(0.1, 10.0, size=e.size).astype(np.float32))))
     mixed, st = _serve(dags, qs, max_batch=16)
     assert st["completed"] == len(qs)
+    # the diagnostics: every rebuild is counted, the pool filled at least
+    # once, and the longest step is a real duration
+    assert 1 <= st["sfxt_rebuilds"] <= len(qs)
+    assert st["pool_rebuilds"] >= 1 and st["retries"] >= 0
+    assert 0.0 < st["max_step_ms"] < 60_000.0
     csr = [_csr(d) for d in dags]
     for i, (g, k, upd) in enumerate(qs):
         adjp, adj, w = csr[g]

@@ -341,6 +341,69 @@ __device__ void select_hist(const EngineParams& p, unsigned long long n_paths,
   }
 }
 
+// select_pick for a single query by a whole block: each thread sums its
+// share of the bins, a block scan finds the share holding the krem-th key,
+// and its thread walks its few bins.  Each thread then clears its own bins.
+__device__ __noinline__ void select_pick_block(EngineQuery* q0, unsigned int* h, int shift,
+                                               int bits) {
+  __shared__ unsigned long long s_wsum[kEngWarps];
+  EngineQuery& Q = *q0;
+  if (Q.mode == 0) return;  // the same for every thread
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int bins = 1 << bits;
+  const int per = (bins + static_cast<int>(blockDim.x) - 1) / static_cast<int>(blockDim.x);
+  const int b0 = static_cast<int>(threadIdx.x) * per;
+  unsigned int mine[2] = {0u, 0u};  // per <= 2 (2048 bins, 1024 threads)
+  unsigned long long sum = 0;
+#pragma unroll
+  for (int t = 0; t < 2; ++t)
+    if (t < per && b0 + t < bins) {
+      mine[t] = __ldcg(h + b0 + t);
+      sum += mine[t];
+    }
+  // inclusive scan over the block, in thread (= bin) order
+  unsigned long long incl = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned long long y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) s_wsum[wid] = incl;
+  __syncthreads();
+  if (wid == 0) {
+    const int nwarps = static_cast<int>(blockDim.x >> 5);
+    unsigned long long w = lane < nwarps ? s_wsum[lane] : 0ull;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned long long y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    if (lane < nwarps) s_wsum[lane] = w;  // inclusive over warps
+  }
+  __syncthreads();
+  incl += wid > 0 ? s_wsum[wid - 1] : 0ull;
+  const unsigned long long total = s_wsum[(blockDim.x >> 5) - 1];
+  const unsigned long long k = Q.krem;
+  const unsigned long long excl = incl - sum;
+  // k beyond the total (cannot happen when the counts hold): the last thread
+  const bool owner = (excl < k && k <= incl) ||
+                     (k > total && threadIdx.x == blockDim.x - 1);
+  __syncthreads();  // every thread has read krem before the owner updates it
+  if (owner) {
+    unsigned long long acc = excl;
+    int bin = b0;
+    if (per == 2 && acc + mine[0] < k) {  // the key is in the second bin
+      acc += mine[0];
+      ++bin;
+    }
+    Q.prefix |= static_cast<unsigned>(bin) << shift;
+    Q.krem = k - acc;
+  }
+#pragma unroll
+  for (int t = 0; t < 2; ++t)
+    if (t < per && b0 + t < bins) h[b0 + t] = 0u;
+}
+
 // One warp per selecting query (warps gw, gw + nw, ...): find the bin
 // holding the krem-th key.
 __device__ void select_pick(const EngineParams& p, int shift, int bits, int gw, int nw) {
@@ -420,8 +483,11 @@ __device__ bool run_select(const EngineParams& p, unsigned long long n_paths,
     select_hist(p, n_paths, pend, n_pend, shift, bits);
     if (fused) {
       if (!eng_sync_last(p, [&]() {
-            select_pick(p, shift, bits, static_cast<int>(threadIdx.x >> 5),
-                        static_cast<int>(blockDim.x >> 5));
+            if (p.nq == 1)
+              select_pick_block(p.q, p.hist, shift, bits);
+            else
+              select_pick(p, shift, bits, static_cast<int>(threadIdx.x >> 5),
+                          static_cast<int>(blockDim.x >> 5));
             if (last && with_limits) {
               __syncthreads();
               set_limits(p, threadIdx.x, blockDim.x, threadIdx.x == 0);

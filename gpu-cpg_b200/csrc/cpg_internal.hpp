@@ -344,7 +344,7 @@ struct EngineQuery {
   int done;
   float t, lim, tie, root_abs;
   unsigned int prefix;        // radix select state
-  unsigned int pad0;
+  unsigned int coarse;        // growth phase split at a bin's upper edge
   unsigned long long krem;    // rank still wanted inside the prefix
   unsigned long long ksel;    // rank the select started from
   unsigned long long paths_nz, pend_nz, pend_n;     // maintained incrementally
@@ -360,6 +360,7 @@ struct EngineCounters {
   int active;
   int sel_paths;              // some query selects over accepted paths
   int err_stage;              // 1 + the first stage (barriers passed) with an error; 0 none
+  int sel_stop;               // the select of this phase ended a pass early
   // append cursors, each on its own 128-byte line
   alignas(128) unsigned long long paths;
   alignas(128) unsigned long long frontier[3];

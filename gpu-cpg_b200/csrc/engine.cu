@@ -345,7 +345,7 @@ __device__ void select_hist(const EngineParams& p, unsigned long long n_paths,
 // share of the bins, a block scan finds the share holding the krem-th key,
 // and its thread walks its few bins.  Each thread then clears its own bins.
 __device__ __noinline__ void select_pick_block(EngineQuery* q0, unsigned int* h, int shift,
-                                               int bits) {
+                                               int bits, unsigned int* chosen_n) {
   __shared__ unsigned long long s_wsum[kEngWarps];
   EngineQuery& Q = *q0;
   if (Q.mode == 0) return;  // the same for every thread
@@ -398,6 +398,7 @@ __device__ __noinline__ void select_pick_block(EngineQuery* q0, unsigned int* h,
     }
     Q.prefix |= static_cast<unsigned>(bin) << shift;
     Q.krem = k - acc;
+    *chosen_n = bin == b0 ? mine[0] : mine[1];
   }
 #pragma unroll
   for (int t = 0; t < 2; ++t)
@@ -457,8 +458,9 @@ __device__ void set_limits(const EngineParams& p, unsigned t0, unsigned nt, bool
       Q.tie = t;
     } else {
       // accept strictly below the split when anything pending is cheaper
-      // than it (ksel - krem items are), so a tie group at the split waits
-      Q.lim = Q.ksel > Q.krem ? float_below(t) : t;
+      // than it (ksel - krem items are), so a tie group at the split waits;
+      // a coarse split is a bin's upper edge and takes the whole bin
+      Q.lim = (Q.ksel > Q.krem && !Q.coarse) ? float_below(t) : t;
       Q.tie = __int_as_float(0x7fc00000);  // NaN: expand every path
     }
   }
@@ -482,18 +484,38 @@ __device__ bool run_select(const EngineParams& p, unsigned long long n_paths,
     const bool last = pass == p.sel_passes - 1;
     select_hist(p, n_paths, pend, n_pend, shift, bits);
     if (fused) {
+      __shared__ unsigned int s_chosen_n;
       if (!eng_sync_last(p, [&]() {
-            if (p.nq == 1)
-              select_pick_block(p.q, p.hist, shift, bits);
-            else
+            bool done = last;
+            if (p.nq == 1) {
+              select_pick_block(p.q, p.hist, shift, bits, &s_chosen_n);
+              __syncthreads();
+              // A growth phase needs only about j items promoted, not the
+              // j-th exactly: when the bin holding it is small against j,
+              // split at the bin's upper edge and skip the last pass.
+              EngineQuery& Q = p.q[0];
+              if (with_limits && pass == p.sel_passes - 2 && Q.mode == 1 &&
+                  static_cast<unsigned long long>(s_chosen_n) <=
+                      (Q.ksel / 8 > 256 ? Q.ksel / 8 : 256ull)) {
+                __syncthreads();  // every thread has read the query's mode
+                if (threadIdx.x == 0) {
+                  Q.prefix |= (1u << shift) - 1u;
+                  Q.coarse = 1;
+                  p.ctr->sel_stop = 1;
+                }
+                done = true;
+              }
+            } else {
               select_pick(p, shift, bits, static_cast<int>(threadIdx.x >> 5),
                           static_cast<int>(blockDim.x >> 5));
-            if (last && with_limits) {
+            }
+            if (done && with_limits) {
               __syncthreads();
               set_limits(p, threadIdx.x, blockDim.x, threadIdx.x == 0);
             }
           }))
         return false;
+      if (*reinterpret_cast<volatile int*>(&p.ctr->sel_stop)) break;
     } else {
       if (!eng_sync(p)) return false;
       select_pick(p, shift, bits, static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 5),
@@ -800,6 +822,7 @@ __device__ bool decide_query(const EngineParams& p, EngineQuery& Q) {
   Q.mode = 0;
   if (Q.done) return false;
   Q.prefix = 0;
+  Q.coarse = 0;
   // Every path costing <= the last phase's limit is accepted, so once
   // K non-zero paths are, the K-th of them is the answer's K-th cost and
   // the final phase only sweeps items within the rounding margin.
@@ -857,6 +880,7 @@ __device__ void next_phase(const EngineParams& p, int phase, bool finish) {
     if (finish) p.ctr->phases = phase + 1;
     p.ctr->active = 0;
     p.ctr->sel_paths = 0;
+    p.ctr->sel_stop = 0;
   }
   __syncthreads();
   for (int qi = threadIdx.x; qi < p.nq; qi += blockDim.x) {

@@ -549,26 +549,6 @@ __device__ __forceinline__ unsigned long long warp_reserve(unsigned long long* c
   return base + (incl - n);
 }
 
-// Route one candidate (all lanes call): cost <= lim joins the next round's
-// frontier, the rest the next phase's pending pile.  Returns 1 if deferred.
-__device__ __forceinline__ int route(const EngineParams& p, Item* out,
-                                     unsigned long long* out_cnt, Item* pend_out,
-                                     bool exists, const Item& it, float lim) {
-  const bool take = exists && it.cost <= lim;
-  const bool defer = exists && !take;
-  const unsigned long long a = warp_append(out_cnt, take);
-  if (take) {
-    if (a < p.front_cap) out[a] = it;
-    else eng_fail(p, kDevCapacity);
-  }
-  const unsigned long long b = warp_append(&p.ctr->pend_out, defer);
-  if (defer) {
-    if (b < p.pend_cap) pend_out[b] = it;
-    else eng_fail(p, kDevCapacity);
-  }
-  return defer ? 1 : 0;
-}
-
 // Rounds over the frontier until it is empty.  Returns false on error.
 __device__ bool run_closure(const EngineParams& p, Item* pend_out) {
   const unsigned long long tid =

@@ -78,15 +78,6 @@ __device__ __forceinline__ bool cand_row(const PfxtGraph& g, const HeapNode& hn,
   return true;
 }
 
-// Candidate (parent path, heap node, index j): fills its cost.  Returns false
-// if the candidate does not exist.
-__device__ __forceinline__ bool make_candidate(const PfxtGraph& g, int node, int j,
-                                               float parent_cost, float& cost) {
-  if (node < 0) return false;
-  if (j == 0) return cand_top(g, node, parent_cost, cost);
-  return cand_row(g, load_node(g.hnodes, node), j, parent_cost, cost);
-}
-
 // Head of entry j of the sorted row of hn's vertex: the last edge of the
 // path that takes that deviation.
 __device__ __forceinline__ int dev_head(const PfxtGraph& g, const HeapNode& hn, int j) {

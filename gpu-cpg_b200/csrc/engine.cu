@@ -682,15 +682,15 @@ __device__ bool run_closure(const EngineParams& p, Item* pend_out) {
         qadd(p.q, QOFF(pend_next_nz), valid, q, ndef_nz);
       }
     }
-    if (single) {
-      // one query: counts kept per thread through the round, added once
-      qadd(p.q, QOFF(paths_nz), acc_nz != 0, 0u, acc_nz);
-      qadd(p.q, QOFF(pend_next_n), acc_pn != 0, 0u, acc_pn);
-      qadd(p.q, QOFF(pend_next_nz), acc_pnz != 0, 0u, acc_pnz);
-      acc_nz = acc_pn = acc_pnz = 0;
-    }
     if (!eng_sync(p)) return false;
     ++r;
+  }
+  if (single) {
+    // one query: counts kept per thread through the whole closure (nothing
+    // reads them before the phase ends), added once
+    qadd(p.q, QOFF(paths_nz), acc_nz != 0, 0u, acc_nz);
+    qadd(p.q, QOFF(pend_next_n), acc_pn != 0, 0u, acc_pn);
+    qadd(p.q, QOFF(pend_next_nz), acc_pnz != 0, 0u, acc_pnz);
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) p.ctr->rounds += r;
   return true;

@@ -368,6 +368,111 @@ __device__ int build_vertex(const SfxtParams& p, int v, int lvl, bool do_kahn) {
   return lvl;
 }
 
+// Level-synchronous builds of short rows: a warp builds four vertices at
+// once, one per 8-lane group, so a level of low-degree vertices costs a
+// quarter of the warp passes.  Rows of at most kGroupRow edges qualify.
+constexpr int kGroupRow = 8;
+
+__device__ __forceinline__ int group_min_i(int x) {
+#pragma unroll
+  for (int o = 4; o > 0; o >>= 1) x = min(x, __shfl_xor_sync(0xffffffffu, x, o, 8));
+  return x;
+}
+
+__device__ __forceinline__ int group_max_i(int x) {
+#pragma unroll
+  for (int o = 4; o > 0; o >>= 1) x = max(x, __shfl_xor_sync(0xffffffffu, x, o, 8));
+  return x;
+}
+
+// Position of the k-th (from 0) set bit of m; k < popc(m).
+__device__ __forceinline__ int kth_set_bit(unsigned m, int k) {
+  int pos = 0;
+#pragma unroll
+  for (int w = 16; w > 0; w >>= 1) {
+    const int c = __popc(m & ((1u << w) - 1u));
+    if (k >= c) {
+      k -= c;
+      m >>= w;
+      pos += w;
+    }
+  }
+  return pos;
+}
+
+// Builds vertex v (< 0: none) of each 8-lane group, whose row has at most
+// kGroupRow edges, at level lvl: the same distance, successor, sorted
+// deviation row and Kahn step as build_vertex.  Every lane of the warp calls.
+__device__ void build_group8(const SfxtParams& p, int v, int lvl, bool do_kahn) {
+  const int lane = threadIdx.x & 31;
+  const int l = lane & 7, g = lane >> 3;
+  const bool has_v = v >= 0;
+  int rb = 0, re = 0;
+  if (has_v) {
+    rb = p.adjp[v];
+    re = p.adjp[v + 1];
+  }
+  const bool has = has_v && rb + l < re;
+  DevEdge ed;
+  ed.head = -1;
+  ed.w = 0.f;
+  if (has) ed = p.edges[rb + l];
+  const int dh = has ? __ldcg(p.dist + ed.head) : INT_MAX;
+  int best = group_min_i(has ? cand_dist(dh, ed.w) : INT_MAX);
+  if (lvl == 0) best = 0;  // sinks start at distance 0
+  const int s = group_max_i(has && lvl > 0 && cand_dist(dh, ed.w) == best ? ed.head : -1);
+  // deviations: every edge but the successor's, sorted by (key, position)
+  const bool valid = has && ed.head != s && dh != INT_MAX;
+  DevSidetrack rec;
+  rec.head = ed.head;
+  rec.w = ed.w;
+  rec.dist_head = dh;
+  rec.key = deviation_key(dh, best, ed.w);
+  unsigned long long x = valid ? sort_word(rec.key, l) : ~0ull;
+#pragma unroll
+  for (int k = 2; k <= 8; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      const unsigned long long y = __shfl_xor_sync(0xffffffffu, x, j, 8);
+      const bool up = (l & k) == 0;
+      const bool lower = (l & j) == 0;
+      x = (lower == up) ? (x < y ? x : y) : (x > y ? x : y);
+    }
+  }
+  const unsigned bal = __ballot_sync(0xffffffffu, valid);
+  const int cnt = __popc((bal >> (g * 8)) & 0xffu);
+  const int src = (g << 3) | static_cast<int>(x & 7u);
+  DevSidetrack o;
+  o.head = __shfl_sync(0xffffffffu, rec.head, src);
+  o.w = __shfl_sync(0xffffffffu, rec.w, src);
+  o.dist_head = __shfl_sync(0xffffffffu, rec.dist_head, src);
+  o.key = __shfl_sync(0xffffffffu, rec.key, src);
+  if (has_v && l < cnt) p.dev[rb + l] = o;
+  if (has_v && l == 0) {
+    p.dist[v] = best;
+    p.succ[v] = s;
+    p.dev_cnt[v] = cnt;
+    if (cnt > 0) p.best[v] = o;  // the row's first entry
+  }
+  if (do_kahn) {
+    // every fan-in neighbour loses one pending fan-out; the last one to
+    // reach zero joins the next level
+    const int ib = has_v ? p.iadjp[v] : 0;
+    const int ie = has_v ? p.iadjp[v + 1] : 0;
+    const int passes = warp_max_i((ie - ib + 7) >> 3);
+    for (int r = 0; r < passes; ++r) {
+      const int e = ib + r * 8 + l;
+      const int u = e < ie ? p.iadj[e] : -1;
+      const bool ready = u >= 0 && atomicSub(&p.deps[u], 1) == 1;
+      const int slot = warp_append(&p.ctr->tail, ready);
+      if (ready) {
+        p.order[slot] = u;
+        p.level_of[u] = lvl + 1;
+      }
+    }
+  }
+}
+
 // Whether an incremental build rebuilds v (at level lvl).
 __device__ __forceinline__ bool rebuilt(const SfxtParams& p, int v, int lvl) {
   return !p.vgraph || lvl >= __ldg(p.graph_from + __ldg(p.vgraph + v));
@@ -456,37 +561,47 @@ __device__ __forceinline__ void store_heap_node(HeapNode* at, const HeapElem& e,
   q[1] = make_int4(e.head, __float_as_int(e.w), e.dist_head, e.dist_v);
 }
 
-template <bool kPublish = false>
-__device__ void heap_insert(const SfxtParams& p, int v, unsigned long long* chunk = nullptr) {
+// What an insert of v needs: its successor's heap and its element.
+struct InsertPlan {
+  int base_root, base_size;
+  bool empty;   // v has no deviation: its heap is its successor's
+  HeapElem ce;
+};
+
+__device__ __forceinline__ InsertPlan plan_insert(const SfxtParams& p, int v) {
+  InsertPlan q;
   const int s = __ldcg(p.succ + v);
   const int cnt = __ldcg(p.dev_cnt + v);
-  const int base_root = s >= 0 ? __ldcg(p.ht_root + s) : -1;
-  const int base_size = s >= 0 ? __ldcg(p.ht_size + s) : 0;
-  if (cnt == 0) {
-    heap_store<kPublish>(p, v, base_root, base_size);
-    return;
-  }
-  // v's element: its cheapest deviation, as the build left it
-  HeapElem ce;
-  {
+  q.base_root = s >= 0 ? __ldcg(p.ht_root + s) : -1;
+  q.base_size = s >= 0 ? __ldcg(p.ht_size + s) : 0;
+  q.empty = cnt == 0;
+  if (!q.empty) {
+    // v's element: its cheapest deviation, as the build left it
     const int4 b = __ldcg(reinterpret_cast<const int4*>(p.best + v));
-    ce.vtx = v;
-    ce.row = __ldg(p.adjp + v);
-    ce.head = b.x;
-    ce.w = __int_as_float(b.y);
-    ce.dist_head = b.z;
-    ce.key = __int_as_float(b.w);
-    ce.dist_v = __ldcg(p.dist + v);
+    q.ce.vtx = v;
+    q.ce.row = __ldg(p.adjp + v);
+    q.ce.head = b.x;
+    q.ce.w = __int_as_float(b.y);
+    q.ce.dist_head = b.z;
+    q.ce.key = __int_as_float(b.w);
+    q.ce.dist_v = __ldcg(p.dist + v);
   }
-  const unsigned pos = static_cast<unsigned>(base_size) + 1u;
+  return q;
+}
+
+// Nodes an insert into a heap of base_size elements copies.
+__device__ __forceinline__ unsigned insert_nodes(int base_size) {
+  return static_cast<unsigned>(31 - __clz(static_cast<unsigned>(base_size) + 1u)) + 1u;
+}
+
+// The insert itself, into nodes a .. a + depth already taken from the pool.
+template <bool kPublish>
+__device__ __forceinline__ void heap_insert_at(const SfxtParams& p, int v, const InsertPlan& q,
+                                               unsigned long long a) {
+  HeapElem ce = q.ce;
+  const unsigned pos = static_cast<unsigned>(q.base_size) + 1u;
   const int depth = 31 - __clz(pos);
-  const unsigned long long a = heap_alloc(p, static_cast<unsigned>(depth + 1), chunk);
-  if (a == ~0ull) {
-    atomicCAS(&p.ctr->err, kDevOk, kDevCapacity);
-    heap_store<kPublish>(p, v, -1, 0);
-    return;
-  }
-  int cur = base_root;
+  int cur = q.base_root;
   for (int d = depth - 1; d >= 0; --d) {
     const HeapNode old = load_heap_node(p.hnodes, cur);
     const HeapElem oe = elem_of(old);
@@ -500,6 +615,56 @@ __device__ void heap_insert(const SfxtParams& p, int v, unsigned long long* chun
   }
   store_heap_node(p.hnodes + a + depth, ce, -1, -1);
   heap_store<kPublish>(p, v, static_cast<int>(a), static_cast<int>(pos));
+}
+
+template <bool kPublish = false>
+__device__ void heap_insert(const SfxtParams& p, int v, unsigned long long* chunk = nullptr) {
+  const InsertPlan q = plan_insert(p, v);
+  if (q.empty) {
+    heap_store<kPublish>(p, v, q.base_root, q.base_size);
+    return;
+  }
+  const unsigned long long a = heap_alloc(p, insert_nodes(q.base_size), chunk);
+  if (a == ~0ull) {
+    atomicCAS(&p.ctr->err, kDevOk, kDevCapacity);
+    heap_store<kPublish>(p, v, -1, 0);
+    return;
+  }
+  heap_insert_at<kPublish>(p, v, q, a);
+}
+
+// Level-synchronous inserts, one vertex per lane (v < 0: none): the warp
+// takes all its lanes' nodes with one atomic on the pool cursor.  Every lane
+// of the warp calls.
+__device__ void heap_insert_lanes(const SfxtParams& p, int v) {
+  const int lane = threadIdx.x & 31;
+  InsertPlan q;
+  q.empty = true;
+  q.base_root = -1;
+  q.base_size = 0;
+  if (v >= 0) q = plan_insert(p, v);
+  const unsigned need = v >= 0 && !q.empty ? insert_nodes(q.base_size) : 0u;
+  unsigned incl = need;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  const unsigned tot = __shfl_sync(0xffffffffu, incl, 31);
+  unsigned long long base = 0;
+  if (lane == 31 && tot) base = atomicAdd(&p.ctr->hnode_used, static_cast<unsigned long long>(tot));
+  base = __shfl_sync(0xffffffffu, base, 31);
+  if (v < 0) return;
+  if (q.empty) {
+    heap_store<false>(p, v, q.base_root, q.base_size);
+    return;
+  }
+  if (base + tot > p.hnode_cap) {
+    atomicCAS(&p.ctr->err, kDevOk, kDevCapacity);
+    heap_store<false>(p, v, -1, 0);
+    return;
+  }
+  heap_insert_at<false>(p, v, q, base + (incl - need));
 }
 
 // BVSS form of the Kahn step.  A vertex that joins level L sets its bit in
@@ -625,16 +790,45 @@ sfxt_persistent_kernel(SfxtParams p) {
       if (lvl > first && !p.append_pool)
         p.pool_mark[lvl - 1] = *reinterpret_cast<volatile unsigned long long*>(&p.ctr->hnode_used);
     }
-    for (int i = beg + gwarp; i < end; i += nwarps) {
-      const int v = __ldcg(p.order + i);
-      if (full || rebuilt(p, v, lvl)) build_vertex(p, v, lvl, full && !kBvss);
+    {
+      // a warp takes c consecutive vertices of the level (4..32, so that all
+      // warps share a wide level): short rows four at a time by 8-lane
+      // groups, the others one at a time by the whole warp
+      const int lane = threadIdx.x & 31;
+      const int per = (end - beg + nwarps - 1) / nwarps;
+      const int c = per <= 4 ? 4 : per >= 32 ? 32 : (per + 3) & ~3;
+      for (int i0 = beg + c * gwarp; i0 < end; i0 += c * nwarps) {
+        const int i = i0 + lane;
+        int v = -1;
+        bool shortrow = false;
+        if (lane < c && i < end) {
+          v = __ldcg(p.order + i);
+          if (!(full || rebuilt(p, v, lvl))) v = -1;
+          else shortrow = p.adjp[v + 1] - p.adjp[v] <= kGroupRow;
+        }
+        const unsigned sm = __ballot_sync(0xffffffffu, v >= 0 && shortrow);
+        const unsigned lg = __ballot_sync(0xffffffffu, v >= 0 && !shortrow);
+        const int ns = __popc(sm);
+        for (int t = 0; t < ns; t += 4) {
+          const int k = t + (lane >> 3);
+          const int from = k < ns ? kth_set_bit(sm, k) : 0;
+          const int vg = __shfl_sync(0xffffffffu, v, from);
+          build_group8(p, k < ns ? vg : -1, lvl, full && !kBvss);
+        }
+        for (unsigned b = lg; b; b &= b - 1) {
+          const int vb = __shfl_sync(0xffffffffu, v, __ffs(b) - 1);
+          build_vertex(p, vb, lvl, full && !kBvss);
+        }
+      }
     }
     if (kBvss && pull)
       for (int i = abeg + gwarp; i < aend; i += nwarps)
         bvss_pull_interval(p, __ldcg(p.act_list + i), lvl, n_tensor, n_scalar);
-    for (int i = pbeg + tid; i < pend; i += nth) {
-      const int v = __ldcg(p.order + i);
-      if (full || rebuilt(p, v, lvl - 1)) heap_insert(p, v);
+    for (int i0 = pbeg + (tid & ~31); i0 < pend; i0 += nth) {
+      const int i = i0 + (threadIdx.x & 31);
+      int v = i < pend ? __ldcg(p.order + i) : -1;
+      if (v >= 0 && !(full || rebuilt(p, v, lvl - 1))) v = -1;
+      heap_insert_lanes(p, v);
     }
     // the tail keeps growing as soon as the next level starts appending, so
     // the level bound is the snapshot the last arriving block took
@@ -656,9 +850,11 @@ sfxt_persistent_kernel(SfxtParams p) {
   // heaps of the last level
   if (blockIdx.x == 0 && threadIdx.x == 0 && lvl > first && !p.append_pool)
     p.pool_mark[lvl - 1] = *reinterpret_cast<volatile unsigned long long*>(&p.ctr->hnode_used);
-  for (int i = pbeg + tid; i < pend; i += nth) {
-    const int v = __ldcg(p.order + i);
-    if (full || rebuilt(p, v, lvl - 1)) heap_insert(p, v);
+  for (int i0 = pbeg + (tid & ~31); i0 < pend; i0 += nth) {
+    const int i = i0 + (threadIdx.x & 31);
+    int v = i < pend ? __ldcg(p.order + i) : -1;
+    if (v >= 0 && !(full || rebuilt(p, v, lvl - 1))) v = -1;
+    heap_insert_lanes(p, v);
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     p.ctr->levels = lvl;

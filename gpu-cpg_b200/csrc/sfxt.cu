@@ -369,19 +369,21 @@ __device__ int build_vertex(const SfxtParams& p, int v, int lvl, bool do_kahn) {
 }
 
 // Level-synchronous builds of short rows: a warp builds four vertices at
-// once, one per 8-lane group, so a level of low-degree vertices costs a
-// quarter of the warp passes.  Rows of at most kGroupRow edges qualify.
-constexpr int kGroupRow = 8;
+// once, one per 8-lane group (rows of at most 8 edges), or two, one per
+// 16-lane group (at most 16), so a level of low-degree vertices costs a
+// fraction of the warp passes.
 
+template <int G>
 __device__ __forceinline__ int group_min_i(int x) {
 #pragma unroll
-  for (int o = 4; o > 0; o >>= 1) x = min(x, __shfl_xor_sync(0xffffffffu, x, o, 8));
+  for (int o = G / 2; o > 0; o >>= 1) x = min(x, __shfl_xor_sync(0xffffffffu, x, o, G));
   return x;
 }
 
+template <int G>
 __device__ __forceinline__ int group_max_i(int x) {
 #pragma unroll
-  for (int o = 4; o > 0; o >>= 1) x = max(x, __shfl_xor_sync(0xffffffffu, x, o, 8));
+  for (int o = G / 2; o > 0; o >>= 1) x = max(x, __shfl_xor_sync(0xffffffffu, x, o, G));
   return x;
 }
 
@@ -400,27 +402,38 @@ __device__ __forceinline__ int kth_set_bit(unsigned m, int k) {
   return pos;
 }
 
-// Builds vertex v (< 0: none) of each 8-lane group, whose row has at most
-// kGroupRow edges, at level lvl: the same distance, successor, sorted
-// deviation row and Kahn step as build_vertex.  Every lane of the warp calls.
-__device__ void build_group8(const SfxtParams& p, int v, int lvl, bool do_kahn) {
+// Builds vertex v (< 0: none) of each G-lane group, whose row has at most G
+// edges, at level lvl: the same distance, successor, sorted deviation row and
+// Kahn step as build_vertex.  Every lane of the warp calls.
+template <int G>
+__device__ void build_group(const SfxtParams& p, int v, int lvl, bool do_kahn) {
   const int lane = threadIdx.x & 31;
-  const int l = lane & 7, g = lane >> 3;
+  const int l = lane & (G - 1), g = lane / G;
   const bool has_v = v >= 0;
-  int rb = 0, re = 0;
+  // The build's loads and the Kahn step's are independent, so each round
+  // trip carries both: the row and fan-in ranges, then the row's edge and
+  // the first fan-in tail, then the head's distance and that tail's
+  // decrement.
+  int rb = 0, re = 0, ib = 0, ie = 0;
   if (has_v) {
     rb = p.adjp[v];
     re = p.adjp[v + 1];
+    if (do_kahn) {
+      ib = p.iadjp[v];
+      ie = p.iadjp[v + 1];
+    }
   }
   const bool has = has_v && rb + l < re;
   DevEdge ed;
   ed.head = -1;
   ed.w = 0.f;
   if (has) ed = p.edges[rb + l];
+  const int u0 = ib + l < ie ? p.iadj[ib + l] : -1;
   const int dh = has ? __ldcg(p.dist + ed.head) : INT_MAX;
-  int best = group_min_i(has ? cand_dist(dh, ed.w) : INT_MAX);
+  const bool ready0 = u0 >= 0 && atomicSub(&p.deps[u0], 1) == 1;
+  int best = group_min_i<G>(has ? cand_dist(dh, ed.w) : INT_MAX);
   if (lvl == 0) best = 0;  // sinks start at distance 0
-  const int s = group_max_i(has && lvl > 0 && cand_dist(dh, ed.w) == best ? ed.head : -1);
+  const int s = group_max_i<G>(has && lvl > 0 && cand_dist(dh, ed.w) == best ? ed.head : -1);
   // deviations: every edge but the successor's, sorted by (key, position)
   const bool valid = has && ed.head != s && dh != INT_MAX;
   DevSidetrack rec;
@@ -430,18 +443,18 @@ __device__ void build_group8(const SfxtParams& p, int v, int lvl, bool do_kahn) 
   rec.key = deviation_key(dh, best, ed.w);
   unsigned long long x = valid ? sort_word(rec.key, l) : ~0ull;
 #pragma unroll
-  for (int k = 2; k <= 8; k <<= 1) {
+  for (int k = 2; k <= G; k <<= 1) {
 #pragma unroll
     for (int j = k >> 1; j > 0; j >>= 1) {
-      const unsigned long long y = __shfl_xor_sync(0xffffffffu, x, j, 8);
+      const unsigned long long y = __shfl_xor_sync(0xffffffffu, x, j, G);
       const bool up = (l & k) == 0;
       const bool lower = (l & j) == 0;
       x = (lower == up) ? (x < y ? x : y) : (x > y ? x : y);
     }
   }
   const unsigned bal = __ballot_sync(0xffffffffu, valid);
-  const int cnt = __popc((bal >> (g * 8)) & 0xffu);
-  const int src = (g << 3) | static_cast<int>(x & 7u);
+  const int cnt = __popc((bal >> (g * G)) & ((1u << G) - 1u));
+  const int src = g * G + static_cast<int>(x & static_cast<unsigned long long>(G - 1));
   DevSidetrack o;
   o.head = __shfl_sync(0xffffffffu, rec.head, src);
   o.w = __shfl_sync(0xffffffffu, rec.w, src);
@@ -456,14 +469,12 @@ __device__ void build_group8(const SfxtParams& p, int v, int lvl, bool do_kahn) 
   }
   if (do_kahn) {
     // every fan-in neighbour loses one pending fan-out; the last one to
-    // reach zero joins the next level
-    const int ib = has_v ? p.iadjp[v] : 0;
-    const int ie = has_v ? p.iadjp[v + 1] : 0;
-    const int passes = warp_max_i((ie - ib + 7) >> 3);
+    // reach zero joins the next level (the first G went above)
+    const int passes = warp_max_i((ie - ib + G - 1) / G);
     for (int r = 0; r < passes; ++r) {
-      const int e = ib + r * 8 + l;
-      const int u = e < ie ? p.iadj[e] : -1;
-      const bool ready = u >= 0 && atomicSub(&p.deps[u], 1) == 1;
+      const int e = ib + r * G + l;
+      const int u = r == 0 ? u0 : (e < ie ? p.iadj[e] : -1);
+      const bool ready = r == 0 ? ready0 : u >= 0 && atomicSub(&p.deps[u], 1) == 1;
       const int slot = warp_append(&p.ctr->tail, ready);
       if (ready) {
         p.order[slot] = u;
@@ -799,21 +810,27 @@ sfxt_persistent_kernel(SfxtParams p) {
       const int c = per <= 4 ? 4 : per >= 32 ? 32 : (per + 3) & ~3;
       for (int i0 = beg + c * gwarp; i0 < end; i0 += c * nwarps) {
         const int i = i0 + lane;
-        int v = -1;
-        bool shortrow = false;
+        int v = -1, len = 0;
         if (lane < c && i < end) {
           v = __ldcg(p.order + i);
           if (!(full || rebuilt(p, v, lvl))) v = -1;
-          else shortrow = p.adjp[v + 1] - p.adjp[v] <= kGroupRow;
+          else len = p.adjp[v + 1] - p.adjp[v];
         }
-        const unsigned sm = __ballot_sync(0xffffffffu, v >= 0 && shortrow);
-        const unsigned lg = __ballot_sync(0xffffffffu, v >= 0 && !shortrow);
-        const int ns = __popc(sm);
-        for (int t = 0; t < ns; t += 4) {
+        const unsigned m8 = __ballot_sync(0xffffffffu, v >= 0 && len <= 8);
+        const unsigned m16 = __ballot_sync(0xffffffffu, v >= 0 && len > 8 && len <= 16);
+        const unsigned lg = __ballot_sync(0xffffffffu, v >= 0 && len > 16);
+        const int n8 = __popc(m8), n16 = __popc(m16);
+        for (int t = 0; t < n8; t += 4) {
           const int k = t + (lane >> 3);
-          const int from = k < ns ? kth_set_bit(sm, k) : 0;
+          const int from = k < n8 ? kth_set_bit(m8, k) : 0;
           const int vg = __shfl_sync(0xffffffffu, v, from);
-          build_group8(p, k < ns ? vg : -1, lvl, full && !kBvss);
+          build_group<8>(p, k < n8 ? vg : -1, lvl, full && !kBvss);
+        }
+        for (int t = 0; t < n16; t += 2) {
+          const int k = t + (lane >> 4);
+          const int from = k < n16 ? kth_set_bit(m16, k) : 0;
+          const int vg = __shfl_sync(0xffffffffu, v, from);
+          build_group<16>(p, k < n16 ? vg : -1, lvl, full && !kBvss);
         }
         for (unsigned b = lg; b; b &= b - 1) {
           const int vb = __shfl_sync(0xffffffffu, v, __ffs(b) - 1);

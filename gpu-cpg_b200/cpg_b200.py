@@ -654,17 +654,20 @@ class Server:
     def __exit__(self, *a):
         self.close()
 
+    def add_graph(self, n, adjp, adj, w) -> int:
+        adjp = np.ascontiguousarray(adjp, np.int32)
+        adj = np.ascontiguousarray(adj, np.int32)
+        w = np.ascontiguousarray(w, np.float32)
+        gid = C.c_int32()
+        self._check(lib.cpg_server_add_graph(self._s, int(n), int(adj.size), _ptr(adjp), _ptr(adj),
+                                             _ptr(w), C.byref(gid)), "add_graph")
+        return gid.value
+
     def add_dag(self, dag: "Dag") -> int:
         order = np.argsort(dag.src, kind="stable")
         adjp = np.zeros(dag.n + 1, np.int64)
         np.add.at(adjp, dag.src + 1, 1)
-        adjp = np.cumsum(adjp).astype(np.int32)
-        adj = np.ascontiguousarray(dag.dst[order], np.int32)
-        w = np.ascontiguousarray(dag.w[order], np.float32)
-        gid = C.c_int32()
-        self._check(lib.cpg_server_add_graph(self._s, int(dag.n), int(adj.size), _ptr(adjp), _ptr(adj),
-                                             _ptr(w), C.byref(gid)), "add_graph")
-        return gid.value
+        return self.add_graph(dag.n, np.cumsum(adjp).astype(np.int32), dag.dst[order], dag.w[order])
 
     def start(self):
         self._check(lib.cpg_server_start(self._s), "start")

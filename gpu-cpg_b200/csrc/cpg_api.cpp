@@ -61,6 +61,12 @@ struct cpg_handle {
   std::vector<int32_t> graph_voff;  // first vertex of each graph
   std::vector<int32_t> graph_from;  // per graph: lowest changed level (INT32_MAX: clean)
   DevMem d_vgraph, d_graph_from, d_upd, d_queue, d_dl, d_long;
+  // side-by-side graphs relabelled in level order by cpg_batch_commit: the
+  // caller's id of each vertex (device) and the new position of each of the
+  // caller's edges (host, for delay updates); empty otherwise
+  bool relabeled = false;
+  std::vector<int32_t> emap;
+  DevMem d_orig_id;
   // BVSS form of the fan-out CSR, for the pull Kahn step
   bool use_bvss = false;
   double bvss_bps = 0;  // set bits per slice (sampled, or exact once built)
@@ -265,6 +271,8 @@ Status upload_graph(cpg_handle* h, int32_t n, int32_t m, const int32_t* adjp,
   CK(cudaSetDevice(h->device), "cudaSetDevice");
   h->has_graph = false;
   h->multi_graph = false;  // cpg_batch_commit sets it after the upload
+  h->relabeled = false;    // so does it this
+  h->emap.clear();
   h->graph_voff.clear();
   h->graph_from.clear();
   const size_t nn = static_cast<size_t>(n), mm = static_cast<size_t>(m);
@@ -439,6 +447,7 @@ SfxtParams sfxt_params(cpg_handle* h, int32_t start_level) {
   p.heap_warps = std::min(std::max(h->opts.sfxt_heap_warps, 0), 16);
   p.early_push = h->opts.sfxt_late_push != 1 && p.heap_warps == 0;
   p.dl = P<unsigned long long>(h->d_dl);
+  p.orig_id = h->relabeled ? P<int32_t>(h->d_orig_id) : nullptr;
   if (start_level > 0) {
     // a dataflow build allocates heap nodes out of level order, so rebuilt
     // levels take fresh nodes; a pool overflow falls back to a full build
@@ -1131,7 +1140,7 @@ cpg_status cpg_destroy(cpg_handle* h) {
                    &h->d_bv_ptr, &h->d_bv_masks, &h->d_bv_rows, &h->d_bv_cnt,
                    &h->d_bv_deps, &h->d_fbits, &h->d_iact, &h->d_act_list,
                    &h->d_vgraph, &h->d_graph_from, &h->d_upd, &h->d_queue, &h->d_dl,
-                   &h->d_long};
+                   &h->d_long, &h->d_orig_id};
   for (DevMem* b : all) release(*b);
   for (auto& e : h->ev)
     if (e) cudaEventDestroy(e);
@@ -1234,6 +1243,17 @@ cpg_status cpg_update_delays(cpg_handle* h, int64_t count, const int32_t* eids,
   if (count == 0) return CPG_OK;
   if (!eids || !w) return fail(h, CPG_ERR_INVALID, "null delay buffer");
   CK(cudaSetDevice(h->device), "cudaSetDevice");
+  // a relabelled graph stores the caller's edges at new positions
+  std::vector<int32_t> mapped;
+  if (!h->emap.empty()) {
+    mapped.resize(static_cast<size_t>(count));
+    for (int64_t i = 0; i < count; ++i) {
+      const int32_t e = eids[i];
+      if (e < 0 || e >= h->g.m) return fail(h, CPG_ERR_INVALID, "edge id out of range");
+      mapped[i] = h->emap[e];
+    }
+    eids = mapped.data();
+  }
   int32_t lowest = INT32_MAX;
   const bool have_levels = h->sfxt_valid || h->dirty_level > 0;
   if (have_levels) {
@@ -1517,6 +1537,8 @@ struct cpg_batch {
   std::vector<int32_t> voff{0};     // first vertex of each graph
   bool committed = false;
   std::vector<int32_t> src_beg, src_end;  // per graph: its sources in d_srcs
+  // the committed graph, relabelled in level order (what the device holds)
+  std::vector<int32_t> padjp, padj;
   // queries
   std::vector<EngineQuery> qs;
   unsigned long long k_total = 0;
@@ -1531,6 +1553,90 @@ struct cpg_batch {
 };
 
 namespace {
+
+// Side-by-side graphs in level order.  Within each graph's id range the
+// vertices are renumbered by (suffix-tree level, caller id): sinks are level
+// 0, any other vertex one more than its highest head.  One level of the
+// side-by-side graph is then one contiguous block per graph, so a build step
+// reads and writes per-vertex words packed together instead of one DRAM burst
+// per 4-byte word.  Rows keep their edge order.  A vertex on a cycle gets no
+// level and goes last; the device build then reports the cycle.
+struct LevelOrder {
+  std::vector<int32_t> orig;        // new id -> caller id
+  std::vector<int32_t> adjp, adj;   // the relabelled CSR
+  std::vector<float> w;
+  std::vector<int32_t> emap;        // caller edge position -> new edge position
+};
+
+void relabel_by_level(const std::vector<int32_t>& voff, const std::vector<int32_t>& adjp,
+                      const std::vector<int32_t>& adj, const std::vector<float>& w,
+                      LevelOrder& lo) {
+  const int32_t n = voff.back();
+  const size_t m = adj.size();
+  const int ng = static_cast<int>(voff.size()) - 1;
+  std::vector<int32_t> perm(static_cast<size_t>(n));
+  lo.orig.assign(static_cast<size_t>(n), 0);
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int g = 0; g < ng; ++g) {
+    const int32_t v0 = voff[g], nv = voff[g + 1] - voff[g];
+    const int32_t e0 = adjp[v0], e1 = adjp[v0 + nv];
+    // fan-in lists of the graph
+    std::vector<int32_t> ip(static_cast<size_t>(nv) + 1, 0), iadj(static_cast<size_t>(e1 - e0));
+    for (int32_t e = e0; e < e1; ++e) ++ip[adj[e] - v0 + 1];
+    for (int32_t i = 0; i < nv; ++i) ip[i + 1] += ip[i];
+    std::vector<int32_t> cur(ip.begin(), ip.end() - 1);
+    for (int32_t i = 0; i < nv; ++i)
+      for (int32_t e = adjp[v0 + i]; e < adjp[v0 + i + 1]; ++e) iadj[cur[adj[e] - v0]++] = i;
+    // Kahn from the sinks: a vertex's level is final when its last head is done
+    std::vector<int32_t> lvl(static_cast<size_t>(nv), -1), left(static_cast<size_t>(nv)), q;
+    q.reserve(static_cast<size_t>(nv));
+    for (int32_t i = 0; i < nv; ++i) {
+      left[i] = adjp[v0 + i + 1] - adjp[v0 + i];
+      if (left[i] == 0) {
+        lvl[i] = 0;
+        q.push_back(i);
+      }
+    }
+    int32_t top = 0;
+    for (size_t x = 0; x < q.size(); ++x) {
+      const int32_t u = q[x];
+      top = std::max(top, lvl[u]);
+      for (int32_t j = ip[u]; j < ip[u + 1]; ++j) {
+        const int32_t t = iadj[j];
+        lvl[t] = std::max(lvl[t], lvl[u] + 1);
+        if (--left[t] == 0) q.push_back(t);
+      }
+    }
+    // stable counting sort by level (caller-id order within a level; no level last)
+    std::vector<int32_t> at(static_cast<size_t>(top) + 3, 0);
+    auto bucket = [&](int32_t i) { return lvl[i] >= 0 && left[i] == 0 ? lvl[i] : top + 1; };
+    for (int32_t i = 0; i < nv; ++i) ++at[bucket(i) + 1];
+    for (int32_t b = 0; b <= top + 1; ++b) at[b + 1] += at[b];
+    for (int32_t i = 0; i < nv; ++i) {
+      const int32_t pos = at[bucket(i)]++;
+      perm[v0 + i] = v0 + pos;
+      lo.orig[v0 + pos] = v0 + i;
+    }
+  }
+  lo.adjp.assign(static_cast<size_t>(n) + 1, 0);
+  for (int32_t v = 0; v < n; ++v) {
+    const int32_t o = lo.orig[v];
+    lo.adjp[v + 1] = lo.adjp[v] + (adjp[o + 1] - adjp[o]);
+  }
+  lo.adj.resize(m);
+  lo.w.resize(m);
+  lo.emap.resize(m);
+#pragma omp parallel for schedule(static)
+  for (int32_t v = 0; v < n; ++v) {
+    const int32_t o = lo.orig[v];
+    for (int32_t j = 0; j < adjp[o + 1] - adjp[o]; ++j) {
+      const int32_t e = adjp[o] + j, f = lo.adjp[v] + j;
+      lo.adj[f] = perm[adj[e]];
+      lo.w[f] = w[e];
+      lo.emap[e] = f;
+    }
+  }
+}
 
 void batch_drop_graph(cpg_batch* b) {
   if (b->exec) cudaGraphExecDestroy(b->exec);
@@ -1699,9 +1805,19 @@ cpg_status cpg_batch_commit(cpg_batch* b) {
   if (!b) return CPG_ERR_INVALID;
   cpg_handle* h = b->h;
   const int32_t n = b->voff.back();
-  Status st = upload_graph(h, n, static_cast<int32_t>(b->adj.size()), b->adjp.data(),
-                           b->adj.data(), b->w.data());
+  // each graph relabelled in level order (invisible to the caller: the batch
+  // returns costs, the successor tie-break and the root order use caller ids,
+  // delay updates name the caller's edges)
+  LevelOrder lo;
+  relabel_by_level(b->voff, b->adjp, b->adj, b->w, lo);
+  Status st = upload_graph(h, n, static_cast<int32_t>(lo.adj.size()), lo.adjp.data(),
+                           lo.adj.data(), lo.w.data());
   if (st != CPG_OK) return st;
+  CK(ensure(h->d_orig_id, std::max<size_t>(lo.orig.size(), 1) * 4), "alloc caller ids");
+  if (n) CK(cudaMemcpy(h->d_orig_id.p, lo.orig.data(), lo.orig.size() * 4, cudaMemcpyHostToDevice),
+            "H2D caller ids");
+  h->relabeled = true;
+  h->emap.swap(lo.emap);
   // sources of each graph: a contiguous run of the id-sorted source list
   std::vector<int32_t> srcs(h->n_srcs);
   if (h->n_srcs)
@@ -1714,7 +1830,14 @@ cpg_status cpg_batch_commit(cpg_batch* b) {
         std::lower_bound(srcs.begin(), srcs.end(), b->voff[g]) - srcs.begin());
     b->src_end[g] = static_cast<int32_t>(
         std::lower_bound(srcs.begin(), srcs.end(), b->voff[g + 1]) - srcs.begin());
+    // within a graph, roots are seeded in caller-id order (gpucpg.cu:531-533)
+    std::sort(srcs.begin() + b->src_beg[g], srcs.begin() + b->src_end[g],
+              [&](int32_t a, int32_t c) { return lo.orig[a] < lo.orig[c]; });
   }
+  if (h->n_srcs > 1)
+    CK(cudaMemcpy(h->d_srcs.p, srcs.data(), srcs.size() * 4, cudaMemcpyHostToDevice), "H2D sources");
+  b->padjp.swap(lo.adjp);
+  b->padj.swap(lo.adj);
   // per-vertex graph ids for incremental rebuilds of single graphs
   h->multi_graph = true;
   h->graph_voff = b->voff;
@@ -1827,11 +1950,11 @@ cpg_status cpg_batch_autotune(cpg_batch* b) {
   // The BVSS frontier is a candidate only when its slices are dense enough
   // to have a chance; it is built once, from the host CSR, when it is.
   const bool try_bvss = h->use_bvss || h->bvss_bps >= 1.5 ||
-                        bvss_density_sample(b->voff.back(), b->adjp.data(), b->adj.data(), 4096) >= 1.5;
+                        bvss_density_sample(b->voff.back(), b->padjp.data(), b->padj.data(), 4096) >= 1.5;
   if (try_bvss && !h->use_bvss) {
     const int32_t keep = h->opts.frontier;
     h->opts.frontier = CPG_FRONTIER_BVSS;
-    Status st = setup_bvss(h, b->voff.back(), b->adjp.data(), b->adj.data());
+    Status st = setup_bvss(h, b->voff.back(), b->padjp.data(), b->padj.data());
     h->opts.frontier = keep;
     if (st != CPG_OK) return static_cast<cpg_status>(st);
     h->use_bvss = false;  // built; each candidate below turns it on or off

@@ -170,6 +170,10 @@ struct SfxtParams {
   int32_t heap_warps;      // dataflow: warps per CTA that only insert heaps (0: none)
   int32_t early_push;      // dataflow: push tails before the build, poll dl[]
   unsigned long long* dl;  // dataflow: published (level << 32 | dist) per vertex
+  // Side-by-side graphs relabelled in level order (batched and served forms):
+  // the caller's id of each vertex, for the successor tie-break; null when
+  // the ids are the caller's
+  const int32_t* orig_id;
   // BVSS pull for the Kahn step of a full build; used when bvss != 0
   int32_t bvss;
   const int32_t* bv_ptr;       // VSS range of each interval of 8 vertices

@@ -194,6 +194,27 @@ __device__ __forceinline__ int cand_dist(int dh, float w) {
   return static_cast<int>(static_cast<unsigned>(dh) + static_cast<unsigned>(fixed_delay(w)));
 }
 
+// Successor tie-break on relabelled graphs (p.orig_id set): among the heads
+// that tie for the least distance, the one with the largest caller id, as
+// update_successors_bu picks it (gpucpg.cu:2606-2628).  The word orders by
+// caller id and carries the head's own id; 0 is "none".  Ties are rare, so
+// the callers read caller ids only when more than one head ties.
+__device__ __forceinline__ unsigned long long succ_word(const SfxtParams& p, int head) {
+  return (static_cast<unsigned long long>(static_cast<unsigned>(__ldg(p.orig_id + head)) + 1u)
+          << 32) |
+         static_cast<unsigned>(head);
+}
+
+template <int G>
+__device__ __forceinline__ unsigned long long group_max_u64(unsigned long long x) {
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) {
+    const unsigned long long y = __shfl_xor_sync(0xffffffffu, x, o, G);
+    x = y > x ? y : x;
+  }
+  return x;
+}
+
 // kLevel (dataflow build): the level is not known in advance; it is one
 // more than the heads' highest level (0 for a sink), read with their
 // distances, and written to level_of[v].  Returns the level.
@@ -237,10 +258,25 @@ __device__ int build_vertex(const SfxtParams& p, int v, int lvl, bool do_kahn) {
       for (int c = 0; c < kRegChunks; ++c)
         if (ed[c].head >= 0) best = min(best, cand_dist(dh[c], ed[c].w));
       best = warp_min_i(best);
+      int nt = 0;  // this lane's tied heads
 #pragma unroll
       for (int c = 0; c < kRegChunks; ++c)
-        if (ed[c].head >= 0 && cand_dist(dh[c], ed[c].w) == best) s = max(s, ed[c].head);
-      s = warp_max_i(s);
+        if (ed[c].head >= 0 && cand_dist(dh[c], ed[c].w) == best) {
+          s = max(s, ed[c].head);
+          ++nt;
+        }
+      if (p.orig_id && __reduce_add_sync(0xffffffffu, nt) > 1) {
+        unsigned long long k = 0;
+#pragma unroll
+        for (int c = 0; c < kRegChunks; ++c)
+          if (ed[c].head >= 0 && cand_dist(dh[c], ed[c].w) == best) {
+            const unsigned long long x = succ_word(p, ed[c].head);
+            k = x > k ? x : k;
+          }
+        s = static_cast<int>(group_max_u64<32>(k) & 0xffffffffu);
+      } else {
+        s = warp_max_i(s);
+      }
     }
     // deviations: fan-out edges whose head is not the successor and has a
     // finite distance, compacted in edge order into v's own fan-out slots
@@ -300,11 +336,27 @@ __device__ int build_vertex(const SfxtParams& p, int v, int lvl, bool do_kahn) {
         best = min(best, cand_dist(__ldcg(p.dist + ed.head), ed.w));
       }
       best = warp_min_i(best);
+      int nt = 0;
       for (int e = rb + lane; e < re; e += 32) {
         const DevEdge ed = p.edges[e];
-        if (cand_dist(__ldcg(p.dist + ed.head), ed.w) == best) s = max(s, ed.head);
+        if (cand_dist(__ldcg(p.dist + ed.head), ed.w) == best) {
+          s = max(s, ed.head);
+          ++nt;
+        }
       }
-      s = warp_max_i(s);
+      if (p.orig_id && __reduce_add_sync(0xffffffffu, nt) > 1) {
+        unsigned long long k = 0;
+        for (int e = rb + lane; e < re; e += 32) {
+          const DevEdge ed = p.edges[e];
+          if (cand_dist(__ldcg(p.dist + ed.head), ed.w) == best) {
+            const unsigned long long x = succ_word(p, ed.head);
+            k = x > k ? x : k;
+          }
+        }
+        s = static_cast<int>(group_max_u64<32>(k) & 0xffffffffu);
+      } else {
+        s = warp_max_i(s);
+      }
     }
     BestDev bd = best_none();
     for (int base = rb; base < re; base += 32) {
@@ -433,7 +485,15 @@ __device__ void build_group(const SfxtParams& p, int v, int lvl, bool do_kahn) {
   const bool ready0 = u0 >= 0 && atomicSub(&p.deps[u0], 1) == 1;
   int best = group_min_i<G>(has ? cand_dist(dh, ed.w) : INT_MAX);
   if (lvl == 0) best = 0;  // sinks start at distance 0
-  const int s = group_max_i<G>(has && lvl > 0 && cand_dist(dh, ed.w) == best ? ed.head : -1);
+  const bool tie = has && lvl > 0 && cand_dist(dh, ed.w) == best;
+  int s = group_max_i<G>(tie ? ed.head : -1);
+  if (p.orig_id) {
+    const int gt = __popc((__ballot_sync(0xffffffffu, tie) >> (g * G)) & ((1u << G) - 1u));
+    if (__any_sync(0xffffffffu, gt > 1)) {
+      const unsigned long long k = group_max_u64<G>(tie && gt > 1 ? succ_word(p, ed.head) : 0ull);
+      if (gt > 1) s = static_cast<int>(k & 0xffffffffu);
+    }
+  }
   // deviations: every edge but the successor's, sorted by (key, position)
   const bool valid = has && ed.head != s && dh != INT_MAX;
   DevSidetrack rec;
@@ -1007,10 +1067,25 @@ __device__ int build_vertex_polled(const SfxtParams& p, int v) {
       for (int c = 0; c < kRegChunks; ++c)
         if (ed[c].head >= 0) best = min(best, cand_dist(dh[c], ed[c].w));
       best = warp_min_i(best);
+      int nt = 0;  // this lane's tied heads
 #pragma unroll
       for (int c = 0; c < kRegChunks; ++c)
-        if (ed[c].head >= 0 && cand_dist(dh[c], ed[c].w) == best) s = max(s, ed[c].head);
-      s = warp_max_i(s);
+        if (ed[c].head >= 0 && cand_dist(dh[c], ed[c].w) == best) {
+          s = max(s, ed[c].head);
+          ++nt;
+        }
+      if (p.orig_id && __reduce_add_sync(0xffffffffu, nt) > 1) {
+        unsigned long long k = 0;
+#pragma unroll
+        for (int c = 0; c < kRegChunks; ++c)
+          if (ed[c].head >= 0 && cand_dist(dh[c], ed[c].w) == best) {
+            const unsigned long long x = succ_word(p, ed[c].head);
+            k = x > k ? x : k;
+          }
+        s = static_cast<int>(group_max_u64<32>(k) & 0xffffffffu);
+      } else {
+        s = warp_max_i(s);
+      }
     }
     if (re - rb <= 32) {
       const bool valid = ed[0].head >= 0 && ed[0].head != s && dh[0] != INT_MAX;
@@ -1080,11 +1155,27 @@ __device__ int build_vertex_polled(const SfxtParams& p, int v) {
       best = min(best, cand_dist(dist_of(ed.head), ed.w));
     }
     best = warp_min_i(best);
+    int nt = 0;
     for (int e = rb + lane; e < re; e += 32) {
       const DevEdge ed = p.edges[e];
-      if (cand_dist(dist_of(ed.head), ed.w) == best) s = max(s, ed.head);
+      if (cand_dist(dist_of(ed.head), ed.w) == best) {
+        s = max(s, ed.head);
+        ++nt;
+      }
     }
-    s = warp_max_i(s);
+    if (p.orig_id && __reduce_add_sync(0xffffffffu, nt) > 1) {
+      unsigned long long k = 0;
+      for (int e = rb + lane; e < re; e += 32) {
+        const DevEdge ed = p.edges[e];
+        if (cand_dist(dist_of(ed.head), ed.w) == best) {
+          const unsigned long long x = succ_word(p, ed.head);
+          k = x > k ? x : k;
+        }
+      }
+      s = static_cast<int>(group_max_u64<32>(k) & 0xffffffffu);
+    } else {
+      s = warp_max_i(s);
+    }
     BestDev bd = best_none();
     for (int base = rb; base < re; base += 32) {
       const int e = base + lane;

@@ -68,3 +68,71 @@ def test_batch_replay_without_rebuild_and_autotune():
         tuned = [b.costs(q) for q in range(6)]
     for a, c, t in zip(first, again, tuned):
         assert np.array_equal(a, c) and np.array_equal(a, t)
+
+
+@pytest.mark.parametrize("roots", [cpg_b200.ROOTS_REFERENCE, cpg_b200.ROOTS_ALL])
+def test_batch_of_reference_fixtures_matches_alone(roots):
+    """A batch renumbers each graph's vertices in level order.  On the
+    reference's fixtures -- unit delays, so many heads tie for a vertex's
+    distance and the successor tie-break decides, and many sources, so the
+    root order decides -- every query still returns exactly what its graph
+    returns alone, and a delay update names the caller's edge ids."""
+    import cases
+    names = ["tv80_unit_wgts", "simple", "dac21_paper_example", "small_int_s13"]
+    graphs = [cases.load_case(nm) for nm in names]
+    ks = [10_000, 1_000, 1_000, 5_000]
+    rng = np.random.default_rng(5)
+    upd = []  # (input edge indices, new delays) per graph
+    for n, src, dst, w in graphs:
+        e = rng.choice(src.size, size=max(1, src.size // 10), replace=False).astype(np.int64)
+        upd.append((e, np.round(rng.uniform(1.0, 9.0, size=e.size)).astype(np.float32)))
+
+    def alone(i):
+        n, src, dst, w = graphs[i]
+        with cpg_b200.CpGen(division=cpg_b200.DIV_IEEE, root_seeding=roots) as g:
+            g.load_edges(n, src, dst, w)
+            g.report_paths(ks[i])
+            return g.get_slacks(ks[i])
+
+    def csr(n, src, dst, w):
+        order = np.argsort(src, kind="stable")
+        adjp = np.zeros(n + 1, np.int64)
+        np.add.at(adjp, src + 1, 1)
+        return np.cumsum(adjp).astype(np.int32), dst[order], w[order]
+
+    with cpg_b200.Batch(division=cpg_b200.DIV_IEEE, root_seeding=roots) as b:
+        for n, src, dst, w in graphs:
+            b.add_graph(n, *csr(n, src, dst, w))
+        b.commit()
+        b.set_queries(list(range(len(graphs))), ks)
+        b.run(True)
+        for i in range(len(graphs)):
+            want = alone(i)
+            assert np.array_equal(b.costs(i).view(np.uint32), want.view(np.uint32)), names[i]
+    # the served form holds the batch: re-asks with delay updates by the
+    # caller's edge ids (positions in the graph's own CSR)
+    with cpg_b200.Server(division=cpg_b200.DIV_IEEE, root_seeding=roots) as s:
+        for n, src, dst, w in graphs:
+            s.add_graph(n, *csr(n, src, dst, w))
+        s.start()
+        for i in range(len(graphs)):
+            n, src, dst, w = graphs[i]
+            # the caller's edge ids are positions in its CSR (rows in file order)
+            order = np.argsort(src, kind="stable")
+            pos = np.empty(src.size, np.int64)
+            pos[order] = np.arange(src.size)
+            e, nw = upd[i]
+            got, _ = s.wait(s.submit(i, ks[i], pos[e].astype(np.int32), nw))
+            want = alone_csr_update(graphs[i], pos[e].astype(np.int32), nw, ks[i], roots)
+            assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), names[i]
+
+
+def alone_csr_update(graph, eids, nw, k, roots):
+    """One graph alone, its CSR edges eids given delays nw."""
+    n, src, dst, w = graph
+    with cpg_b200.CpGen(division=cpg_b200.DIV_IEEE, root_seeding=roots) as g:
+        g.load_edges(n, src, dst, w)
+        g.report_paths(k)          # levels known: the update rebuilds incrementally
+        g.update_delays(eids, nw)
+        g.report_paths(k)
+        return g.get_slacks(k)

@@ -48,7 +48,7 @@ class Options(C.Structure):
         ("host_stepped", C.c_int32), ("bvss_tiles", C.c_int32),
         ("bvss_min_bits", C.c_int32), ("bvss_min_slices", C.c_int32),
         ("sfxt_level_sync", C.c_int32), ("sfxt_heap_warps", C.c_int32),
-        ("sfxt_late_push", C.c_int32),
+        ("sfxt_late_push", C.c_int32), ("batch_caller_order", C.c_int32),
     ]
 
 
@@ -533,13 +533,15 @@ class Batch:
     sequence (see cpg_batch_* in include/cpg.h)."""
 
     def __init__(self, device: int = 0, stream: int | None = None,
-                 division: int = DIV_REFERENCE, root_seeding: int = ROOTS_REFERENCE):
+                 division: int = DIV_REFERENCE, root_seeding: int = ROOTS_REFERENCE,
+                 caller_order: bool = False):
         o = Options()
         lib.cpg_options_init(C.byref(o))
         o.device = device
         o.stream = stream
         o.division = division
         o.root_seeding = root_seeding
+        o.batch_caller_order = 1 if caller_order else 0
         self._b = C.c_void_p()
         st = lib.cpg_batch_create(C.byref(self._b), C.byref(o))
         if st != CPG_OK:

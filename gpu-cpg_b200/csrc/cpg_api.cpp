@@ -1809,14 +1809,22 @@ cpg_status cpg_batch_commit(cpg_batch* b) {
   // returns costs, the successor tie-break and the root order use caller ids,
   // delay updates name the caller's edges)
   LevelOrder lo;
-  relabel_by_level(b->voff, b->adjp, b->adj, b->w, lo);
+  if (h->opts.batch_caller_order == 1) {
+    lo.orig.resize(static_cast<size_t>(n));
+    for (int32_t v = 0; v < n; ++v) lo.orig[v] = v;
+    lo.adjp = b->adjp;
+    lo.adj = b->adj;
+    lo.w = b->w;
+  } else {
+    relabel_by_level(b->voff, b->adjp, b->adj, b->w, lo);
+  }
   Status st = upload_graph(h, n, static_cast<int32_t>(lo.adj.size()), lo.adjp.data(),
                            lo.adj.data(), lo.w.data());
   if (st != CPG_OK) return st;
   CK(ensure(h->d_orig_id, std::max<size_t>(lo.orig.size(), 1) * 4), "alloc caller ids");
   if (n) CK(cudaMemcpy(h->d_orig_id.p, lo.orig.data(), lo.orig.size() * 4, cudaMemcpyHostToDevice),
             "H2D caller ids");
-  h->relabeled = true;
+  h->relabeled = h->opts.batch_caller_order != 1;
   h->emap.swap(lo.emap);
   // sources of each graph: a contiguous run of the id-sorted source list
   std::vector<int32_t> srcs(h->n_srcs);
@@ -2052,6 +2060,10 @@ struct cpg_server {
   int64_t paths = 0, launches = 0, rebuilds = 0, retries = 0, pool_rebuilds = 0;
   double busy_ms = 0, sfxt_ms = 0, first_submit = -1, last_done = 0, max_step_ms = 0;
   int32_t max_batch_seen = 0;
+  // pinned staging of a launch's costs (grown geometrically, kept): one fast
+  // copy from the device, one copy into the results
+  float* pin_out = nullptr;
+  size_t pin_cap = 0;
 };
 
 namespace {
@@ -2088,15 +2100,29 @@ int server_launch(cpg_server* sv, const std::vector<ServerReq>& batch,
   cudaEventElapsedTime(&ms, h->ev[4], h->ev[5]);
   sv->busy_ms += ms;
   sv->launches += 1;
-  // all outputs in one copy, then split per query
+  // all outputs in one copy into the pinned staging, then split per query
   unsigned long long total = 0;
   for (const EngineQuery& q : qs) total = std::max(total, q.out_off + q.k_out);
-  std::vector<float> all(total);
-  if (total)
-    CK(cudaMemcpy(all.data(), h->d_out_cost.p, total * 4, cudaMemcpyDeviceToHost), "D2H costs");
+  if (total > sv->pin_cap) {
+    if (sv->pin_out) cudaFreeHost(sv->pin_out);
+    sv->pin_out = nullptr;
+    const size_t want = std::max<size_t>(total, 2 * sv->pin_cap);
+    if (cudaMallocHost(&sv->pin_out, want * 4) != cudaSuccess) {
+      sv->pin_out = nullptr;
+      sv->pin_cap = 0;
+      cudaGetLastError();
+      return fail(h, CPG_ERR_OOM, "pinned staging of the costs");
+    }
+    sv->pin_cap = want;
+  }
+  if (total) {
+    CK(cudaMemcpyAsync(sv->pin_out, h->d_out_cost.p, total * 4, cudaMemcpyDeviceToHost, s),
+       "D2H costs");
+    CK(cudaStreamSynchronize(s), "D2H costs");
+  }
   out.resize(qs.size());
   for (size_t i = 0; i < qs.size(); ++i)
-    out[i].assign(all.begin() + qs[i].out_off, all.begin() + qs[i].out_off + qs[i].k_out);
+    out[i].assign(sv->pin_out + qs[i].out_off, sv->pin_out + qs[i].out_off + qs[i].k_out);
   return CPG_OK;
 }
 
@@ -2227,6 +2253,7 @@ cpg_status cpg_server_stop(cpg_server* sv) {
 cpg_status cpg_server_destroy(cpg_server* sv) {
   if (!sv) return CPG_ERR_INVALID;
   cpg_server_stop(sv);
+  if (sv->pin_out) cudaFreeHost(sv->pin_out);
   if (sv->b) cpg_batch_destroy(sv->b);
   delete sv;
   return CPG_OK;

@@ -96,6 +96,9 @@ typedef struct {
   int32_t sfxt_late_push;   /* dataflow build: 1 = a vertex's tails are
                                decremented after it is built instead of when
                                it is taken (A/B checks) */
+  int32_t batch_caller_order; /* batched and served forms: 1 = keep the
+                               callers' vertex order instead of renumbering
+                               each graph in level order (A/B checks) */
 } cpg_options;
 
 typedef struct cpg_handle cpg_handle;

@@ -70,13 +70,15 @@ def test_batch_replay_without_rebuild_and_autotune():
         assert np.array_equal(a, c) and np.array_equal(a, t)
 
 
+@pytest.mark.parametrize("caller_order", [False, True])
 @pytest.mark.parametrize("roots", [cpg_b200.ROOTS_REFERENCE, cpg_b200.ROOTS_ALL])
-def test_batch_of_reference_fixtures_matches_alone(roots):
+def test_batch_of_reference_fixtures_matches_alone(roots, caller_order):
     """A batch renumbers each graph's vertices in level order.  On the
     reference's fixtures -- unit delays, so many heads tie for a vertex's
     distance and the successor tie-break decides, and many sources, so the
     root order decides -- every query still returns exactly what its graph
-    returns alone, and a delay update names the caller's edge ids."""
+    returns alone, and a delay update names the caller's edge ids.
+    caller_order keeps the callers' numbering (the A/B check)."""
     import cases
     names = ["tv80_unit_wgts", "simple", "dac21_paper_example", "small_int_s13"]
     graphs = [cases.load_case(nm) for nm in names]
@@ -100,7 +102,8 @@ def test_batch_of_reference_fixtures_matches_alone(roots):
         np.add.at(adjp, src + 1, 1)
         return np.cumsum(adjp).astype(np.int32), dst[order], w[order]
 
-    with cpg_b200.Batch(division=cpg_b200.DIV_IEEE, root_seeding=roots) as b:
+    with cpg_b200.Batch(division=cpg_b200.DIV_IEEE, root_seeding=roots,
+                        caller_order=caller_order) as b:
         for n, src, dst, w in graphs:
             b.add_graph(n, *csr(n, src, dst, w))
         b.commit()

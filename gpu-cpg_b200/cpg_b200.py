@@ -104,6 +104,7 @@ class ServerStats(C.Structure):
         ("sfxt_rebuilds", C.c_int64), ("busy_ms", C.c_double), ("max_batch_seen", C.c_int32),
         ("reserved", C.c_int32), ("sfxt_ms", C.c_double), ("retries", C.c_int64),
         ("pool_rebuilds", C.c_int64), ("max_step_ms", C.c_double),
+        ("max_update_ms", C.c_double), ("max_rebuild_ms", C.c_double), ("max_launch_ms", C.c_double),
     ]
 
 

@@ -2021,6 +2021,9 @@ double now_s() {
 
 // Predicted device bytes of one query of k paths: path store, frontier and
 // pending piles, sort buffers and outputs at the engine's initial sizing.
+// Paths the server's piles are sized for at start (see cpg_server_start).
+constexpr unsigned long long kServerPresizePaths = 4ull << 20;
+
 int64_t predicted_bytes(int64_t k) {
   const int64_t kk = std::max<int64_t>(k, 1);
   return 4 * kk * 24 + 4 * kk * 16 + 16 * kk * 16 + 6 * kk * 4 + kk * 28 + (64 << 10);
@@ -2059,6 +2062,7 @@ struct cpg_server {
   std::vector<double> lat_ms;
   int64_t paths = 0, launches = 0, rebuilds = 0, retries = 0, pool_rebuilds = 0;
   double busy_ms = 0, sfxt_ms = 0, first_submit = -1, last_done = 0, max_step_ms = 0;
+  double max_update_ms = 0, max_rebuild_ms = 0, max_launch_ms = 0;
   int32_t max_batch_seen = 0;
   // pinned staging of a launch's costs (grown geometrically, kept): one fast
   // copy from the device, one copy into the results
@@ -2170,11 +2174,13 @@ void server_loop(cpg_server* sv) {
       st = cpg_update_delays(h, static_cast<int64_t>(r.eids.size()), r.eids.data(), r.w.data());
       updated = true;
     }
+    const double t_upd = now_s();
     if (st == CPG_OK && updated) {
       st = ensure_sfxt(h);  // incremental: levels at or above the lowest change
       sv->rebuilds += 1;
       sv->sfxt_ms += h->stats.sfxt_ms;
     }
+    const double t_sfxt = now_s();
     std::vector<std::vector<float>> out;
     for (int attempt = 0; st == CPG_OK && attempt < 10; ++attempt) {
       const int r = server_launch(sv, batch, out);
@@ -2191,6 +2197,9 @@ void server_loop(cpg_server* sv) {
       std::lock_guard<std::mutex> lk(sv->mu);
       sv->max_batch_seen = std::max<int32_t>(sv->max_batch_seen, static_cast<int32_t>(batch.size()));
       sv->max_step_ms = std::max(sv->max_step_ms, (t - t_step) * 1e3);
+      sv->max_update_ms = std::max(sv->max_update_ms, (t_upd - t_step) * 1e3);
+      sv->max_rebuild_ms = std::max(sv->max_rebuild_ms, (t_sfxt - t_upd) * 1e3);
+      sv->max_launch_ms = std::max(sv->max_launch_ms, (t - t_sfxt) * 1e3);
       sv->pool_rebuilds += h->pool_rebuilds - pool_before;
       for (size_t i = 0; i < batch.size(); ++i) {
         ServerResult& res = sv->results[batch[i].ticket];
@@ -2281,6 +2290,21 @@ cpg_status cpg_server_start(cpg_server* sv) {
   if (st != CPG_OK) return st;
   st = cpg_levelize(sv->b->h);
   if (st != CPG_OK) return st;
+  // The engine's path and item piles, sized once for a launch answering
+  // kServerPresizePaths paths (about 1.7 GB at 4 M; less under a smaller
+  // admission budget).  Growing a pile mid-stream reallocates it and reruns
+  // the launch, and those steps set the tail latency.
+  {
+    cpg_handle* h = sv->b->h;
+    unsigned long long pre = kServerPresizePaths;
+    if (sv->so.hbm_budget_bytes > 0)
+      pre = std::min<unsigned long long>(
+          pre, static_cast<unsigned long long>(sv->so.hbm_budget_bytes) / (8 * 512));
+    const unsigned long long ns = static_cast<unsigned long long>(h->n_srcs);
+    h->cap_paths = std::max(h->cap_paths, 4 * pre + ns);
+    h->cap_front = std::max(h->cap_front, 2 * pre);
+    h->cap_pend = std::max(h->cap_pend, 8 * pre + ns);
+  }
   sv->stopping = false;
   sv->running = true;
   sv->th = std::thread(server_loop, sv);
@@ -2372,6 +2396,9 @@ cpg_status cpg_server_get_stats(const cpg_server* svc, cpg_server_stats* out) {
   out->retries = sv->retries;
   out->pool_rebuilds = sv->pool_rebuilds;
   out->max_step_ms = sv->max_step_ms;
+  out->max_update_ms = sv->max_update_ms;
+  out->max_rebuild_ms = sv->max_rebuild_ms;
+  out->max_launch_ms = sv->max_launch_ms;
   return CPG_OK;
 }
 

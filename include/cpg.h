@@ -315,6 +315,10 @@ typedef struct {
   int64_t retries;            /* launches rerun after a query buffer grew */
   int64_t pool_rebuilds;      /* full suffix-tree rebuilds after the heap pool filled */
   double max_step_ms;         /* longest loop step: updates, rebuild, launch, results */
+  /* the longest of each part of a step, for diagnosis */
+  double max_update_ms;       /* applying the admitted delay updates */
+  double max_rebuild_ms;      /* the suffix-tree rebuild (incremental, or full after the pool filled) */
+  double max_launch_ms;       /* the engine launch with its reruns after a buffer grew */
 } cpg_server_stats;
 
 void cpg_server_options_init(cpg_server_options* o);

@@ -105,6 +105,7 @@ class ServerStats(C.Structure):
         ("reserved", C.c_int32), ("sfxt_ms", C.c_double), ("retries", C.c_int64),
         ("pool_rebuilds", C.c_int64), ("max_step_ms", C.c_double),
         ("max_update_ms", C.c_double), ("max_rebuild_ms", C.c_double), ("max_launch_ms", C.c_double),
+        ("max_engine_ms", C.c_double),
     ]
 
 

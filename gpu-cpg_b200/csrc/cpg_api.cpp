@@ -2062,7 +2062,7 @@ struct cpg_server {
   std::vector<double> lat_ms;
   int64_t paths = 0, launches = 0, rebuilds = 0, retries = 0, pool_rebuilds = 0;
   double busy_ms = 0, sfxt_ms = 0, first_submit = -1, last_done = 0, max_step_ms = 0;
-  double max_update_ms = 0, max_rebuild_ms = 0, max_launch_ms = 0;
+  double max_update_ms = 0, max_rebuild_ms = 0, max_launch_ms = 0, max_engine_ms = 0;
   int32_t max_batch_seen = 0;
   // pinned staging of a launch's costs (grown geometrically, kept): one fast
   // copy from the device, one copy into the results
@@ -2103,6 +2103,7 @@ int server_launch(cpg_server* sv, const std::vector<ServerReq>& batch,
   float ms = 0.f;
   cudaEventElapsedTime(&ms, h->ev[4], h->ev[5]);
   sv->busy_ms += ms;
+  sv->max_engine_ms = std::max(sv->max_engine_ms, static_cast<double>(ms));
   sv->launches += 1;
   // all outputs in one copy into the pinned staging, then split per query
   unsigned long long total = 0;
@@ -2292,8 +2293,10 @@ cpg_status cpg_server_start(cpg_server* sv) {
   if (st != CPG_OK) return st;
   // The engine's path and item piles, sized once for a launch answering
   // kServerPresizePaths paths (about 1.7 GB at 4 M; less under a smaller
-  // admission budget).  Growing a pile mid-stream reallocates it and reruns
-  // the launch, and those steps set the tail latency.
+  // admission budget), and allocated here with the tables of max_batch
+  // queries and the pinned cost staging.  Growing a pile mid-stream
+  // reallocates it and reruns the launch, and an allocation in the loop
+  // stalls every query queued behind it: those steps set the tail latency.
   {
     cpg_handle* h = sv->b->h;
     unsigned long long pre = kServerPresizePaths;
@@ -2304,6 +2307,17 @@ cpg_status cpg_server_start(cpg_server* sv) {
     h->cap_paths = std::max(h->cap_paths, 4 * pre + ns);
     h->cap_front = std::max(h->cap_front, 2 * pre);
     h->cap_pend = std::max(h->cap_pend, 8 * pre + ns);
+    const std::vector<EngineQuery> none(static_cast<size_t>(std::max(1, sv->so.max_batch)));
+    const Status ws = engine_prepare(h, none, pre);
+    if (ws != CPG_OK) return static_cast<cpg_status>(ws);
+    if (!sv->pin_out) {
+      if (cudaMallocHost(&sv->pin_out, pre * 4) == cudaSuccess) {
+        sv->pin_cap = pre;
+      } else {
+        sv->pin_out = nullptr;  // the loop allocates it when first needed
+        cudaGetLastError();
+      }
+    }
   }
   sv->stopping = false;
   sv->running = true;
@@ -2399,6 +2413,7 @@ cpg_status cpg_server_get_stats(const cpg_server* svc, cpg_server_stats* out) {
   out->max_update_ms = sv->max_update_ms;
   out->max_rebuild_ms = sv->max_rebuild_ms;
   out->max_launch_ms = sv->max_launch_ms;
+  out->max_engine_ms = sv->max_engine_ms;
   return CPG_OK;
 }
 

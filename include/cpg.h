@@ -319,6 +319,7 @@ typedef struct {
   double max_update_ms;       /* applying the admitted delay updates */
   double max_rebuild_ms;      /* the suffix-tree rebuild (incremental, or full after the pool filled) */
   double max_launch_ms;       /* the engine launch with its reruns after a buffer grew */
+  double max_engine_ms;       /* the longest engine run on the GPU (CUDA events) */
 } cpg_server_stats;
 
 void cpg_server_options_init(cpg_server_options* o);

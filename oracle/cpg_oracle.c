@@ -381,12 +381,115 @@ typedef struct {
   size_t n, cap;
 } vec_t;
 
+/* Pruning tables (orc_closure_topk_paths, prune != 0): each vertex's
+ * deviation edges ordered by exact delta, and the least delta on each
+ * vertex's suffix chain. */
+typedef struct {
+  int32_t* off;     /* n+1 row offsets */
+  int32_t* edge;    /* fan-out edge of each deviation, rows ordered by delta */
+  double* delta;    /* exact delta of each deviation */
+  double* chain;    /* least delta on the suffix chain from v; +inf if none */
+  double emax;      /* 2 max dist/10000 + max |w| */
+} prune_t;
+
+typedef struct {
+  double d;
+  int32_t e;
+} dev_key;
+
+static int cmp_dev(const void* pa, const void* pb) {
+  const dev_key* a = pa;
+  const dev_key* b = pb;
+  if (a->d < b->d) return -1;
+  if (a->d > b->d) return 1;
+  return (a->e > b->e) - (a->e < b->e);
+}
+
+static void prune_free(prune_t* p) {
+  free(p->off);
+  free(p->edge);
+  free(p->delta);
+  free(p->chain);
+}
+
+static int prune_build(const orc_graph* g, const int32_t* dist, const int32_t* succ,
+                       prune_t* p) {
+  const int32_t n = g->n;
+  memset(p, 0, sizeof(*p));
+  p->off = malloc(sizeof(int32_t) * ((size_t)n + 1));
+  p->edge = malloc(sizeof(int32_t) * (g->m ? (size_t)g->m : 1));
+  p->delta = malloc(sizeof(double) * (g->m ? (size_t)g->m : 1));
+  p->chain = malloc(sizeof(double) * (n ? (size_t)n : 1));
+  dev_key* row = malloc(sizeof(dev_key) * (g->m ? (size_t)g->m : 1));
+  int32_t* stack = malloc(sizeof(int32_t) * (n ? (size_t)n : 1));
+  unsigned char* done = calloc(n ? (size_t)n : 1, 1);
+  if (!p->off || !p->edge || !p->delta || !p->chain || !row || !stack || !done) {
+    free(row);
+    free(stack);
+    free(done);
+    prune_free(p);
+    return -1;
+  }
+  double dmax = 0.0, wmax = 0.0;
+  int32_t c = 0;
+  for (int32_t v = 0; v < n; ++v) {
+    p->off[v] = c;
+    if (dist[v] != INT_MAX && fabs(dist[v] / 1e4) > dmax) dmax = fabs(dist[v] / 1e4);
+    int32_t r = 0;
+    for (int32_t e = g->adjp[v]; e < g->adjp[v + 1]; ++e) {
+      const int32_t nb = g->adj[e];
+      if (fabs((double)g->w[e]) > wmax) wmax = fabs((double)g->w[e]);
+      if (nb == succ[v] || dist[nb] == INT_MAX) continue;
+      row[r].d = ((double)dist[nb] - (double)dist[v]) / 1e4 + (double)g->w[e];
+      row[r].e = e;
+      ++r;
+    }
+    qsort(row, (size_t)r, sizeof(dev_key), cmp_dev);
+    for (int32_t i = 0; i < r; ++i) {
+      p->edge[c + i] = row[i].e;
+      p->delta[c + i] = row[i].d;
+    }
+    c += r;
+  }
+  p->off[n] = c;
+  p->emax = 2.0 * dmax + wmax;
+  /* chain minima, memoised along successor chains (a cycle in succ cannot
+   * occur: dist strictly decreases along it unless delays are zero, and the
+   * walk stops at vertices already on the stack) */
+  for (int32_t v = 0; v < n; ++v) {
+    if (done[v]) continue;
+    int32_t top = 0;
+    for (int32_t u = v; u >= 0 && !done[u]; u = succ[u]) {
+      done[u] = 2;
+      stack[top++] = u;
+    }
+    while (top > 0) {
+      const int32_t u = stack[--top];
+      double m = p->off[u + 1] > p->off[u] ? p->delta[p->off[u]] : INFINITY;
+      const int32_t s = succ[u];
+      if (s >= 0 && done[s] == 1 && p->chain[s] < m) m = p->chain[s];
+      p->chain[u] = m;
+      done[u] = 1;
+    }
+  }
+  free(row);
+  free(stack);
+  free(done);
+  return 0;
+}
+
+static inline double prune_bound(const prune_t* p, float s) {
+  return 0x1p-20 * (fabs((double)s) + p->emax);
+}
+
 /* Accept every path whose cost is <= lim, expanding accepted paths along their
  * suffix chain.  Returns 0 on success, 1 if more than cap paths were accepted,
- * -1 on allocation failure.  *complete is set when no child was rejected. */
+ * -1 on allocation failure.  *complete is set when no child was rejected.
+ * With pr, rows and chain tails that cannot hold a child costing <= lim are
+ * skipped (counted as rejected). */
 static int closure(const orc_graph* g, const int32_t* dist, const int32_t* succ,
                    const int32_t* srcs, int32_t ns, float lim, size_t cap,
-                   vec_t* acc, int* complete) {
+                   const prune_t* pr, vec_t* acc, int* complete) {
   acc->n = 0;
   *complete = 1;
   for (int32_t i = 0; i < ns; ++i) {
@@ -400,6 +503,32 @@ static int closure(const orc_graph* g, const int32_t* dist, const int32_t* succ,
   }
   for (size_t i = 0; i < acc->n; ++i) {
     orc_node p = acc->a[i];
+    if (pr) {
+      const double room = (double)lim - (double)p.slack + prune_bound(pr, p.slack);
+      for (int32_t v = p.to; v != -1; v = succ[v]) {
+        if (pr->chain[v] > room) {
+          if (pr->chain[v] != INFINITY) *complete = 0;
+          break;
+        }
+        for (int32_t j = pr->off[v]; j < pr->off[v + 1]; ++j) {
+          if (pr->delta[j] > room) {
+            *complete = 0;
+            break;
+          }
+          const int32_t e = pr->edge[j], nb = g->adj[e];
+          float c = orc_child_cost(p.slack, dist[nb], g->w[e], dist[v]);
+          if (!(c <= lim)) {
+            *complete = 0;
+            continue;
+          }
+          if (acc->n >= cap) return 1;
+          if (grow((void**)&acc->a, &acc->cap, acc->n + 1, sizeof(orc_node))) return -1;
+          orc_node x = {p.level + 1, v, nb, (int32_t)i, 0, c};
+          acc->a[acc->n++] = x;
+        }
+      }
+      continue;
+    }
     for (int32_t v = p.to; v != -1; v = succ[v]) {
       for (int32_t e = g->adjp[v]; e < g->adjp[v + 1]; ++e) {
         int32_t nb = g->adj[e];
@@ -491,7 +620,17 @@ int64_t orc_closure_topk(const orc_graph* g, const int32_t* dist,
 int64_t orc_closure_topk_ex(const orc_graph* g, const int32_t* dist,
                             const int32_t* succ, int64_t k, int ref_roots,
                             orc_node* out, float* split_out) {
-  if (k <= 0) return 0;
+  return orc_closure_topk_paths(g, dist, succ, k, ref_roots, 1, out, split_out, NULL, NULL, 0);
+}
+
+int64_t orc_closure_topk_paths(const orc_graph* g, const int32_t* dist,
+                               const int32_t* succ, int64_t k, int ref_roots, int prune,
+                               orc_node* out, float* split_out, int64_t* path_off,
+                               int32_t* verts, int64_t verts_cap) {
+  if (k <= 0) {
+    if (path_off) path_off[0] = 0;
+    return 0;
+  }
   int32_t ns = 0;
   int32_t* srcs = seed_roots(g, dist, ref_roots, &ns);
   if (!srcs) return -1;
@@ -506,7 +645,17 @@ int64_t orc_closure_topk_ex(const orc_graph* g, const int32_t* dist,
   vec_t acc = {0};
   if (c0 == INFINITY) {
     free(srcs);
+    if (path_off) path_off[0] = 0;
     return 0;
+  }
+  prune_t pt;
+  const prune_t* pr = NULL;
+  if (prune) {
+    if (prune_build(g, dist, succ, &pt)) {
+      free(srcs);
+      return -1;
+    }
+    pr = &pt;
   }
   /* Children may cost a few ulps less than their parent after rounding; the
    * margin keeps such descendants in the closure. */
@@ -516,7 +665,7 @@ int64_t orc_closure_topk_ex(const orc_graph* g, const int32_t* dist,
   for (int iter = 0; iter < 400 && !done; ++iter) {
     t = c0 + d;
     float m = fmaxf(fmaxf(fabsf(t), 2.0f * dmax), 1.0f) * 0x1p-17f;
-    rc = closure(g, dist, succ, srcs, ns, t + m, cap, &acc, &complete);
+    rc = closure(g, dist, succ, srcs, ns, t + m, cap, pr, &acc, &complete);
     if (rc < 0) break;
     if (rc == 1) { /* over the cap: bisect down, or grow the cap on a tie wall */
       hi = d;
@@ -549,6 +698,7 @@ int64_t orc_closure_topk_ex(const orc_graph* g, const int32_t* dist,
   }
   if (!done && rc == 0) rc = -1;
   free(srcs);
+  if (pr) prune_free(&pt);
   if (rc != 0) {
     free(acc.a);
     return -1;
@@ -579,10 +729,51 @@ int64_t orc_closure_topk_ex(const orc_graph* g, const int32_t* dist,
     x.parent = x.parent >= 0 ? (int32_t)pos[x.parent] : -1;
     out[j] = x;
   }
+  int64_t status = nout;
+  if (path_off) {
+    /* vertex sequence: deviations from the root down, then the chain walk
+     * that leaves the chain at each deviation's tail for its head */
+    int64_t w = 0;
+    int32_t* devs = NULL;
+    size_t dcap = 0;
+    path_off[0] = 0;
+    for (int64_t j = 0; j < nout && status >= 0; ++j) {
+      size_t nd = 0;
+      int64_t cur = r[j].idx;
+      while (acc.a[cur].parent >= 0) {
+        if (grow((void**)&devs, &dcap, 2 * (nd + 1), sizeof(int32_t))) {
+          status = -1;
+          break;
+        }
+        devs[2 * nd] = acc.a[cur].from;
+        devs[2 * nd + 1] = acc.a[cur].to;
+        ++nd;
+        cur = acc.a[cur].parent;
+      }
+      if (status < 0) break;
+      int32_t v = acc.a[cur].to;
+      size_t d = nd;
+      while (v >= 0) {
+        if (w >= verts_cap) {
+          status = -2;
+          break;
+        }
+        verts[w++] = v;
+        if (d > 0 && devs[2 * (d - 1)] == v) {
+          v = devs[2 * (d - 1) + 1];
+          --d;
+        } else {
+          v = succ[v];
+        }
+      }
+      path_off[j + 1] = w;
+    }
+    free(devs);
+  }
   free(r);
   free(pos);
   free(acc.a);
-  return nout;
+  return status;
 }
 
 /* ------------------------------------------------------------ BVSS checks */

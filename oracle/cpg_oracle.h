@@ -101,6 +101,55 @@ int64_t orc_closure_topk_ex(const orc_graph* g, const int32_t* dist,
                             const int32_t* succ, int64_t k, int ref_roots,
                             orc_node* out, float* split_out);
 
+/* orc_closure_topk_ex with two additions.
+ *
+ * prune != 0 gives the same set faster.  Each vertex's deviation edges are
+ * ordered by their exact cost delta (dist_head - dist_tail)/10000 + w in
+ * double precision, and each vertex keeps the least delta on its suffix
+ * chain.  A parent of cost s stops scanning a row, or walking its chain, once
+ * s + delta exceeds the limit by more than a float-rounding bound
+ * E = 2^-20 (|s| + 2 max dist/10000 + max |w|).  The fp32 child cost
+ * ((s + a) + w) - b is at least the exact s + delta minus about 6 ulps of
+ * those magnitudes, so no child that could cost <= the limit is skipped.
+ * The closure's set, the split search and the float costs are unchanged;
+ * only the work per accepted path drops from the whole chain times the
+ * degree to the children that are accepted plus a few.
+ *
+ * When path_off is not NULL, the vertex sequence of returned path j (source to
+ * sink: the root's source, the suffix chain up to each deviation's tail, the
+ * deviation's head, and so on) is written to verts[path_off[j] ..
+ * path_off[j+1]).  path_off holds k+1 entries.  At most verts_cap vertices are
+ * written; the call returns -2 if they do not fit.
+ *
+ * Returns the number of paths, -1 on allocation failure, -2 if verts_cap is
+ * too small. */
+int64_t orc_closure_topk_paths(const orc_graph* g, const int32_t* dist,
+                               const int32_t* succ, int64_t k, int ref_roots, int prune,
+                               orc_node* out, float* split_out, int64_t* path_off,
+                               int32_t* verts, int64_t verts_cap);
+
+/* Parameters of the seeded levelised DAG (field order of the product's
+ * cpg_gen_params, so the same settings describe both generators). */
+typedef struct {
+  uint64_t seed;
+  int32_t n_pins, n_levels, n_first, n_last, level_span;
+  int32_t degree_kind; /* 0: uniform {deg_lo..deg_hi}; 1: geometric of mean deg_mean */
+  int32_t deg_lo, deg_hi;
+  double deg_mean;
+  int32_t deg_cap;
+  int32_t weight_kind; /* 0: fp32 uniform [w_lo, w_hi]; 1: integers {iw_lo..iw_hi} */
+  float w_lo, w_hi;
+  int32_t iw_lo, iw_hi;
+  int32_t add_virtual; /* super-source n_pins and super-sink n_pins+1 */
+} orc_gen_params;
+
+/* Seeded levelised DAG (cpg_gen.c).  On success *src, *dst, *w hold *m_out
+ * edges (free each with orc_free) and *n_out vertices; returns 0, -1 on
+ * allocation failure, -2 on bad parameters. */
+int orc_generate(const orc_gen_params* p, int32_t* n_out, int64_t* m_out, int32_t** src,
+                 int32_t** dst, float** w);
+void orc_free(void* p);
+
 /* Deviation edges of every vertex: fan-out edges whose head is not the
  * successor and whose head and tail distances are finite, with their cost
  * delta dist_head/10000 + w - dist_tail/10000 (build_compact_static_deviation_csr,

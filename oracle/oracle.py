@@ -27,6 +27,23 @@ class Graph(C.Structure):
                 ("iadj", C.c_void_p)]
 
 
+class GenParams(C.Structure):
+    """orc_gen_params (the field order of the product's cpg_gen_params)."""
+    _fields_ = [
+        ("seed", C.c_uint64), ("n_pins", C.c_int32), ("n_levels", C.c_int32),
+        ("n_first", C.c_int32), ("n_last", C.c_int32), ("level_span", C.c_int32),
+        ("degree_kind", C.c_int32), ("deg_lo", C.c_int32), ("deg_hi", C.c_int32),
+        ("deg_mean", C.c_double), ("deg_cap", C.c_int32), ("weight_kind", C.c_int32),
+        ("w_lo", C.c_float), ("w_hi", C.c_float), ("iw_lo", C.c_int32),
+        ("iw_hi", C.c_int32), ("add_virtual", C.c_int32),
+    ]
+
+
+GEN_DEFAULTS = dict(seed=1, n_pins=20000, n_levels=60, n_first=64, n_last=64, level_span=3,
+                    degree_kind=0, deg_lo=1, deg_hi=4, deg_mean=20.0, deg_cap=256,
+                    weight_kind=0, w_lo=0.1, w_hi=10.0, iw_lo=1, iw_hi=100, add_virtual=1)
+
+
 def build() -> None:
     subprocess.run(["make", "-s", "-C", HERE], check=True)
 
@@ -49,6 +66,16 @@ def _lib():
     lib.orc_closure_topk_ex.argtypes = [G, C.c_void_p, C.c_void_p, C.c_int64, C.c_int,
                                         C.c_void_p, C.POINTER(C.c_float)]
     lib.orc_closure_topk_ex.restype = C.c_int64
+    lib.orc_closure_topk_paths.argtypes = [G, C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_int,
+                                           C.c_void_p, C.POINTER(C.c_float), C.c_void_p,
+                                           C.c_void_p, C.c_int64]
+    lib.orc_closure_topk_paths.restype = C.c_int64
+    lib.orc_generate.argtypes = [C.POINTER(GenParams), C.POINTER(C.c_int32), C.POINTER(C.c_int64),
+                                 C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                                 C.POINTER(C.c_void_p)]
+    lib.orc_generate.restype = C.c_int
+    lib.orc_free.argtypes = [C.c_void_p]
+    lib.orc_free.restype = None
     lib.orc_deviation_csr.argtypes = [C.c_int32] + [C.c_void_p] * 8
     lib.orc_deviation_csr.restype = C.c_int32
     lib.orc_child_cost.argtypes = [C.c_float, C.c_int32, C.c_float, C.c_int32]
@@ -74,6 +101,27 @@ def lib():
 
 def _p(a):
     return a.ctypes.data_as(C.c_void_p)
+
+
+def generate(**kw):
+    """The seeded levelised DAG (cpg_gen.c) as (n, src, dst, w) arrays; the
+    same settings as the product's generator give the same edge list."""
+    p = GenParams(**{**GEN_DEFAULTS, **kw})
+    n, m = C.c_int32(), C.c_int64()
+    ps, pd, pw = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    rc = lib().orc_generate(C.byref(p), C.byref(n), C.byref(m), C.byref(ps), C.byref(pd),
+                            C.byref(pw))
+    if rc != 0:
+        raise ValueError(f"oracle generator rejected the parameters ({rc})")
+    try:
+        mm = m.value
+        src = np.ctypeslib.as_array(C.cast(ps, C.POINTER(C.c_int32)), (max(mm, 1),))[:mm].copy()
+        dst = np.ctypeslib.as_array(C.cast(pd, C.POINTER(C.c_int32)), (max(mm, 1),))[:mm].copy()
+        w = np.ctypeslib.as_array(C.cast(pw, C.POINTER(C.c_float)), (max(mm, 1),))[:mm].copy()
+    finally:
+        for q in (ps, pd, pw):
+            lib().orc_free(q)
+    return n.value, src, dst, w
 
 
 class OracleGraph:
@@ -137,17 +185,40 @@ class OracleGraph:
             raise MemoryError("oracle sequential failed")
         return out[:n]
 
-    def closure_topk(self, k: int, ref_roots: bool = True) -> tuple[np.ndarray, float]:
+    def closure_topk(self, k: int, ref_roots: bool = True,
+                     prune: bool = True) -> tuple[np.ndarray, float]:
         """k cheapest non-zero paths; ref_roots applies the reference
-        G-PathGen's root seeding (the default, as the reference behaves)."""
+        G-PathGen's root seeding (the default, as the reference behaves);
+        prune skips children that cannot cost <= the split (same set)."""
         d, s, _ = self.sfxt()
         out = np.empty(max(k, 1), NODE_DTYPE)
         split = C.c_float()
-        n = lib().orc_closure_topk_ex(C.byref(self.g), _p(d), _p(s), int(k), int(ref_roots),
-                                      _p(out), C.byref(split))
+        n = lib().orc_closure_topk_paths(C.byref(self.g), _p(d), _p(s), int(k), int(ref_roots),
+                                         int(prune), _p(out), C.byref(split), None, None, 0)
         if n < 0:
             raise MemoryError("oracle closure failed")
         return out[:n], split.value
+
+    def closure_paths(self, k: int, ref_roots: bool = True, prune: bool = True):
+        """closure_topk plus each returned path's vertex sequence (source to
+        sink) as a list of int32 arrays."""
+        d, s, _ = self.sfxt()
+        out = np.empty(max(k, 1), NODE_DTYPE)
+        off = np.zeros(max(k, 0) + 1, np.int64)
+        cap = max(1, int(k)) * 64
+        while True:
+            verts = np.empty(cap, np.int32)
+            split = C.c_float()
+            n = lib().orc_closure_topk_paths(C.byref(self.g), _p(d), _p(s), int(k),
+                                             int(ref_roots), int(prune), _p(out),
+                                             C.byref(split), _p(off), _p(verts), cap)
+            if n == -2:
+                cap *= 4
+                continue
+            if n < 0:
+                raise MemoryError("oracle closure failed")
+            break
+        return out[:n], [verts[off[j]:off[j + 1]].copy() for j in range(n)]
 
 
 def deviation_csr(adjp, adj, w, succ, dist):

@@ -50,12 +50,14 @@ for _name, (_deg, _k) in SWEEP.items():
 
 
 def load_case(name):
-    """(n, src, dst, w) numpy arrays of a case's graph."""
+    """(n, src, dst, w) numpy arrays of a case's graph.  Synthetic cases come
+    from the oracle's generator, which gives the same edge lists as the
+    product's cpg_dag_generate (tests/test_oracle.py checks that), so test
+    inputs never depend on the library under test."""
     import numpy as np
     c = CASES[name]
     if c["kind"] == "npz":
         z = np.load(os.path.join(HERE, "inputs", name + ".npz"))
         return int(z["n"]), z["src"], z["dst"], z["w"]
-    import cpg_b200
-    d = cpg_b200.generate(cpg_b200.gen_params(**c["gen"]))
-    return d.n, d.src, d.dst, d.w
+    import oracle
+    return oracle.generate(**c["gen"])

@@ -6,7 +6,7 @@ row order the reference's read_input builds (edges grouped by tail vertex in
 file order, gpucpg/gpucpg.cu:500-541), parsed by the oracle's restatement of
 read_input.  Output: tests/golden/inputs/<name>.npz with n, src, dst, w.
 
-    python tests/golden/make_inputs.py [/path/to/reference]
+    python tests/golden/make_inputs.py REFERENCE_DIR    (or CPG_REFERENCE=...)
 """
 import os
 import sys
@@ -21,8 +21,7 @@ import oracle  # noqa: E402
 NAMES = ["simple", "dac21_paper_example", "tv80_unit_wgts"]
 
 
-def main(ref=None):
-    ref = ref or "/root/reference"
+def main(ref):
     out = os.path.join(HERE, "inputs")
     os.makedirs(out, exist_ok=True)
     for name in NAMES:
@@ -35,4 +34,7 @@ def main(ref=None):
 
 
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("CPG_REFERENCE")
+    if not ref:
+        sys.exit("usage: make_inputs.py REFERENCE_DIR (or set CPG_REFERENCE)")
+    main(ref)

@@ -1,9 +1,22 @@
 """Pack the reference's raw golden outputs into tests/golden/ref_goldens.npz.
 
-Input: the directory make_goldens.py wrote on the GPU box (default
-gpurun_out/goldens): <case>.sfxt.txt ("succ dist" per vertex, from the
-reference's dump_succ_dists / dump_sfxt_by_vertex) and <case>.k<K>.txt (the
-reference G-PathGen's get_slacks(K), 9 significant digits).
+Record of how the fixture was made: the reference library (gpucpg/gpucpg.cu,
+compiled from its own sources with its own flags: --use_fast_math, RDC,
+C++20) was linked to a small driver that called CpGen exactly as the
+reference's golden writer does (examples/tc-pfxt-gate5.cu:15-44: reset(),
+report_paths(k, 10, true, LEVELIZE_THEN_RELAX, SHORT_LONG, false, 0.005f,
+5.0f, 8, false, false, false, true, CsrReorderMethod::NONE, false),
+get_slacks(k), costs written with 9 significant digits) and dumped
+dump_succ_dists / dump_sfxt_by_vertex.  It ran once on a B200.  The
+reference finished simple, dac21_paper_example and tv80_unit_wgts (suffix
+tree and costs) and the suffix tree of single20k_f32, then died with
+cudaErrorIllegalAddress ("device free failed") in G-PathGen on single20k_f32
+at K=10000.  The reference's GPU code is not run again, and the driver and
+its runner are no longer part of the repository; this packer and the
+fixture it wrote remain.
+
+Input: a directory of raw outputs: <case>.sfxt.txt ("succ dist" per vertex)
+and <case>.k<K>.txt (get_slacks(K), 9 significant digits).
 
 Small cases keep full arrays.  Large cases keep, per prefix K in
 {1e3, 1e4, 1e5, 1e6} that fits: the sha256 of the float32 costs of that
@@ -11,7 +24,7 @@ prefix, their float64 sum, and every 100th cost; plus the sha256 of the
 suffix-tree arrays.  That keeps the fixture small while still pinning every
 prefix bit for bit.
 
-    python tests/golden/pack_goldens.py [RAW_DIR]
+    python tests/golden/pack_goldens.py RAW_DIR
 """
 import glob
 import hashlib
@@ -34,8 +47,7 @@ def sha(a: np.ndarray) -> str:
     return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
 
 
-def main(raw=None):
-    raw = raw or os.path.join(ROOT, "gpurun_out", "goldens")
+def main(raw):
     out_path = os.path.join(HERE, "ref_goldens.npz")
     data = dict(np.load(out_path)) if os.path.exists(out_path) else {}
     for name, c in cases.CASES.items():
@@ -73,4 +85,6 @@ def main(raw=None):
 
 
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    if len(sys.argv) != 2:
+        sys.exit("usage: pack_goldens.py RAW_DIR")
+    main(sys.argv[1])

@@ -29,6 +29,11 @@ def _gen(name, **over):
     return cpg_b200.generate(cpg_b200.gen_params(**{**cases.CASES[name]["gen"], **over}))
 
 
+def _oracle_from_csr(n, adjp, adj, w):
+    src = np.repeat(np.arange(n, dtype=np.int32), np.diff(adjp))
+    return oracle.OracleGraph.from_edges(n, src, adj, w)
+
+
 def _run(n, src, dst, w, k, division=cpg_b200.DIV_IEEE, roots=cpg_b200.ROOTS_REFERENCE):
     with cpg_b200.CpGen(division=division, root_seeding=roots) as g:
         g.load_edges(n, src, dst, w)
@@ -218,6 +223,14 @@ def test_incremental_delay_update_matches_fresh_build():
         d_f, s_f, _ = g2.get_sfxt()
     assert np.array_equal(d_inc, d_f) and np.array_equal(s_inc, s_f)
     assert np.array_equal(inc, fresh)
+    # and both against the oracle on the updated delays
+    og = _oracle_from_csr(n, adjp, adj, ww)
+    od, os_, _ = og.sfxt()
+    np.testing.assert_array_equal(d_inc, od)
+    np.testing.assert_array_equal(s_inc, os_)
+    want = og.closure_topk(2000)[0]["slack"]
+    assert inc.size == want.size
+    np.testing.assert_allclose(inc, want, rtol=RTOL, atol=0)
 
 
 def test_hbm_budget_is_enforced():
@@ -323,6 +336,14 @@ def test_many_incremental_updates_overflow_pool_and_stay_exact():
     np.testing.assert_array_equal(s, s2)
     np.testing.assert_array_equal(lv, lv2)
     assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    # the final delays through the oracle: suffix tree and costs bit-exact
+    og = _oracle_from_csr(n, adjp, adj, ww)
+    od, os_, ol = og.sfxt()
+    np.testing.assert_array_equal(d, od)
+    np.testing.assert_array_equal(s, os_)
+    np.testing.assert_array_equal(lv, ol)
+    oc = og.closure_topk(3000)[0]["slack"]
+    assert np.array_equal(got.view(np.uint32), oc.view(np.uint32))
 
 
 def test_report_paths_batch_equals_single_calls():
@@ -341,3 +362,32 @@ def test_report_paths_batch_equals_single_calls():
         b, _, _, _ = _run(n, src, dst, w, k)
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), name
         g.close()
+
+
+@pytest.mark.parametrize("name", ["small_f32_s11", "small_int_s13", "single20k_f32",
+                                  "single20k_int", "tv80_unit_wgts"])
+def test_path_sets_equal_oracle(name):
+    """get_pfxt_nodes identities (gpucpg.cu:21422-21440): the returned paths,
+    as vertex sequences, are the oracle's closure paths.  Paths costing
+    strictly less than the K-th cost must be the same set; at the K-th cost
+    itself a tie group may be cut differently, so there both sides must hold
+    the same number of paths, each a valid path of that cost."""
+    k = 3000
+    n, src, dst, w = _load(name)
+    og = oracle.OracleGraph.from_edges(n, src, dst, w)
+    want_nodes, want_paths = og.closure_paths(k)
+    want_costs = want_nodes["slack"]
+    with cpg_b200.CpGen(division=cpg_b200.DIV_IEEE) as g:
+        g.load_edges(n, src, dst, w)
+        g.report_paths(k)
+        costs = g.get_slacks(k)
+        assert np.array_equal(costs.view(np.uint32), want_costs.view(np.uint32))
+        kth = costs[-1]
+        got_paths = [tuple(g.path_vertices(i)) for i in range(costs.size)]
+    got = {p for p, c in zip(got_paths, costs) if c < kth}
+    want = {tuple(p) for p, c in zip(want_paths, want_costs) if c < kth}
+    assert len(got) == int(np.count_nonzero(costs < kth))
+    assert got == want
+    # boundary tie group: distinct paths, as many as the oracle's
+    tie = {p for p, c in zip(got_paths, costs) if c == kth}
+    assert len(tie) == int(np.count_nonzero(want_costs == kth))

@@ -148,3 +148,89 @@ def test_oracle_against_reference_goldens():
         np.testing.assert_allclose(clo, ref, rtol=1e-5, atol=0)
         costs_checked += 1
     assert sfxt_checked >= 4 and costs_checked >= 3
+
+
+@pytest.mark.parametrize("name", ["single20k_f32", "single20k_int", "small_f32_s11",
+                                  "small_int_s14"])
+def test_oracle_generator_equals_product_generator(name):
+    """The oracle's restated generator and the product's cpg_dag_generate give
+    the same edge list (host code only; no GPU)."""
+    import cpg_b200
+    gen = cases.CASES[name]["gen"]
+    d = cpg_b200.generate(cpg_b200.gen_params(**gen))
+    n, src, dst, w = oracle.generate(**gen)
+    assert n == d.n
+    np.testing.assert_array_equal(src, d.src)
+    np.testing.assert_array_equal(dst, d.dst)
+    np.testing.assert_array_equal(w.view(np.uint32), d.w.view(np.uint32))
+
+
+def test_oracle_generator_density_settings():
+    """The density-sweep settings (geometric degree, larger mean) agree too, on
+    a smaller pin count."""
+    import cpg_b200
+    gen = {**cases.CASES["large1m_d50"]["gen"], "n_pins": 30_000, "n_first": 100,
+           "n_last": 100, "n_levels": 40}
+    d = cpg_b200.generate(cpg_b200.gen_params(**gen))
+    n, src, dst, w = oracle.generate(**gen)
+    assert n == d.n and np.array_equal(src, d.src) and np.array_equal(dst, d.dst)
+    assert np.array_equal(w.view(np.uint32), d.w.view(np.uint32))
+
+
+@pytest.mark.parametrize("name,k", [("simple", 100), ("tv80_unit_wgts", 5000),
+                                    ("single20k_f32", 10000), ("single20k_int", 10000),
+                                    ("small_f32_s11", 20000), ("small_int_s13", 20000)])
+@pytest.mark.parametrize("ref_roots", [True, False])
+def test_pruned_closure_equals_full_scan(name, k, ref_roots):
+    """Skipping rows and chain tails that cannot hold a child <= the limit
+    returns the same costs and the same final split as scanning every
+    deviation edge of every chain."""
+    g = _graph(name)
+    a, sa = g.closure_topk(k, ref_roots=ref_roots, prune=False)
+    b, sb = g.closure_topk(k, ref_roots=ref_roots, prune=True)
+    assert sa == sb
+    assert np.array_equal(a["slack"].view(np.uint32), b["slack"].view(np.uint32))
+
+
+@pytest.mark.parametrize("name", ["small_f32_s12", "tv80_unit_wgts"])
+def test_closure_path_vertices(name):
+    """Each returned path's vertex sequence runs from a source to a sink over
+    fan-out edges, and its cost rebuilt by the reference's left-to-right
+    recurrence is the reported cost."""
+    g = _graph(name)
+    out, paths = g.closure_paths(1500)
+    d, s, _ = g.sfxt()
+    adjp, adj, w = g.csr()
+    indeg = np.zeros(g.n, np.int64)
+    np.add.at(indeg, adj, 1)
+    assert len(paths) == out.size and len({tuple(p) for p in paths}) == out.size
+    for nd, verts in zip(out, paths):
+        assert indeg[verts[0]] == 0 and adjp[verts[-1]] == adjp[verts[-1] + 1]
+        c = np.float32(np.float32(d[verts[0]]) / np.float32(10000))
+        for a, b in zip(verts[:-1], verts[1:]):
+            row = adj[adjp[a]:adjp[a + 1]]
+            assert b in row
+            if s[a] != b:
+                e = adjp[a] + int(np.flatnonzero(row == b)[0])
+                c = np.float32(oracle.child_cost(float(c), int(d[b]), float(w[e]), int(d[a])))
+        assert c == nd["slack"]
+
+
+PINS = os.path.join(os.path.dirname(__file__), "golden", "oracle_pins.npz")
+
+
+def test_oracle_pins_reproduce():
+    """The committed full-size pins are what the oracle computes: the
+    1M-pin fp32 workload's suffix tree and its first 1e5 costs."""
+    import hashlib
+    z = np.load(PINS)
+    name = "large1m_f32"
+    g = _graph(name)
+    d, s, lv = g.sfxt()
+    sha = lambda a: hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+    assert sha(d) == str(z[f"{name}/sfxt_sha_dist"])
+    assert sha(s) == str(z[f"{name}/sfxt_sha_succ"])
+    assert sha(lv) == str(z[f"{name}/sfxt_sha_level"])
+    costs = g.closure_topk(100_000, ref_roots=False)[0]["slack"]
+    for p in (1000, 10_000, 100_000):
+        assert sha(costs[:p]) == str(z[f"{name}/p{p}_sha"]), p

@@ -14,11 +14,24 @@ upload, query and cost download inside the timed region: steps streamed
 through two handles on two host threads, so that one step's upload overlaps
 the previous step's query (`e2e.serial`: one handle, each step in turn).
 
+The same JSON line carries the rest of the metric, measured in the same run
+on the same GPU (N = 1 only): `batched` (256 queries in one captured launch
+against plain per-graph handles), `served` (the 5,000-query Poisson stream:
+open-loop p50/p99 and saturation capacity, each against plain), `density`
+(mean degree 10/30/40/50) and `config1` (the 20,000-pin query at K = 1,000
+beside the CPU port of the reference's SEQUENTIAL path).  --plain-only skips
+them.
+
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 With N > 1 (torchrun) every rank runs an independent replica of the query on
 its own GPU (replicas only: the path has no exchange step); value = all
 ranks' paths / max-over-ranks time.
+
+--impl reference times the reference's CPU implementation of the path (the
+oracle port of its SEQUENTIAL heap; the reference's GPU code is not run,
+because its G-PathGen faulted on this hardware) on the same workload at a
+bounded K, without loading the product library.
 """
 import argparse
 import json
@@ -202,22 +215,28 @@ def barrier(world):
         dist.barrier()
 
 
-def cpu_reference(k_sample, dag=None):
-    """The reference's CPU path restated (oracle port): CPU levelise/relax/
-    successor + the SEQUENTIAL priority-queue enumeration, one host thread."""
+def cpu_reference(k_sample, dag=None, name=WORKLOAD):
+    """The reference's CPU path restated (oracle port): the SEQUENTIAL
+    priority-queue enumeration (gpucpg.cu:21230-21300) on one host thread,
+    timed alone as the reference's expand_time times it; the CPU suffix tree
+    it needs (the reference builds that on the GPU) is timed separately.
+    The graph comes from the oracle's generator unless one is given, so this
+    leg never loads the product library.  Returns (paths, heap seconds,
+    suffix-tree seconds)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     import cases
     if dag is None:
-        n, src, dst, w = cases.load_case(WORKLOAD)
+        n, src, dst, w = oracle.generate(**cases.CASES[name]["gen"])
     else:
         n, src, dst, w = dag.n, dag.src, dag.dst, dag.w
-    t0 = time.perf_counter()
     og = oracle.OracleGraph.from_edges(n, src, dst, w)
+    t0 = time.perf_counter()
     og.sfxt()
-    out = og.sequential(k_sample)
     t1 = time.perf_counter()
-    return len(out), t1 - t0
+    out = og.sequential(k_sample)
+    t2 = time.perf_counter()
+    return len(out), t2 - t1, t1 - t0
 
 
 def run_reference(args):
@@ -226,23 +245,37 @@ def run_reference(args):
     world, rank, _ = ranks()
     if rank != 0:
         return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    import cases
     k_sample = args.cpu_k
-    vals = []
+    n, src, dst, w = oracle.generate(**cases.CASES[WORKLOAD]["gen"])
+    og = oracle.OracleGraph.from_edges(n, src, dst, w)
+    t0 = time.perf_counter()
+    og.sfxt()
+    sfxt_s = time.perf_counter() - t0
+    vals, got = [], 0
     for i in range(args.warmup + args.steps):
-        nk, sec = cpu_reference(k_sample)
+        t0 = time.perf_counter()
+        got = og.sequential(k_sample).size
+        sec = time.perf_counter() - t0
         if i >= args.warmup:
-            vals.append(nk / sec)
+            vals.append(got / sec)
     v = float(np.median(vals))
+    sample = (f"oracle port of the reference CPU path: the SEQUENTIAL heap (gpucpg.cu:21230-"
+              f"21300) on one host thread, timed alone as expand_time is, on the same graph at "
+              f"K={k_sample} (the full K=1e6 would take about 2e9 heap pushes); its CPU suffix "
+              f"tree, which the reference builds on the GPU, took {sfxt_s:.2f} s and is not in "
+              f"the value")
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "paths/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1000.0 * k_sample / v, "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": 1000.0 * got / v, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "desc": WORKLOAD_DESC, "k": args.k,
-                   "sample_k": k_sample},
+                   "sample_k": k_sample, "paths_per_step": got},
         "cpu_baseline": {"value": v, "unit": "paths/s", "cores": 1, "kind": "port",
-                         "sample": f"oracle port of the reference CPU path (CPU suffix tree + "
-                                   f"SEQUENTIAL heap) on the same graph at K={k_sample}"},
+                         "sample": sample, "sfxt_s": sfxt_s},
         "e2e": {"value": v, "unit": "paths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -423,12 +456,22 @@ def run_ours(args):
         "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        nk, sec = cpu_reference(args.cpu_k, dag)
+        nk, sec, sfxt_s = cpu_reference(args.cpu_k, dag)
         line["cpu_baseline"] = {
             "value": nk / sec, "unit": "paths/s", "cores": 1, "kind": "port",
-            "sample": f"oracle port of the reference CPU path (CPU suffix tree + SEQUENTIAL "
-                      f"heap), same graph, K={args.cpu_k}, {sec:.1f} s"}
+            "sample": f"oracle port of the reference CPU path: SEQUENTIAL heap alone (as "
+                      f"expand_time), one host thread, same graph, K={args.cpu_k}, {sec:.2f} s; "
+                      f"CPU suffix tree {sfxt_s:.2f} s, not in the value",
+            "sfxt_s": sfxt_s}
     g.close()
+    if world == 1 and not args.plain_only:
+        # the rest of the metric, measured in the same run on the same GPU:
+        # batched and served forms against plain, the density sweep, and the
+        # 20,000-pin query the reference's CPU path runs in full
+        line["batched"] = batched_record(steps=5, warmup=2, autotune=args.autotune)
+        line["served"] = served_record(args.served_queries)
+        line["density"] = density_record(steps=3, warmup=2)
+        line["config1"] = config1_record(steps=20, warmup=3, cpu=not args.no_cpu_baseline)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -459,7 +502,7 @@ def batch_workload(seed=4, count=256):
     return dags, ks
 
 
-def run_batched(args):
+def batched_record(steps, warmup, autotune=True):
     """K-paths/sec of the batched form (one captured step answers all 256
     queries, suffix trees rebuilt each step) against the plain form answering
     the same queries one at a time on resident graphs."""
@@ -473,19 +516,19 @@ def run_batched(args):
         b.commit()
         b.set_queries(list(range(len(dags))), ks)
         b.run(True)
-        if args.autotune:
+        if autotune:
             b.autotune()
-        for _ in range(args.warmup):
+        for _ in range(warmup):
             b.run(True)
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        for _ in range(args.steps):
+        for _ in range(steps):
             b.run(True)
         e1.record(stream)
         torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / args.steps
+        ms = e0.elapsed_time(e1) / steps
         total = sum(int(b.costs(q).size) for q in range(len(ks)))
         st = b.stats()
     # plain form: the same queries one at a time (graphs resident, suffix
@@ -508,9 +551,9 @@ def run_batched(args):
     plain_ms = e0.elapsed_time(e1)
     for g in handles:
         g.close()
-    line = {
+    return {
         "form": "batched", "metric": METRIC, "value": total / (ms / 1e3), "unit": "paths/s",
-        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "n_gpus": 1, "steps": steps, "warmup": warmup, "ms_per_step": ms,
         "higher_is_better": True, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "batch256", "desc": BATCH_DESC, "queries": len(ks),
                    "paths_returned": total, "pins": int(sum(d.n for d in dags)),
@@ -518,9 +561,16 @@ def run_batched(args):
         "plain_sequential": {"value": total / (plain_ms / 1e3), "unit": "paths/s",
                              "ms": plain_ms},
         "speedup_vs_plain": plain_ms / ms,
+        "autotune": {"ran": bool(autotune),
+                     "choice": {k: st[k] for k in ("sfxt_mode", "frontier_used",
+                                                   "select_schedule", "sfxt_ctas_per_sm",
+                                                   "engine_ctas_per_sm") if k in st}},
         "batch_stats": st,
     }
-    print(json.dumps(line), flush=True)
+
+
+def run_batched(args):
+    print(json.dumps(batched_record(args.steps, args.warmup, args.autotune)), flush=True)
 
 
 # ---------------------------------------------------------------- served form
@@ -605,14 +655,17 @@ def _plain_replay(dags, qs, open_loop=True):
             "paths_per_s": paths / wall}
 
 
-def run_served(args):
+def served_record(n_queries):
+    """The served form on the config-5 stream: open-loop Poisson arrivals
+    (latency) and the same queries submitted at once (capacity), each beside
+    the plain form answering the stream one query at a time."""
     dags, _ = batch_workload(seed=5, count=32)
-    qs = served_stream(len(dags), [d.m for d in dags], count=args.served_queries)
+    qs = served_stream(len(dags), [d.m for d in dags], count=n_queries)
     served = _serve_replay(dags, qs, open_loop=True)
     plain = _plain_replay(dags, qs, open_loop=True)
     served_sat = _serve_replay(dags, qs, open_loop=False)
     plain_sat = _plain_replay(dags, qs, open_loop=False)
-    line = {
+    return {
         "form": "served", "metric": METRIC, "value": served["paths_per_s"], "unit": "paths/s",
         "n_gpus": 1, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "served5000", "desc": SERVED_DESC, "queries": len(qs),
@@ -622,14 +675,118 @@ def run_served(args):
         "plain_sequential": {"value": plain["paths_per_s"], "p50_ms": plain["p50_ms"],
                              "p99_ms": plain["p99_ms"], "stats": plain},
         "speedup_vs_plain": served["paths_per_s"] / max(plain["paths_per_s"], 1e-9),
-        # the same 5,000 queries submitted at once: the largest K-paths/sec
-        # each form sustains on this mix (the open-loop rate caps the above)
+        # the same queries submitted at once: the largest K-paths/sec each
+        # form sustains on this mix (the open-loop arrival rate caps the above)
         "capacity": {"served": served_sat["paths_per_s"], "plain": plain_sat["paths_per_s"],
                      "speedup_vs_plain": served_sat["paths_per_s"] /
                      max(plain_sat["paths_per_s"], 1e-9),
+                     "served_p50_ms": served_sat["p50_ms"], "served_p99_ms": served_sat["p99_ms"],
+                     "plain_p50_ms": plain_sat["p50_ms"], "plain_p99_ms": plain_sat["p99_ms"],
                      "served_stats": served_sat, "plain_stats": plain_sat},
     }
-    print(json.dumps(line), flush=True)
+
+
+def run_served(args):
+    print(json.dumps(served_record(args.served_queries)), flush=True)
+
+
+# ---------------------------------------------------------------- density sweep
+def density_record(steps, warmup):
+    """The density sweep on the 1M-pin generator (mean degree 10 / 30 / 40 /
+    50 at K = 1e6 / 2e5 / 2e5 / 1e5): K-paths/sec per degree with the
+    suffix tree rebuilt each query, and the split into suffix tree and
+    engine."""
+    import torch
+    import cpg_b200
+    import cases
+    hbm, _ = peaks()
+    out = {}
+    for name in sorted(cases.SWEEP, key=lambda x: cases.SWEEP[x][0]):
+        deg, k = cases.SWEEP[name]
+        dag = cpg_b200.generate(cpg_b200.gen_params(**cases.CASES[name]["gen"]))
+        stream = torch.cuda.Stream()
+        with cpg_b200.CpGen(stream=stream.cuda_stream) as g:
+            g.load_dag(dag)
+            n, m = g.num_verts(), g.num_edges()
+            for _ in range(warmup):
+                g.levelize()
+                g.report_paths(k)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            sf, sfk, pf = [], [], []
+            e0.record(stream)
+            for _ in range(steps):
+                g.levelize()
+                g.report_paths(k)
+                st = g.stats()
+                sf.append(st["sfxt_ms"])
+                sfk.append(st["sfxt_kernel_ms"])
+                pf.append(st["pfxt_ms"])
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / steps
+            got = int(g.get_slacks(k).size)
+            st = g.stats()
+        sfk_ms = float(np.mean(sfk))
+        out[name] = {
+            "mean_degree": deg, "k": k, "n": n, "m": m, "paths_returned": got,
+            "value": got / (ms / 1e3), "unit": "paths/s", "ms_per_query": ms,
+            "sfxt_ms": float(np.mean(sf)), "engine_ms": float(np.mean(pf)),
+            "paths_accepted": st["paths_accepted"], "items_generated": st["items_generated"],
+            "phases": st["phases"], "rounds": st["rounds"],
+            "sfxt_kernel_ms": sfk_ms,
+            "sfxt_frac_of_hbm": (36 * m + 32 * n) / (sfk_ms * 1e-3) / 1e9 / hbm,
+        }
+        del dag
+    return {"config": "density sweep, 1,000,000 pins / 200 levels, fp32 delays U[0.1,10]",
+            "steps": steps, "warmup": warmup, "graphs": out}
+
+
+# ---------------------------------------------------------------- config 1
+def config1_record(steps, warmup, cpu=True):
+    """The 20,000-pin / 60-level single query at K = 1,000 (the workload the
+    reference's CPU path runs in full): the GPU plain form beside the CPU port
+    of the reference's SEQUENTIAL heap on the same graph."""
+    import torch
+    import cpg_b200
+    import cases
+    name, k = "single20k_f32", 1000
+    dag = cpg_b200.generate(cpg_b200.gen_params(**cases.CASES[name]["gen"]))
+    stream = torch.cuda.Stream()
+    with cpg_b200.CpGen(stream=stream.cuda_stream) as g:
+        g.load_dag(dag)
+        for _ in range(warmup):
+            g.levelize()
+            g.report_paths(k)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            g.levelize()
+            g.report_paths(k)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        got = int(g.get_slacks(k).size)
+        st = g.stats()
+    rec = {"workload": name, "desc": "20,000 pins / 60 levels, out-degree U{1..4}, fp32 delays "
+                                     "U[0.1,10], 64 sources / 64 sinks, K=1,000",
+           "k": k, "paths_returned": got, "value": got / (ms / 1e3), "unit": "paths/s",
+           "ms_per_query": ms, "sfxt_ms": st["sfxt_ms"], "engine_ms": st["pfxt_ms"],
+           "steps": steps, "warmup": warmup}
+    if cpu:
+        reps, secs, nk, sfxt_s = 20, [], 0, 0.0
+        for _ in range(reps):
+            nk, sec, sfxt_s = cpu_reference(k, dag)
+            secs.append(sec)
+        sec = float(np.median(secs))
+        rec["cpu_baseline"] = {"value": nk / sec, "unit": "paths/s", "cores": 1, "kind": "port",
+                               "sample": f"SEQUENTIAL heap alone, one host thread, K={k}, median "
+                                         f"of {reps} runs ({sec * 1e3:.2f} ms); CPU suffix tree "
+                                         f"{sfxt_s * 1e3:.2f} ms, not in the value"}
+    return rec
 
 
 # ---------------------------------------------------------------- BVSS
@@ -794,10 +951,13 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-case", action="store_true",
                     help="one warm-up and one measured query only (for ncu)")
-    ap.add_argument("--form", default="plain", choices=["plain", "batched", "served", "bvss", "ingest"])
+    ap.add_argument("--form", default="plain",
+                    choices=["plain", "batched", "served", "density", "config1", "bvss", "ingest"])
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="batched form: skip cpg_batch_autotune before timing")
     ap.add_argument("--served-queries", type=int, default=5000)
+    ap.add_argument("--plain-only", action="store_true",
+                    help="skip the batched, served, density and config-1 records")
     ap.add_argument("--bvss-graphs", default="both", choices=["both", "sparse", "dense"])
     args = ap.parse_args()
     if args.profile_case:
@@ -806,6 +966,11 @@ def main():
         run_batched(args)
     elif args.form == "served":
         run_served(args)
+    elif args.form == "density":
+        print(json.dumps(density_record(args.steps, args.warmup)), flush=True)
+    elif args.form == "config1":
+        print(json.dumps(config1_record(args.steps, args.warmup, not args.no_cpu_baseline)),
+              flush=True)
     elif args.form == "bvss":
         run_bvss(args)
     elif args.form == "ingest":

@@ -105,7 +105,7 @@ class ServerStats(C.Structure):
         ("reserved", C.c_int32), ("sfxt_ms", C.c_double), ("retries", C.c_int64),
         ("pool_rebuilds", C.c_int64), ("max_step_ms", C.c_double),
         ("max_update_ms", C.c_double), ("max_rebuild_ms", C.c_double), ("max_launch_ms", C.c_double),
-        ("max_engine_ms", C.c_double),
+        ("max_engine_ms", C.c_double), ("loop_allocs", C.c_int64),
     ]
 
 
@@ -166,6 +166,8 @@ def _load():
         "cpg_num_edges": (C.c_int64, [H]),
         "cpg_get_csr": (C.c_int, [H, C.c_void_p, C.c_void_p, C.c_void_p]),
         "cpg_levelize": (C.c_int, [H]),
+        "cpg_set_spin_limit": (C.c_int, [H, C.c_uint32]),
+        "cpg_debug_fail_allocs_above": (None, [C.c_int64]),
         "cpg_update_delays": (C.c_int, [H, C.c_int64, C.c_void_p, C.c_void_p]),
         "cpg_get_sfxt": (C.c_int, [H, C.c_void_p, C.c_void_p, C.c_void_p]),
         "cpg_num_levels": (C.c_int32, [H]),
@@ -462,6 +464,10 @@ class CpGen:
     # suffix tree
     def levelize(self):
         self._check(lib.cpg_levelize(self._h), "levelize")
+
+    def set_spin_limit(self, limit: int):
+        """Device-wait poll limit for the calls that follow (0 = default)."""
+        self._check(lib.cpg_set_spin_limit(self._h, int(limit)), "set_spin_limit")
 
     def update_delays(self, eids, w):
         eids = np.ascontiguousarray(eids, np.int32)
@@ -829,6 +835,12 @@ def select_topk(d_costs: int, n: int, k: int, d_out: int, stream: int | None = N
     if st != CPG_OK:
         raise CpgError(st, "cpg_select_topk failed")
     return got.value
+
+
+def debug_fail_allocs_above(max_bytes: int) -> None:
+    """Failure injection for tests: device buffers above max_bytes fail as
+    out of memory (0 lifts the cap); process-wide."""
+    lib.cpg_debug_fail_allocs_above(int(max_bytes))
 
 
 def header_symbols(path: str = HEADER_PATH) -> list[str]:

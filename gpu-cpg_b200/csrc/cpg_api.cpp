@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <climits>
 #include <cmath>
@@ -134,14 +135,26 @@ Status cuda_fail(cpg_handle* h, int e, const char* what) {
     if (_e != cudaSuccess) return cuda_fail(h, _e, what); \
   } while (0)
 
+// Failure injection (cpg_debug_fail_allocs_above): device buffers larger
+// than this fail as out of memory without reaching cudaMalloc; 0 = off.
+std::atomic<int64_t> g_alloc_cap{0};
+// Allocations made by the calling thread (device buffers and the server's
+// pinned staging); the server loop reports the ones made inside it.
+thread_local int64_t t_allocs = 0;
+
 cudaError_t ensure(DevMem& b, size_t bytes) {
   if (bytes == 0) bytes = 16;
   if (b.bytes >= bytes) return cudaSuccess;
   if (b.p) cudaFree(b.p);
   b.p = nullptr;
   b.bytes = 0;
+  const int64_t cap = g_alloc_cap.load(std::memory_order_relaxed);
+  if (cap > 0 && bytes > static_cast<size_t>(cap)) return cudaErrorMemoryAllocation;
   cudaError_t e = cudaMalloc(&b.p, bytes);
-  if (e == cudaSuccess) b.bytes = bytes;
+  if (e == cudaSuccess) {
+    b.bytes = bytes;
+    ++t_allocs;
+  }
   return e;
 }
 
@@ -1236,6 +1249,16 @@ cpg_status cpg_levelize(cpg_handle* h) {
   return ensure_sfxt(h);
 }
 
+cpg_status cpg_set_spin_limit(cpg_handle* h, uint32_t spin_limit) {
+  if (check_handle(h) != CPG_OK) return CPG_ERR_INVALID;
+  h->opts.spin_limit = spin_limit;
+  return CPG_OK;
+}
+
+void cpg_debug_fail_allocs_above(int64_t max_bytes) {
+  g_alloc_cap.store(max_bytes > 0 ? max_bytes : 0, std::memory_order_relaxed);
+}
+
 cpg_status cpg_update_delays(cpg_handle* h, int64_t count, const int32_t* eids,
                              const float* w) {
   if (check_handle(h) != CPG_OK || count < 0) return CPG_ERR_INVALID;
@@ -1280,7 +1303,7 @@ cpg_status cpg_update_delays(cpg_handle* h, int64_t count, const int32_t* eids,
   }
   // staging kept by the handle: no allocation (and no device-wide
   // synchronisation) per update
-  CK(ensure(h->d_upd, static_cast<size_t>(count) * 8), "alloc delay update");
+  CK(ensure_grow(h->d_upd, static_cast<size_t>(count) * 8), "alloc delay update");
   int32_t* up_e = P<int32_t>(h->d_upd);
   float* up_w = reinterpret_cast<float*>(up_e + count);
   CK(cudaMemcpyAsync(up_e, eids, count * 4, cudaMemcpyHostToDevice, h->stream), "H2D eids");
@@ -2064,6 +2087,7 @@ struct cpg_server {
   double busy_ms = 0, sfxt_ms = 0, first_submit = -1, last_done = 0, max_step_ms = 0;
   double max_update_ms = 0, max_rebuild_ms = 0, max_launch_ms = 0, max_engine_ms = 0;
   int32_t max_batch_seen = 0;
+  int64_t loop_allocs = 0;  // allocations made inside the request loop
   // pinned staging of a launch's costs (grown geometrically, kept): one fast
   // copy from the device, one copy into the results
   float* pin_out = nullptr;
@@ -2118,6 +2142,7 @@ int server_launch(cpg_server* sv, const std::vector<ServerReq>& batch,
       cudaGetLastError();
       return fail(h, CPG_ERR_OOM, "pinned staging of the costs");
     }
+    ++t_allocs;
     sv->pin_cap = want;
   }
   if (total) {
@@ -2168,6 +2193,7 @@ void server_loop(cpg_server* sv) {
     }
     const double t_step = now_s();
     const int64_t pool_before = h->pool_rebuilds;
+    const int64_t allocs_before = t_allocs;
     Status st = CPG_OK;
     bool updated = false;
     for (const ServerReq& r : batch) {
@@ -2202,6 +2228,7 @@ void server_loop(cpg_server* sv) {
       sv->max_rebuild_ms = std::max(sv->max_rebuild_ms, (t_sfxt - t_upd) * 1e3);
       sv->max_launch_ms = std::max(sv->max_launch_ms, (t - t_sfxt) * 1e3);
       sv->pool_rebuilds += h->pool_rebuilds - pool_before;
+      sv->loop_allocs += t_allocs - allocs_before;
       for (size_t i = 0; i < batch.size(); ++i) {
         ServerResult& res = sv->results[batch[i].ticket];
         res.status = st;
@@ -2304,12 +2331,31 @@ cpg_status cpg_server_start(cpg_server* sv) {
       pre = std::min<unsigned long long>(
           pre, static_cast<unsigned long long>(sv->so.hbm_budget_bytes) / (8 * 512));
     const unsigned long long ns = static_cast<unsigned long long>(h->n_srcs);
+    // engine_prepare sizes the piles from the handle's capacities; if it
+    // fails they go back to what they were, so a later start or batch call
+    // does not retry the same oversized growth
+    const unsigned long long old_paths = h->cap_paths, old_front = h->cap_front,
+                             old_pend = h->cap_pend;
     h->cap_paths = std::max(h->cap_paths, 4 * pre + ns);
     h->cap_front = std::max(h->cap_front, 2 * pre);
     h->cap_pend = std::max(h->cap_pend, 8 * pre + ns);
     const std::vector<EngineQuery> none(static_cast<size_t>(std::max(1, sv->so.max_batch)));
     const Status ws = engine_prepare(h, none, pre);
-    if (ws != CPG_OK) return static_cast<cpg_status>(ws);
+    if (ws != CPG_OK) {
+      h->cap_paths = old_paths;
+      h->cap_front = old_front;
+      h->cap_pend = old_pend;
+      sv->err = cpg_last_error(h);
+      return static_cast<cpg_status>(ws);
+    }
+    // the delay-update staging, for a request that re-samples every edge of
+    // the largest graph
+    size_t max_edges = 1;
+    const cpg_batch* b = sv->b;
+    for (size_t g = 0; g + 1 < b->voff.size(); ++g)
+      max_edges = std::max<size_t>(
+          max_edges, static_cast<size_t>(b->adjp[b->voff[g + 1]] - b->adjp[b->voff[g]]));
+    CK(ensure_grow(h->d_upd, max_edges * 8), "alloc delay update");
     if (!sv->pin_out) {
       if (cudaMallocHost(&sv->pin_out, pre * 4) == cudaSuccess) {
         sv->pin_cap = pre;
@@ -2414,6 +2460,7 @@ cpg_status cpg_server_get_stats(const cpg_server* svc, cpg_server_stats* out) {
   out->max_rebuild_ms = sv->max_rebuild_ms;
   out->max_launch_ms = sv->max_launch_ms;
   out->max_engine_ms = sv->max_engine_ms;
+  out->loop_allocs = sv->loop_allocs;
   return CPG_OK;
 }
 

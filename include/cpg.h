@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define CPG_ABI_VERSION 2
+#define CPG_ABI_VERSION 3
 
 /* Replaces exit(1) in cudaCheckErrors / checkError_t (gpucpg.cu:87-98,
  * 269-275) and the std::runtime_error throws of read_input (gpucpg.cu:457). */
@@ -179,6 +179,19 @@ cpg_status cpg_get_csr(const cpg_handle* h, int32_t* adjp, int32_t* adjncy,
 cpg_status cpg_load_csr_bin(cpg_handle* h, const char* path);
 cpg_status cpg_write_csr_bin(const cpg_handle* h, const char* path);
 
+/* Changes the handle's device-wait poll limit (cpg_options.spin_limit; 0 =
+ * the default) for the calls that follow.  A wait that runs out returns
+ * CPG_ERR_TIMEOUT and leaves the handle usable: the next call starts its
+ * device work afresh.  The reference's waits are unbounded (the cooperative
+ * loop's grid.sync(), gpucpg.cu:9152-9415); it has no such limit. */
+cpg_status cpg_set_spin_limit(cpg_handle* h, uint32_t spin_limit);
+
+/* Failure-injection hook for tests: from now on, every device buffer of a
+ * handle, batch or server larger than max_bytes fails as out of device memory
+ * (CPG_ERR_OOM) without calling cudaMalloc; 0 lifts the cap.  Process-wide.
+ * The reference exits on any CUDA error instead (gpucpg.cu:87-98). */
+void cpg_debug_fail_allocs_above(int64_t max_bytes);
+
 /* ------------------------------------------------------------ suffix tree */
 /* LEVELIZE_THEN_RELAX + update_successors_bu (gpucpg.cu:17642-17963,
  * 18421-18432): levels, fixed-point distances, successors and the sorted
@@ -320,6 +333,9 @@ typedef struct {
   double max_rebuild_ms;      /* the suffix-tree rebuild (incremental, or full after the pool filled) */
   double max_launch_ms;       /* the engine launch with its reruns after a buffer grew */
   double max_engine_ms;       /* the longest engine run on the GPU (CUDA events) */
+  int64_t loop_allocs;        /* device or pinned buffers allocated inside the request
+                                 loop (buffer growth); 0 while the admitted mix fits
+                                 what cpg_server_start allocated */
 } cpg_server_stats;
 
 void cpg_server_options_init(cpg_server_options* o);
@@ -378,7 +394,10 @@ cpg_status cpg_select_topk(const float* d_costs, int64_t n, int64_t k,
  *  - The scratch (about 4.3 MiB) is reserved on every GPU that loads the
  *    library and kept until the process exits.
  *  - The first call on a device looks up the scratch's device address (with
- *    that device current); make it before any stream capture.
+ *    that device current); make it before any stream capture.  The address
+ *    is kept for the life of the process: after cudaDeviceReset on that
+ *    device the module is loaded again and the kept address is stale, so do
+ *    not call this entry point across a device reset.
  *  - All calls share the one array: calls that overlap on the GPU (from two
  *    streams or threads at once) race and must be serialised by the caller.
  *  - Calls no cudaMalloc/cudaFree; returns after the result is written. */

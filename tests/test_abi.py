@@ -21,7 +21,7 @@ def test_library_exports_every_header_symbol():
     assert len(names) >= 30
     missing = [n for n in names if not hasattr(cpg_b200.lib, n)]
     assert not missing, missing
-    assert cpg_b200.lib.cpg_abi_version() == 2
+    assert cpg_b200.lib.cpg_abi_version() == 3
 
 
 def test_status_strings():

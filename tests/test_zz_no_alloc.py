@@ -53,3 +53,34 @@ def test_noalloc_rejects_k_above_its_limit():
     out = torch.empty(16, dtype=torch.float32, device="cuda")
     st, n = _run(cpg_b200.lib.cpg_select_topk_noalloc, d, 16, MAX_K + 1, out)
     assert st == 4 and n == 0          # CPG_ERR_CAPACITY, nothing written
+
+
+@pytest.mark.parametrize("case", ["n_below_k", "all_zero", "few_nonzero_at_max_k"])
+def test_noalloc_edge_cases_match_numpy(case):
+    """k above n (min(k, n) is selected), an all-zero input (nothing is
+    returned), and fewer non-zero costs than k at the largest k (the sort
+    runs on fewer keys than the scratch is laid out for); each against
+    np.sort(c[c != 0])[:k] and against the allocating entry point."""
+    import torch
+    rng = np.random.default_rng(11)
+    if case == "n_below_k":
+        n, k = 5000, 20000
+        c = rng.uniform(0.0, 10.0, size=n).astype(np.float32)
+    elif case == "all_zero":
+        n, k = 100_000, 5000
+        c = np.zeros(n, np.float32)
+    else:
+        n, k = 1_000_000, MAX_K
+        c = np.zeros(n, np.float32)
+        nz = rng.choice(n, size=70_000, replace=False)
+        c[nz] = rng.uniform(0.5, 50.0, size=nz.size).astype(np.float32)
+    d = torch.from_numpy(c).cuda()
+    a = torch.full((k,), -1.0, dtype=torch.float32, device="cuda")
+    b = torch.full((k,), -2.0, dtype=torch.float32, device="cuda")
+    st_a, na = _run(cpg_b200.lib.cpg_select_topk, d, n, k, a)
+    st_b, nb = _run(cpg_b200.lib.cpg_select_topk_noalloc, d, n, k, b)
+    want = np.sort(c[c != 0.0])[:k]
+    assert st_a == 0 and st_b == 0
+    assert na == nb == want.size
+    assert np.array_equal(b[:nb].cpu().numpy(), want)
+    assert torch.equal(a[:na].view(torch.int32), b[:nb].view(torch.int32))

@@ -459,6 +459,7 @@ SfxtParams sfxt_params(cpg_handle* h, int32_t start_level) {
   p.level_sync = h->opts.sfxt_level_sync == 1;
   p.heap_warps = std::min(std::max(h->opts.sfxt_heap_warps, 0), 16);
   p.early_push = h->opts.sfxt_late_push != 1 && p.heap_warps == 0;
+  p.heap_phase = p.heap_warps == 0 && h->opts.sfxt_inline_heaps != 1;
   p.dl = P<unsigned long long>(h->d_dl);
   p.orig_id = h->relabeled ? P<int32_t>(h->d_orig_id) : nullptr;
   if (start_level > 0) {

@@ -706,7 +706,8 @@ __device__ void heap_insert(const SfxtParams& p, int v, unsigned long long* chun
 
 // Level-synchronous inserts, one vertex per lane (v < 0: none): the warp
 // takes all its lanes' nodes with one atomic on the pool cursor.  Every lane
-// of the warp calls.
+// of the warp calls.  kPublish: other threads poll the new heaps' sizes.
+template <bool kPublish = false>
 __device__ void heap_insert_lanes(const SfxtParams& p, int v) {
   const int lane = threadIdx.x & 31;
   InsertPlan q;
@@ -727,15 +728,58 @@ __device__ void heap_insert_lanes(const SfxtParams& p, int v) {
   base = __shfl_sync(0xffffffffu, base, 31);
   if (v < 0) return;
   if (q.empty) {
-    heap_store<false>(p, v, q.base_root, q.base_size);
+    heap_store<kPublish>(p, v, q.base_root, q.base_size);
     return;
   }
   if (base + tot > p.hnode_cap) {
     atomicCAS(&p.ctr->err, kDevOk, kDevCapacity);
-    heap_store<false>(p, v, -1, 0);
+    heap_store<kPublish>(p, v, -1, 0);
     return;
   }
-  heap_insert_at<false>(p, v, q, base + (incl - need));
+  heap_insert_at<kPublish>(p, v, q, base + (incl - need));
+}
+
+// The chain-heap phase of a dataflow build (p.heap_phase): after every
+// vertex is built, each lane inserts the heaps of the queue slots it owns,
+// in queue order (a vertex's successor is queued before it).  A heap waits
+// only for its successor's, so the waits follow successor chains (about 80
+// hops on the 1M-pin graph) instead of the 200 levels, and no build waits on
+// a heap.  The 32 lanes of a warp take 32 consecutive slots; a lane's
+// successor may be one of them, so the warp inserts, round after round, the
+// lanes whose successor's heap is complete, with one pool reservation per
+// round.  Returns false if a wait ran out.
+__device__ bool heap_phase(const SfxtParams& p) {
+  const int lane = threadIdx.x & 31;
+  const int nw = gridDim.x * (blockDim.x >> 5);
+  const int gw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  for (int base = gw * 32; base < p.n; base += nw * 32) {
+    const int g = base + lane;
+    const int v = g < p.n ? __ldcg(p.queue + g) : -1;
+    const int s = v >= 0 ? __ldcg(p.succ + v) : -1;
+    bool pending = v >= 0;
+    unsigned int it = 0;
+    while (__any_sync(0xffffffffu, pending)) {
+      bool ready = false;
+      if (pending)
+        ready = s < 0 || *reinterpret_cast<const volatile int*>(p.ht_size + s) >= 0;
+      if (!__any_sync(0xffffffffu, ready)) {
+        ++it;
+        const bool bail = __any_sync(0xffffffffu, it > p.spin_limit ||
+                                     ((it & 31) == 0 &&
+                                      *reinterpret_cast<volatile int*>(&p.ctr->err) != kDevOk));
+        if (bail) {
+          if (lane == 0) atomicCAS(&p.ctr->err, kDevOk, kDevTimeout);
+          return false;
+        }
+        __nanosleep(32);
+        continue;
+      }
+      __threadfence();  // the successors' heaps before their nodes are read
+      heap_insert_lanes<true>(p, ready ? v : -1);
+      pending = pending && !ready;
+    }
+  }
+  return true;
 }
 
 // BVSS form of the Kahn step.  A vertex that joins level L sets its bit in
@@ -1358,7 +1402,8 @@ sfxt_dataflow_kernel(SfxtParams p) {
         const int lvl = build_vertex_polled(p, v);
         if (lvl < 0) break;
         max_lvl = max(max_lvl, lvl);
-        if (lane == 0 && wait_heap(p, __ldcg(p.succ + v))) heap_insert<true>(p, v, chunk);
+        if (!p.heap_phase && lane == 0 && wait_heap(p, __ldcg(p.succ + v)))
+          heap_insert<true>(p, v, chunk);
         __syncwarp();
         continue;
       }
@@ -1370,7 +1415,7 @@ sfxt_dataflow_kernel(SfxtParams p) {
         *reinterpret_cast<volatile int*>(p.order + v) = 1;
       }
       dataflow_push<true>(p, v);
-      if (heap_warps == 0 && lane == 0 && wait_heap(p, __ldcg(p.succ + v)))
+      if (heap_warps == 0 && !p.heap_phase && lane == 0 && wait_heap(p, __ldcg(p.succ + v)))
         heap_insert<true>(p, v, chunk);
       __syncwarp();
     }
@@ -1388,6 +1433,11 @@ sfxt_dataflow_kernel(SfxtParams p) {
   }
   if (lane == 0) atomicMax(&p.ctr->levels, max_lvl + 1);
   if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit)) return;
+  if (p.heap_phase) {
+    const bool ok = heap_phase(p);
+    if (!__syncthreads_and(ok) && threadIdx.x == 0) atomicCAS(&p.ctr->err, kDevOk, kDevTimeout);
+    if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit)) return;
+  }
   // counting sort by level: histogram (block-local when the levels fit)
   const int L = *reinterpret_cast<volatile int*>(&p.ctr->levels);
   if (L <= kSfxtThreads) {

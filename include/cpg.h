@@ -99,6 +99,10 @@ typedef struct {
   int32_t batch_caller_order; /* batched and served forms: 1 = keep the
                                callers' vertex order instead of renumbering
                                each graph in level order (A/B checks) */
+  int32_t sfxt_inline_heaps; /* dataflow build: 1 = the building warp inserts
+                               each vertex's chain heap right after its build,
+                               instead of a heap phase after every build (A/B
+                               checks) */
 } cpg_options;
 
 typedef struct cpg_handle cpg_handle;

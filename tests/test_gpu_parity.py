@@ -275,7 +275,8 @@ def test_host_stepped_and_engine_agree(name):
     assert np.array_equal(out[0].view(np.uint32), out[1].view(np.uint32))
 
 
-@pytest.mark.parametrize("mode", ["early_push", "late_push", "heap_warps"])
+@pytest.mark.parametrize("mode", ["early_push", "late_push", "heap_warps", "inline_heaps",
+                                  "late_inline_heaps"])
 @pytest.mark.parametrize("name", ["simple", "tv80_unit_wgts", "single20k_f32", "small_int_s13"])
 def test_dataflow_build_equals_level_sync(name, mode):
     """The default full suffix-tree build (dataflow work queue) and the
@@ -290,7 +291,8 @@ def test_dataflow_build_equals_level_sync(name, mode):
         with cpg_b200.CpGen(division=cpg_b200.DIV_IEEE, frontier=cpg_b200.FRONTIER_CSR,
                             sfxt_level_sync=level_sync,
                             sfxt_heap_warps=4 if mode == "heap_warps" else 0,
-                            sfxt_late_push=mode != "early_push") as g:
+                            sfxt_inline_heaps=mode.endswith("inline_heaps"),
+                            sfxt_late_push=mode.startswith("late") or mode == "heap_warps") as g:
             g.load_edges(n, src, dst, w)
             g.report_paths(2000)
             first = (g.get_sfxt(), g.get_slacks(2000), g.num_levels())

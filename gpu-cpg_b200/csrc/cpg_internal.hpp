@@ -121,6 +121,8 @@ struct SfxtCounters {
   alignas(128) int n_long;   // rows left for the row-sort pass (long_rows[])
   // dataflow build: append cursors of the kSfxtQueues work queues, one line each
   alignas(128) int qtail[8][32];
+  alignas(128) int sort_blocks;  // dataflow build: blocks whose level histogram is in
+  int sort_ready;                // ... and the level offsets are scanned
   alignas(128) unsigned long long vss_tensor;  // BVSS tiles counted on the tensor cores
   unsigned long long vss_scalar;               // ... and with scalar popc
   alignas(128) GridBarrier bar;

@@ -1173,71 +1173,96 @@ __device__ int build_vertex_polled(const SfxtParams& p, int v) {
     }
     lmax = lvl;
   } else {
-    // long rows: wait for every head once, then read the distances plainly
+    // Long rows (a super-source's, say), eight chunks of 32 edges per pass
+    // with every load of a pass issued before any is used.  Pass 1 waits for
+    // each head's published word and takes, per lane, the least candidate
+    // distance and the largest head reaching it; pass 2 writes the row.
+    constexpr int kC = 8;
+    int lbest = INT_MAX, ls = -1, lnt = 0;
     bool ok = true;
-    for (int e = rb + lane; e < re && ok; e += 32) {
-      const int h = p.edges[e].head;
-      unsigned int it = 0;
-      unsigned long long x;
-      while ((x = ld_dl(p, h)) == kNone) {
-        if (++it > p.spin_limit ||
-          ((it & 31) == 0 && *reinterpret_cast<volatile int*>(&p.ctr->err) != kDevOk)) {
-          atomicCAS(&p.ctr->err, kDevOk, kDevTimeout);
-          ok = false;
-          break;
-        }
-        __nanosleep(32);
+    for (int base = rb; base < re && ok; base += kC * 32) {
+      DevEdge ed[kC];
+      unsigned long long x[kC];
+#pragma unroll
+      for (int c = 0; c < kC; ++c) {
+        const int e = base + c * 32 + lane;
+        ed[c].head = -1;
+        ed[c].w = 0.f;
+        if (e < re) ed[c] = p.edges[e];
       }
-      if (ok) lmax = max(lmax, static_cast<int>(x >> 32));
+#pragma unroll
+      for (int c = 0; c < kC; ++c) x[c] = ed[c].head >= 0 ? ld_dl(p, ed[c].head) : 0ull;
+#pragma unroll
+      for (int c = 0; c < kC; ++c) {
+        if (ed[c].head < 0) continue;
+        unsigned int it = 0;
+        while (x[c] == kNone && ok) {
+          if (++it > p.spin_limit ||
+              ((it & 31) == 0 && *reinterpret_cast<volatile int*>(&p.ctr->err) != kDevOk)) {
+            atomicCAS(&p.ctr->err, kDevOk, kDevTimeout);
+            ok = false;
+            break;
+          }
+          __nanosleep(32);
+          x[c] = ld_dl(p, ed[c].head);
+        }
+        if (!ok) break;
+        lmax = max(lmax, static_cast<int>(x[c] >> 32));
+        const int cd = cand_dist(static_cast<int>(x[c] & 0xffffffffu), ed[c].w);
+        if (cd < lbest) {
+          lbest = cd;
+          ls = ed[c].head;
+          lnt = 1;
+        } else if (cd == lbest) {
+          ls = max(ls, ed[c].head);
+          ++lnt;
+        }
+      }
     }
     if (!__all_sync(0xffffffffu, ok)) return -1;
     const int lvl = warp_max_i(lmax) + 1;
+    best = warp_min_i(lbest);
+    s = warp_max_i(lbest == best ? ls : -1);
     // the heads' distances come from their published words
     auto dist_of = [&](int h) { return static_cast<int>(ld_dl(p, h) & 0xffffffffu); };
-    for (int e = rb + lane; e < re; e += 32) {
-      const DevEdge ed = p.edges[e];
-      best = min(best, cand_dist(dist_of(ed.head), ed.w));
-    }
-    best = warp_min_i(best);
-    int nt = 0;
-    for (int e = rb + lane; e < re; e += 32) {
-      const DevEdge ed = p.edges[e];
-      if (cand_dist(dist_of(ed.head), ed.w) == best) {
-        s = max(s, ed.head);
-        ++nt;
-      }
-    }
-    if (p.orig_id && __reduce_add_sync(0xffffffffu, nt) > 1) {
+    if (p.orig_id && __reduce_add_sync(0xffffffffu, lbest == best ? lnt : 0) > 1) {
       unsigned long long k = 0;
       for (int e = rb + lane; e < re; e += 32) {
         const DevEdge ed = p.edges[e];
         if (cand_dist(dist_of(ed.head), ed.w) == best) {
-          const unsigned long long x = succ_word(p, ed.head);
-          k = x > k ? x : k;
+          const unsigned long long y = succ_word(p, ed.head);
+          k = y > k ? y : k;
         }
       }
       s = static_cast<int>(group_max_u64<32>(k) & 0xffffffffu);
-    } else {
-      s = warp_max_i(s);
     }
     BestDev bd = best_none();
-    for (int base = rb; base < re; base += 32) {
-      const int e = base + lane;
-      bool valid = false;
-      DevSidetrack rec;
-      if (e < re) {
-        const DevEdge ed = p.edges[e];
-        const int dh = dist_of(ed.head);
-        valid = ed.head != s && dh != INT_MAX;
-        rec.head = ed.head;
-        rec.w = ed.w;
-        rec.dist_head = dh;
-        rec.key = deviation_key(dh, best, ed.w);
+    for (int base = rb; base < re; base += kC * 32) {
+      DevEdge ed[kC];
+      int dh[kC];
+#pragma unroll
+      for (int c = 0; c < kC; ++c) {
+        const int e = base + c * 32 + lane;
+        ed[c].head = -1;
+        ed[c].w = 0.f;
+        if (e < re) ed[c] = p.edges[e];
       }
-      const unsigned bal = __ballot_sync(0xffffffffu, valid);
-      if (valid) p.dev[rb + cnt + __popc(bal & lanemask_lt())] = rec;
-      best_take(bd, valid, rec, e - rb);
-      cnt += __popc(bal);
+#pragma unroll
+      for (int c = 0; c < kC; ++c) dh[c] = ed[c].head >= 0 ? dist_of(ed[c].head) : INT_MAX;
+#pragma unroll
+      for (int c = 0; c < kC; ++c) {
+        const int e = base + c * 32 + lane;
+        const bool valid = ed[c].head >= 0 && ed[c].head != s && dh[c] != INT_MAX;
+        DevSidetrack rec;
+        rec.head = ed[c].head;
+        rec.w = ed[c].w;
+        rec.dist_head = dh[c];
+        rec.key = deviation_key(dh[c], best, ed[c].w);
+        const unsigned bal = __ballot_sync(0xffffffffu, valid);
+        if (valid) p.dev[rb + cnt + __popc(bal & lanemask_lt())] = rec;
+        best_take(bd, valid, rec, e - rb);
+        cnt += __popc(bal);
+      }
     }
     top = best_reduce(bd);
     lmax = lvl;
@@ -1325,25 +1350,46 @@ __device__ __forceinline__ void queue_push(const SfxtParams& p, bool on, int u) 
 // Kahn step of the dataflow build: take one pending fan-out off each tail;
 // tails reaching zero are queued.  kRelease: v's build precedes the push and
 // is published by it (late push); an early push publishes nothing.
+// Up to eight chunks of 32 tails per pass: their loads, then their
+// decrements, then one queue reservation for all the tails that became
+// ready, so a hub (the super-sink's 2,000 fan-in edges, say) costs a few
+// round trips per 256 tails instead of several per 32.
 template <bool kRelease>
 __device__ __forceinline__ void dataflow_push(const SfxtParams& p, int v) {
+  static_assert(kSfxtQueues == 1, "one reservation per pass assumes one queue");
+  constexpr int kC = 8;
   const int lane = threadIdx.x & 31;
   const int ib = p.iadjp[v];
   const int ie = p.iadjp[v + 1];
-  for (int base = ib; base < ie; base += 4 * 32) {
-    int u[4];
-    bool ready[4];
+  for (int base = ib; base < ie; base += kC * 32) {
+    const int nc = min(kC, (ie - base + 31) / 32);  // warp-uniform
+    int u[kC];
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
+    for (int c = 0; c < kC; ++c) {
       const int e = base + c * 32 + lane;
-      u[c] = e < ie ? p.iadj[e] : -1;
+      u[c] = c < nc && e < ie ? p.iadj[e] : -1;
     }
     if (kRelease) __threadfence();  // release: v's dist and level before the counts
+    unsigned ready = 0;  // bit c: this lane's tail of chunk c reached zero
 #pragma unroll
-    for (int c = 0; c < 4; ++c) ready[c] = u[c] >= 0 && atomicSub(&p.deps[u[c]], 1) == 1;
+    for (int c = 0; c < kC; ++c)
+      if (u[c] >= 0 && atomicSub(&p.deps[u[c]], 1) == 1) ready |= 1u << c;
     if (kRelease) __threadfence();
+    // slots: chunk by chunk, lane order within a chunk
+    int total = 0, mine[kC];
 #pragma unroll
-    for (int c = 0; c < 4; ++c) queue_push(p, ready[c], u[c]);
+    for (int c = 0; c < kC; ++c) {
+      const unsigned bal = __ballot_sync(0xffffffffu, (ready >> c) & 1u);
+      mine[c] = total + __popc(bal & lanemask_lt());
+      total += __popc(bal);
+    }
+    if (total == 0) continue;
+    int slot0 = 0;
+    if (lane == 0) slot0 = atomicAdd(&p.ctr->qtail[0][0], total);
+    slot0 = __shfl_sync(0xffffffffu, slot0, 0);
+#pragma unroll
+    for (int c = 0; c < kC; ++c)
+      if ((ready >> c) & 1u) *reinterpret_cast<volatile int*>(p.queue + slot0 + mine[c]) = u[c];
   }
 }
 
@@ -1433,14 +1479,15 @@ sfxt_dataflow_kernel(SfxtParams p) {
   }
   if (lane == 0) atomicMax(&p.ctr->levels, max_lvl + 1);
   if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit)) return;
-  if (p.heap_phase) {
-    const bool ok = heap_phase(p);
-    if (!__syncthreads_and(ok) && threadIdx.x == 0) atomicCAS(&p.ctr->err, kDevOk, kDevTimeout);
-    if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit)) return;
-  }
-  // counting sort by level: histogram (block-local when the levels fit)
+  // Every vertex is built.  What is left: the chain heaps (the heap phase)
+  // and the counting sort by level into order[] / lvlp[].  The sort's level
+  // histogram comes first; block 0 scans it while the others start on the
+  // heaps, and every block scatters its own vertices once its heaps are in,
+  // so the sort costs no grid barrier of its own.
   const int L = *reinterpret_cast<volatile int*>(&p.ctr->levels);
-  if (L <= kSfxtThreads) {
+  const bool small_l = L <= kSfxtThreads;
+  __shared__ int s_base[kSfxtThreads];
+  if (small_l) {
     for (int i = threadIdx.x; i < L; i += blockDim.x) s_hist[i] = 0;
     __syncthreads();
     for (int v = tid; v < p.n; v += nth) atomicAdd(&s_hist[p.level_of[v]], 1);
@@ -1450,38 +1497,94 @@ sfxt_dataflow_kernel(SfxtParams p) {
   } else {
     for (int v = tid; v < p.n; v += nth) atomicAdd(p.lvlp + p.level_of[v] + 1, 1);
   }
-  // the queue is free again: it holds the scatter cursors
-  for (int i = tid; i <= L; i += nth) p.queue[i] = 0;
-  if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit)) return;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(&p.ctr->sort_blocks, 1);
+  }
+  bool ok = true;
   if (blockIdx.x == 0) {
-    // inclusive scan of lvlp[1..L] by one block, kSfxtThreads at a time
-    __shared__ int carry;
-    if (threadIdx.x == 0) carry = 0;
+    // inclusive scan of lvlp[1..L] once every block's histogram is in
+    __shared__ int carry, s_ok;
+    if (threadIdx.x == 0) {
+      carry = 0;
+      unsigned int it = 0;
+      bool w = true;
+      while (*reinterpret_cast<volatile int*>(&p.ctr->sort_blocks) < static_cast<int>(gridDim.x)) {
+        if (++it > p.spin_limit) {
+          atomicCAS(&p.ctr->err, kDevOk, kDevTimeout);
+          w = false;
+          break;
+        }
+        __nanosleep(64);
+      }
+      __threadfence();
+      s_ok = w;
+    }
     __syncthreads();
-    for (int base = 1; base <= L; base += blockDim.x) {
+    ok = s_ok != 0;
+    for (int base = 1; ok && base <= L; base += blockDim.x) {
       const int i = base + threadIdx.x;
-      s_hist[threadIdx.x] = i <= L ? p.lvlp[i] : 0;
+      s_base[threadIdx.x] = i <= L ? __ldcg(p.lvlp + i) : 0;
       __syncthreads();
       for (int o = 1; o < blockDim.x; o <<= 1) {
-        const int y = threadIdx.x >= o ? s_hist[threadIdx.x - o] : 0;
+        const int y = threadIdx.x >= o ? s_base[threadIdx.x - o] : 0;
         __syncthreads();
-        s_hist[threadIdx.x] += y;
+        s_base[threadIdx.x] += y;
         __syncthreads();
       }
-      if (i <= L) p.lvlp[i] = s_hist[threadIdx.x] + carry;
+      if (i <= L) p.lvlp[i] = s_base[threadIdx.x] + carry;
       __syncthreads();
-      if (threadIdx.x == blockDim.x - 1) carry += s_hist[threadIdx.x];
+      if (threadIdx.x == blockDim.x - 1) carry += s_base[threadIdx.x];
       __syncthreads();
     }
-    if (threadIdx.x == 0) {
+    if (threadIdx.x == 0 && ok) {
       p.ctr->sort_beg = 0;
       p.ctr->sort_end = p.n;
+      __threadfence();
+      *reinterpret_cast<volatile int*>(&p.ctr->sort_ready) = 1;
     }
   }
-  if (!grid_sync(&p.ctr->bar, &p.ctr->err, p.spin_limit)) return;
-  for (int v = tid; v < p.n; v += nth) {
-    const int l = p.level_of[v];
-    p.order[__ldcg(p.lvlp + l) + atomicAdd(p.queue + l, 1)] = v;
+  if (p.heap_phase) ok = heap_phase(p) && ok;
+  // scatter this block's vertices by level: one reservation per (block,
+  // level) on the level's cursor (deps[], all zero once every vertex was
+  // queued), then a shared-memory cursor per level
+  __shared__ int s_ready;
+  if (threadIdx.x == 0) {
+    unsigned int it = 0;
+    bool w = true;
+    while (*reinterpret_cast<volatile int*>(&p.ctr->sort_ready) == 0) {
+      if (++it > p.spin_limit ||
+          ((it & 31) == 0 && *reinterpret_cast<volatile int*>(&p.ctr->err) != kDevOk)) {
+        atomicCAS(&p.ctr->err, kDevOk, kDevTimeout);
+        w = false;
+        break;
+      }
+      __nanosleep(64);
+    }
+    __threadfence();
+    s_ready = w;
+  }
+  __syncthreads();
+  if (!__syncthreads_and(ok && s_ready != 0)) {
+    if (threadIdx.x == 0) atomicCAS(&p.ctr->err, kDevOk, kDevTimeout);
+    return;
+  }
+  if (small_l) {
+    for (int i = threadIdx.x; i < L; i += blockDim.x) {
+      s_base[i] = s_hist[i] ? __ldcg(p.lvlp + i) + atomicAdd(p.deps + i, s_hist[i]) : 0;
+      s_hist[i] = 0;
+    }
+    __syncthreads();
+    for (int v = tid; v < p.n; v += nth) {
+      const int l = p.level_of[v];
+      p.order[s_base[l] + atomicAdd(&s_hist[l], 1)] = v;
+    }
+  } else {
+    for (int v = tid; v < p.n; v += nth) {
+      const int l = p.level_of[v];
+      p.order[__ldcg(p.lvlp + l) + atomicAdd(p.deps + l, 1)] = v;
+    }
   }
 }
 

@@ -459,7 +459,8 @@ SfxtParams sfxt_params(cpg_handle* h, int32_t start_level) {
   p.level_sync = h->opts.sfxt_level_sync == 1;
   p.heap_warps = std::min(std::max(h->opts.sfxt_heap_warps, 0), 16);
   p.early_push = h->opts.sfxt_late_push != 1 && p.heap_warps == 0;
-  p.heap_phase = p.heap_warps == 0 && h->opts.sfxt_inline_heaps != 1;
+  p.heap_phase = p.heap_warps > 0 ? 0 : h->opts.sfxt_heap_mode == 1 ? 0
+               : h->opts.sfxt_heap_mode == 2 ? 2 : 1;
   p.dl = P<unsigned long long>(h->d_dl);
   p.orig_id = h->relabeled ? P<int32_t>(h->d_orig_id) : nullptr;
   if (start_level > 0) {
@@ -1024,6 +1025,19 @@ int engine_finish(cpg_handle* h, std::vector<EngineQuery>& qout, EngineCounters&
 // One query through the engine.  Returns kRetry when a bounded buffer
 // overflowed.
 int engine_query(cpg_handle* h, unsigned long long k) {
+  // CTAs of the engine launch: the option, else chosen from K (a small
+  // query's phases are bound by barrier latency, and one CTA's grid barrier
+  // is a block barrier)
+  // (measured on the 20,000-pin and 1M-pin graphs: one CTA is fastest up to
+  // K of about 2,000 -- 0.33 against 0.61 ms at K = 1,000 -- eight around
+  // K = 1e4, then about K / 3,000, up to one per SM at K = 1e6)
+  int ctas = h->opts.engine_ctas;
+  if (ctas <= 0) {
+    if (k <= 2000) ctas = 1;
+    else if (k <= 20000) ctas = 8;
+    else ctas = static_cast<int>(std::min<unsigned long long>(std::max<unsigned long long>(k / 3000, 16), 1u << 20));
+  }
+  h->engine_grid_limit = ctas;  // engine_grid caps it at the co-resident CTAs
   std::vector<EngineQuery> qs(1);
   qs[0].k = static_cast<long long>(k);
   qs[0].src_beg = 0;

@@ -171,8 +171,8 @@ struct SfxtParams {
   int32_t level_sync;
   int32_t heap_warps;      // dataflow: warps per CTA that only insert heaps (0: none)
   int32_t early_push;      // dataflow: push tails before the build, poll dl[]
-  int32_t heap_phase;      // dataflow: chain heaps inserted after every build, not by
-                           // the building warp
+  int32_t heap_phase;      // dataflow: chain heaps inserted after every build instead of
+                           // by the building warp: 0 never, 1 on large graphs, 2 always
   unsigned long long* dl;  // dataflow: published (level << 32 | dist) per vertex
   // Side-by-side graphs relabelled in level order (batched and served forms):
   // the caller's id of each vertex, for the successor tie-break; null when

@@ -92,6 +92,12 @@ __device__ __forceinline__ bool eng_passed(const EngineParams& p) {
 
 __device__ __forceinline__ bool eng_sync(const EngineParams& p) {
   __syncthreads();
+  if (gridDim.x == 1) {
+    // one CTA: the block barrier is the grid barrier
+    if (threadIdx.x == 0) ++s_stage;
+    __syncthreads();
+    return eng_passed(p);
+  }
   if (threadIdx.x == 0) {
     __threadfence();
     const unsigned int old = atomicAdd(&p.ctr->bar.count, 1u);
@@ -108,6 +114,13 @@ __device__ __forceinline__ bool eng_sync_last(const EngineParams& p, F&& f) {
   __shared__ unsigned int s_target;
   __shared__ int s_last;
   __syncthreads();
+  if (gridDim.x == 1) {
+    f();
+    __syncthreads();
+    if (threadIdx.x == 0) ++s_stage;
+    __syncthreads();
+    return eng_passed(p);
+  }
   if (threadIdx.x == 0) {
     __threadfence();
     const unsigned int old = atomicAdd(&p.ctr->bar.count, 1u);
@@ -826,13 +839,17 @@ __device__ bool decide_query(const EngineParams& p, EngineQuery& Q) {
     // little; falling short costs one more phase, which is only worth
     // risking when the overshoot would be large (an extra phase costs
     // about as much as closing ~1e5 more paths).
-    if (p.grow_cap_k && static_cast<unsigned long long>(Q.k) - Q.paths_nz >= (1ull << 17)) {
+    // With fewer than 2^17 paths missing the aim keeps twice the spare
+    // (falling short then costs one more phase, which is cheap against an
+    // overshoot: promoting 4x the accepted count there once closed 8x K).
+    if (p.grow_cap_k) {
       const unsigned long long miss = static_cast<unsigned long long>(Q.k) - Q.paths_nz;
-      unsigned long long aim = miss;
+      const bool far = miss >= (1ull << 17);
+      unsigned long long aim = far ? miss : ~0ull;
       if (Q.last_j > 0 && Q.paths_nz > Q.acc_prev) {
         const double ratio = static_cast<double>(Q.paths_nz - Q.acc_prev) /
                              static_cast<double>(Q.last_j);
-        if (ratio > 1.0) aim = static_cast<unsigned long long>(1.2 * miss / ratio) + 64;
+        if (ratio > 1.0) aim = static_cast<unsigned long long>((far ? 1.2 : 2.0) * miss / ratio) + 64;
       }
       if (j > aim) j = aim;
     }

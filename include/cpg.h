@@ -99,10 +99,13 @@ typedef struct {
   int32_t batch_caller_order; /* batched and served forms: 1 = keep the
                                callers' vertex order instead of renumbering
                                each graph in level order (A/B checks) */
-  int32_t sfxt_inline_heaps; /* dataflow build: 1 = the building warp inserts
-                               each vertex's chain heap right after its build,
-                               instead of a heap phase after every build (A/B
-                               checks) */
+  int32_t sfxt_heap_mode;   /* dataflow build: where chain heaps are inserted.
+                               0 = chosen by size (a heap phase after every
+                               build on large graphs, else by the building
+                               warp right after each build), 1 = always by the
+                               building warp, 2 = always in the heap phase */
+  int32_t engine_ctas;      /* single queries: CTAs of the engine launch
+                               (0 = chosen from k) */
 } cpg_options;
 
 typedef struct cpg_handle cpg_handle;

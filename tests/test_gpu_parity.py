@@ -275,8 +275,8 @@ def test_host_stepped_and_engine_agree(name):
     assert np.array_equal(out[0].view(np.uint32), out[1].view(np.uint32))
 
 
-@pytest.mark.parametrize("mode", ["early_push", "late_push", "heap_warps", "inline_heaps",
-                                  "late_inline_heaps"])
+@pytest.mark.parametrize("mode", ["early_push", "late_push", "heap_warps", "heap_phase",
+                                  "late_heap_phase"])
 @pytest.mark.parametrize("name", ["simple", "tv80_unit_wgts", "single20k_f32", "small_int_s13"])
 def test_dataflow_build_equals_level_sync(name, mode):
     """The default full suffix-tree build (dataflow work queue) and the
@@ -291,7 +291,7 @@ def test_dataflow_build_equals_level_sync(name, mode):
         with cpg_b200.CpGen(division=cpg_b200.DIV_IEEE, frontier=cpg_b200.FRONTIER_CSR,
                             sfxt_level_sync=level_sync,
                             sfxt_heap_warps=4 if mode == "heap_warps" else 0,
-                            sfxt_inline_heaps=mode.endswith("inline_heaps"),
+                            sfxt_heap_mode=2 if mode.endswith("heap_phase") else 0,
                             sfxt_late_push=mode.startswith("late") or mode == "heap_warps") as g:
             g.load_edges(n, src, dst, w)
             g.report_paths(2000)
@@ -393,3 +393,20 @@ def test_path_sets_equal_oracle(name):
     # boundary tie group: distinct paths, as many as the oracle's
     tie = {p for p, c in zip(got_paths, costs) if c == kth}
     assert len(tie) == int(np.count_nonzero(want_costs == kth))
+
+
+@pytest.mark.parametrize("name,k", [("single20k_f32", 1000), ("small_int_s13", 20000),
+                                    ("tv80_unit_wgts", 50000)])
+def test_engine_cta_counts_agree(name, k):
+    """The engine on one CTA (block barriers only), a few CTAs and one per SM
+    returns the same costs (the launch shape is chosen from K by default)."""
+    n, src, dst, w = _load(name)
+    out = []
+    for ctas in (1, 8, 0):
+        with cpg_b200.CpGen(division=cpg_b200.DIV_IEEE, engine_ctas=ctas) as g:
+            g.load_edges(n, src, dst, w)
+            g.report_paths(k)
+            out.append(g.get_slacks(k))
+    want = oracle.OracleGraph.from_edges(n, src, dst, w).closure_topk(k)[0]["slack"]
+    for got in out:
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32))

@@ -35,6 +35,8 @@ struct DevMem {
 };
 
 constexpr unsigned int kDefaultSpinLimit = 1u << 24;
+// single queries: pending items up to which one CTA runs a phase
+constexpr unsigned long long kEngSoloStop = 4096;
 enum { kRetry = 1000 };  // internal: a bounded buffer overflowed, grow and rerun
 constexpr int32_t kMaxRow = 16384;  // longest deviation row the row sort takes
 
@@ -930,7 +932,12 @@ Status engine_prepare(cpg_handle* h, const std::vector<EngineQuery>& qs,
   return CPG_OK;
 }
 
-Status engine_enqueue(cpg_handle* h, int nq, unsigned long long k_total) {
+// solo_stop > 0 (single queries): a one-CTA launch runs the phases while the
+// pending pile holds at most solo_stop items, then the launch on the handle's
+// CTA count resumes where it stopped (or finds the query answered and
+// returns).  *launches receives the number of launches.
+Status engine_enqueue(cpg_handle* h, int nq, unsigned long long k_total,
+                      unsigned long long solo_stop = 0, int* launches = nullptr) {
   cudaStream_t s = h->stream;
   int grid = 0;
   CK(engine_grid(h->device, h->engine_grid_limit, &grid), "engine occupancy");
@@ -988,7 +995,18 @@ Status engine_enqueue(cpg_handle* h, int nq, unsigned long long k_total) {
     p.sel_shift[1] = 10; p.sel_bits[1] = 11;
     p.sel_shift[2] = 0;  p.sel_bits[2] = 10;
   }
+  if (solo_stop > 0 && grid > 1) {
+    EngineParams a = p;
+    a.grid_limit = 1;
+    a.solo_stop = solo_stop;
+    CK(launch_engine(a, h->device, s), "engine launch");
+    p.resume = 1;
+    CK(launch_engine(p, h->device, s), "engine launch");
+    if (launches) *launches = 2;
+    return CPG_OK;
+  }
   CK(launch_engine(p, h->device, s), "engine launch");
+  if (launches) *launches = 1;
   return CPG_OK;
 }
 
@@ -1046,10 +1064,13 @@ int engine_query(cpg_handle* h, unsigned long long k) {
   if (st != CPG_OK) return st;
   cudaStream_t s = h->stream;
   CK(cudaEventRecord(h->ev[2], s), "event");
-  st = engine_enqueue(h, 1, k);
+  // the first phases move a few thousand items at most: one CTA runs them
+  // on block barriers, the full launch takes over once the pile is larger
+  int launches = 0;
+  st = engine_enqueue(h, 1, k, kEngSoloStop, &launches);
   if (st != CPG_OK) return st;
   CK(cudaEventRecord(h->ev[3], s), "event");
-  h->stats.kernel_launches += 1;
+  h->stats.kernel_launches += launches;
   EngineCounters c;
   const int r = engine_finish(h, qs, c, k);
   if (r != CPG_OK) return r;

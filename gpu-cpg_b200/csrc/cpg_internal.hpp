@@ -377,7 +377,9 @@ struct EngineCounters {
   int rounds;
   int phases;
   int sorted_buf;             // which vals[] holds the sorted path indices
-  int pad;
+  int stopped;                // a one-CTA launch stopped at phase res_phase
+  int res_phase, res_pin;     // the phase to resume and which pending pile is in
+  unsigned long long res_paths, res_pend;
   // device time per stage (ns): 0 seed, 1 decide/bookkeeping, 2 select,
   // 3 promote, 4 closure, 5 output select, 6 output sort, 7 emit
   unsigned long long t_ns[8];
@@ -410,6 +412,11 @@ struct EngineParams {
   unsigned int spin_limit;
   int grid_limit;             // persistent CTAs (0: one per co-resident slot)
   int grow_cap_k;             // cap a growth phase's promotion at K - accepted
+  // Two launches for a single query: a one-CTA launch runs the phases while
+  // the pending pile holds at most solo_stop items and stops there (state in
+  // EngineCounters::res_*); the full launch (resume = 1) continues.
+  unsigned long long solo_stop;
+  int resume;
   int sel_passes;             // radix select digit schedule (sum of bits 32)
   int sel_shift[4];
   int sel_bits[4];

@@ -904,20 +904,44 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
   unsigned long long t_last = 0;
   if (threadIdx.x == 0) s_stage = 0;
   if (blockIdx.x == 0 && threadIdx.x == 0) t_last = gtime();
-  // seed roots (pending pile 0)
-  for (int qi = gw; qi < p.nq; qi += nw) seed_query(p, qi);
-  if (!eng_sync_last(p, [&]() { next_phase(p, 0, false); }))
-    return;
-  STAMP(0);
-  int pin = 0;
-  unsigned long long n_pend = *reinterpret_cast<volatile unsigned long long*>(&p.ctr->pend_out);
-  unsigned long long n_paths = 0;
+  int pin = 0, phase0 = 0;
+  unsigned long long n_pend = 0, n_paths = 0;
+  if (p.resume) {
+    // the one-CTA launch before this one either finished the query or
+    // stopped at the top of a phase; an error there ends this launch too
+    if (*reinterpret_cast<volatile int*>(&p.ctr->err) != kDevOk ||
+        !*reinterpret_cast<volatile int*>(&p.ctr->stopped))
+      return;
+    pin = __ldcg(&p.ctr->res_pin);
+    phase0 = __ldcg(&p.ctr->res_phase);
+    n_pend = __ldcg(&p.ctr->res_pend);
+    n_paths = __ldcg(&p.ctr->res_paths);
+  } else {
+    // seed roots (pending pile 0)
+    for (int qi = gw; qi < p.nq; qi += nw) seed_query(p, qi);
+    if (!eng_sync_last(p, [&]() { next_phase(p, 0, false); }))
+      return;
+    STAMP(0);
+    n_pend = *reinterpret_cast<volatile unsigned long long*>(&p.ctr->pend_out);
+  }
 
-  for (int phase = 0;; ++phase) {
+  for (int phase = phase0;; ++phase) {
     const Item* pend = p.pend[pin];
     Item* pend_next = p.pend[pin ^ 1];
     // (per-query counts are kept current by seeding, promotion and closure)
     if (*reinterpret_cast<volatile int*>(&p.ctr->active) == 0) break;
+    if (p.solo_stop && n_pend > p.solo_stop) {
+      // the pile outgrew one CTA: leave the rest to the full launch
+      if (threadIdx.x == 0) {
+        p.ctr->res_pin = pin;
+        p.ctr->res_phase = phase;
+        p.ctr->res_pend = n_pend;
+        p.ctr->res_paths = n_paths;
+        p.ctr->stopped = 1;
+        __threadfence();
+      }
+      return;
+    }
     // C + D. per-query radix select, split and acceptance limit
     if (!run_select(p, n_paths, pend, n_pend, true)) return;
     STAMP(2);

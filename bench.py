@@ -53,10 +53,12 @@ WORKLOAD = "large1m_f32"
 WORKLOAD_DESC = ("levelised DAG, 1,000,000 pins / 200 levels, geometric out-degree mean 20 "
                  "(cap 256), fp32 delays U[0.1,10], 2,000 sources / 2,000 sinks, K=1e6")
 METRIC = "K-paths/sec"
-# DRAM bytes (read + write) per launch of the dominant kernels on this
-# workload, from the ncu captures summarised in profiles/ (the suffix-tree
-# build does not depend on K; the engine's figure is the K = 1e6 capture).
-KERNEL_TRAFFIC = {"sfxt_dataflow_kernel": 1_541_029_120, "engine_kernel": 284_772_352}
+# DRAM bytes (read + write) per query of the dominant kernels on this
+# workload, from the one-pass ncu capture summarised in
+# profiles/sfxt_dataflow_kernel_large400k.md (the suffix-tree build does not
+# depend on K; the engine's figure is its two launches at K = 1e6).
+KERNEL_TRAFFIC = {"sfxt_dataflow_kernel": 705_734_912 + 622_455_808,
+                  "engine_kernel": 736_000 + 105_372_672 + 191_304_704}
 
 
 def peaks():
@@ -934,18 +936,37 @@ def run_ingest(args):
 
 def run_profile_case(args):
     """A short fixed sequence for ncu: one warm-up query, then one query
-    (suffix tree + engine) on the same workload at --k."""
+    (suffix tree + engine) on the same workload at --k.  --profile-pins N
+    scales the workload's generator down to N pins (same levels, degree and
+    delays; sources and sinks in proportion), for captures that must stay
+    small; --form batched runs one warm-up and one measured batched step."""
     import cpg_b200
     import cases
-    c = cases.CASES[WORKLOAD]
-    dag = cpg_b200.generate(cpg_b200.gen_params(**c["gen"]))
+    if args.form == "batched":
+        # the batch with the level-synchronous build, the autotuner's pick
+        dags, ks = batch_workload()
+        with cpg_b200.Batch(sfxt_level_sync=True) as b:
+            for d in dags:
+                b.add_dag(d)
+            b.commit()
+            b.set_queries(list(range(len(dags))), ks)
+            for _ in range(2):
+                b.run(True)
+            print(json.dumps({"profile_case": "batch256", **b.stats()}))
+        return
+    gen = dict(cases.CASES[WORKLOAD]["gen"])
+    if args.profile_pins:
+        side = max(8, gen["n_first"] * args.profile_pins // gen["n_pins"])
+        gen.update(n_pins=args.profile_pins, n_first=side, n_last=side)
+    dag = cpg_b200.generate(cpg_b200.gen_params(**gen))
     with cpg_b200.CpGen() as g:
         g.load_dag(dag)
         for _ in range(2):
             g.levelize()
             g.report_paths(args.k)
         g.sync()
-        print(json.dumps({"profile_case": WORKLOAD, "k": args.k, **g.stats()}))
+        print(json.dumps({"profile_case": WORKLOAD, "pins": gen["n_pins"], "n": dag.n,
+                          "m": dag.m, "k": args.k, **g.stats()}))
 
 
 def main():
@@ -959,6 +980,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-case", action="store_true",
                     help="one warm-up and one measured query only (for ncu)")
+    ap.add_argument("--profile-pins", type=int, default=0,
+                    help="profile case: scale the workload down to this many pins")
     ap.add_argument("--form", default="plain",
                     choices=["plain", "batched", "served", "density", "config1", "bvss", "ingest"])
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",

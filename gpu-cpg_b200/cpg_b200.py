@@ -546,7 +546,7 @@ class Batch:
 
     def __init__(self, device: int = 0, stream: int | None = None,
                  division: int = DIV_REFERENCE, root_seeding: int = ROOTS_REFERENCE,
-                 caller_order: bool = False):
+                 caller_order: bool = False, sfxt_level_sync: bool = False):
         o = Options()
         lib.cpg_options_init(C.byref(o))
         o.device = device
@@ -554,6 +554,7 @@ class Batch:
         o.division = division
         o.root_seeding = root_seeding
         o.batch_caller_order = 1 if caller_order else 0
+        o.sfxt_level_sync = 1 if sfxt_level_sync else 0
         self._b = C.c_void_p()
         st = lib.cpg_batch_create(C.byref(self._b), C.byref(o))
         if st != CPG_OK:

@@ -374,6 +374,10 @@ struct EngineCounters {
   alignas(128) unsigned long long frontier[3];
   alignas(128) unsigned long long pend_out;
   alignas(128) unsigned long long out_total;
+  // single-query output: paths below and at the final split, and the key range
+  alignas(128) unsigned long long out_below;
+  alignas(128) unsigned long long out_at;
+  alignas(128) unsigned int key_min, key_max;
   int rounds;
   int phases;
   int sorted_buf;             // which vals[] holds the sorted path indices

@@ -1008,104 +1008,184 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
     eng_fail(p, kDevCapacity);
     return;
   }
-  // H. per-query counts are current (kept up to date by the closures)
   for (unsigned long long i = tid; i < n_paths; i += nth) p.rank_of[i] = -1;
-  ENG_SYNC();
-  for (unsigned long long qi = tid; qi < static_cast<unsigned long long>(p.nq); qi += nth) {
-    EngineQuery& Q = p.q[qi];
+  // One query: once K non-zero paths were accepted, the final phase's split
+  // T is the K-th cost of the paths and pending items then known, and every
+  // item up to T was accepted with its closure.  Fewer than K accepted paths
+  // cost less than T unless a closure produced a child a few ulps below its
+  // parent's T; so one pass puts the paths below T in the output buffer and
+  // those at T in a side buffer, the first K - (below) of those follow, and
+  // no output select is needed.  (Below T counting K or more falls back to
+  // the select.)  If the paths ran out before K, every one is reported.
+  unsigned int out_lo = 0u, out_hi = 0xffffffffu;  // key range, for the sort
+  bool fast_out = false;
+  if (p.nq == 1) {
+    const EngineQuery& Q = p.q[0];
     const unsigned long long k = static_cast<unsigned long long>(Q.k);
-    Q.k_out = Q.paths_nz < k ? Q.paths_nz : k;
-    Q.mode = Q.k_out > 0 ? 3 : 0;
-    Q.prefix = 0;
-    Q.krem = Q.k_out;
-    Q.out_lt = Q.out_eq = 0;
-  }
-  if (blockIdx.x == 0 && threadIdx.x == 0) p.ctr->sel_paths = 1;
-  ENG_SYNC();
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    unsigned long long acc = 0;
-    for (int qi = 0; qi < p.nq; ++qi) {
-      p.q[qi].out_off = acc;
-      acc += p.q[qi].k_out;
+    const unsigned long long k_out = Q.paths_nz < k ? Q.paths_nz : k;
+    const unsigned kT = Q.paths_nz >= k ? float_key(__ldcg(&Q.t)) : 0xffffffffu;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      p.ctr->key_min = 0xffffffffu;
+      p.ctr->key_max = 0u;
     }
-    p.ctr->out_total = acc;
-  }
-  if (!run_select(p, n_paths, nullptr, 0, false)) return;
-  STAMP(5);
-  const unsigned long long n_out = *reinterpret_cast<volatile unsigned long long*>(&p.ctr->out_total);
-  if (n_out > p.out_cap) {
-    eng_fail(p, kDevCapacity);
-    return;
-  }
-  // J. compaction into per-query segments: keys below the k-th, then the
-  // first ones equal to it
-  {
+    ENG_SYNC();
     const unsigned long long pad = (n_paths + 31) & ~31ull;
+    unsigned kmin = 0xffffffffu, kmax = 0u;
     for (unsigned long long i = tid; i < pad; i += nth) {
       bool lt = false, eq = false;
-      unsigned q = 0, key = 0;
+      unsigned key = 0;
       if (i < n_paths) {
-        q = static_cast<unsigned>(__ldcg(p.pq + i));
         const float c = __ldcg(p.ps.cost + i);
-        const EngineQuery& Q = p.q[q];
-        if (c != 0.0f && __ldcg(&Q.mode) == 3) {
+        if (c != 0.0f) {
           key = float_key(c);
-          const unsigned kth = __ldcg(&Q.prefix);
-          lt = key < kth;
-          eq = key == kth;
+          lt = key < kT;
+          eq = key == kT;
         }
       }
-      const int lane = threadIdx.x & 31;
-      const unsigned ml = __match_any_sync(0xffffffffu, lt ? q : 0xffffffffu);
-      unsigned long long bl = 0;
-      if (lt && (__ffs(ml) - 1) == lane) bl = atomicAdd(&p.q[q].out_lt, static_cast<unsigned long long>(__popc(ml)));
-      bl = __shfl_sync(0xffffffffu, bl, lt ? __ffs(ml) - 1 : lane);
-      const unsigned me = __match_any_sync(0xffffffffu, eq ? q : 0xffffffffu);
-      unsigned long long be = 0;
-      if (eq && (__ffs(me) - 1) == lane) be = atomicAdd(&p.q[q].out_eq, static_cast<unsigned long long>(__popc(me)));
-      be = __shfl_sync(0xffffffffu, be, eq ? __ffs(me) - 1 : lane);
+      const unsigned long long a = warp_append(&p.ctr->out_below, lt);
+      const unsigned long long b = warp_append(&p.ctr->out_at, eq);
+      if (lt && a < k_out) {
+        p.keys[0][a] = key;
+        p.vals[0][a] = static_cast<unsigned>(i);
+        p.qids[0][a] = 0u;
+      }
+      if (eq && b < k_out) p.vals[1][b] = static_cast<unsigned>(i);
       if (lt || eq) {
-        const EngineQuery& Q = p.q[q];
-        const unsigned long long need_eq = __ldcg(&Q.krem);
-        const unsigned long long n_lt = __ldcg(&Q.k_out) - need_eq;
-        const unsigned long long off = __ldcg(&Q.out_off);
-        unsigned long long slot = ~0ull;
-        if (lt) {
-          const unsigned long long r = bl + __popc(ml & lanemask_lt());
-          if (r < n_lt) slot = off + r;
-        } else {
-          const unsigned long long r = be + __popc(me & lanemask_lt());
-          if (r < need_eq) slot = off + n_lt + r;
+        kmin = min(kmin, key);
+        kmax = max(kmax, key);
+      }
+    }
+    kmin = __reduce_min_sync(0xffffffffu, kmin);
+    kmax = __reduce_max_sync(0xffffffffu, kmax);
+    if ((threadIdx.x & 31) == 0 && kmin <= kmax) {
+      atomicMin(&p.ctr->key_min, kmin);
+      atomicMax(&p.ctr->key_max, kmax);
+    }
+    ENG_SYNC();
+    const unsigned long long below = *reinterpret_cast<volatile unsigned long long*>(&p.ctr->out_below);
+    fast_out = below <= k_out;
+    if (fast_out) {
+      const unsigned long long need = k_out - below;
+      for (unsigned long long i = tid; i < need; i += nth) {
+        p.keys[0][below + i] = kT;
+        p.vals[0][below + i] = __ldcg(p.vals[1] + i);
+        p.qids[0][below + i] = 0u;
+      }
+      if (blockIdx.x == 0 && threadIdx.x == 0) {
+        EngineQuery& W = p.q[0];
+        W.k_out = k_out;
+        W.out_off = 0;
+        W.mode = k_out > 0 ? 3 : 0;
+        p.ctr->out_total = k_out;
+      }
+      out_lo = *reinterpret_cast<volatile unsigned int*>(&p.ctr->key_min);
+      out_hi = *reinterpret_cast<volatile unsigned int*>(&p.ctr->key_max);
+      ENG_SYNC();
+    }
+  }
+  if (!fast_out) {
+    // H. per-query counts are current (kept up to date by the closures)
+    ENG_SYNC();
+    for (unsigned long long qi = tid; qi < static_cast<unsigned long long>(p.nq); qi += nth) {
+      EngineQuery& Q = p.q[qi];
+      const unsigned long long k = static_cast<unsigned long long>(Q.k);
+      Q.k_out = Q.paths_nz < k ? Q.paths_nz : k;
+      Q.mode = Q.k_out > 0 ? 3 : 0;
+      Q.prefix = 0;
+      Q.krem = Q.k_out;
+      Q.out_lt = Q.out_eq = 0;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) p.ctr->sel_paths = 1;
+    ENG_SYNC();
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      unsigned long long acc = 0;
+      for (int qi = 0; qi < p.nq; ++qi) {
+        p.q[qi].out_off = acc;
+        acc += p.q[qi].k_out;
+      }
+      p.ctr->out_total = acc;
+    }
+    if (!run_select(p, n_paths, nullptr, 0, false)) return;
+    STAMP(5);
+    const unsigned long long n_out = *reinterpret_cast<volatile unsigned long long*>(&p.ctr->out_total);
+    if (n_out > p.out_cap) {
+      eng_fail(p, kDevCapacity);
+      return;
+    }
+    // J. compaction into per-query segments: keys below the k-th, then the
+    // first ones equal to it
+    {
+      const unsigned long long pad = (n_paths + 31) & ~31ull;
+      for (unsigned long long i = tid; i < pad; i += nth) {
+        bool lt = false, eq = false;
+        unsigned q = 0, key = 0;
+        if (i < n_paths) {
+          q = static_cast<unsigned>(__ldcg(p.pq + i));
+          const float c = __ldcg(p.ps.cost + i);
+          const EngineQuery& Q = p.q[q];
+          if (c != 0.0f && __ldcg(&Q.mode) == 3) {
+            key = float_key(c);
+            const unsigned kth = __ldcg(&Q.prefix);
+            lt = key < kth;
+            eq = key == kth;
+          }
         }
-        if (slot != ~0ull) {
-          p.keys[0][slot] = key;
-          p.qids[0][slot] = q;
-          p.vals[0][slot] = static_cast<unsigned>(i);
+        const int lane = threadIdx.x & 31;
+        const unsigned ml = __match_any_sync(0xffffffffu, lt ? q : 0xffffffffu);
+        unsigned long long bl = 0;
+        if (lt && (__ffs(ml) - 1) == lane) bl = atomicAdd(&p.q[q].out_lt, static_cast<unsigned long long>(__popc(ml)));
+        bl = __shfl_sync(0xffffffffu, bl, lt ? __ffs(ml) - 1 : lane);
+        const unsigned me = __match_any_sync(0xffffffffu, eq ? q : 0xffffffffu);
+        unsigned long long be = 0;
+        if (eq && (__ffs(me) - 1) == lane) be = atomicAdd(&p.q[q].out_eq, static_cast<unsigned long long>(__popc(me)));
+        be = __shfl_sync(0xffffffffu, be, eq ? __ffs(me) - 1 : lane);
+        if (lt || eq) {
+          const EngineQuery& Q = p.q[q];
+          const unsigned long long need_eq = __ldcg(&Q.krem);
+          const unsigned long long n_lt = __ldcg(&Q.k_out) - need_eq;
+          const unsigned long long off = __ldcg(&Q.out_off);
+          unsigned long long slot = ~0ull;
+          if (lt) {
+            const unsigned long long r = bl + __popc(ml & lanemask_lt());
+            if (r < n_lt) slot = off + r;
+          } else {
+            const unsigned long long r = be + __popc(me & lanemask_lt());
+            if (r < need_eq) slot = off + n_lt + r;
+          }
+          if (slot != ~0ull) {
+            p.keys[0][slot] = key;
+            p.qids[0][slot] = q;
+            p.vals[0][slot] = static_cast<unsigned>(i);
+          }
         }
       }
     }
+    ENG_SYNC();
   }
-  ENG_SYNC();
   STAMP(5);
-  // K. stable LSD sort over (query, cost)
+  // K. stable LSD sort over (query, cost); a digit that every key shares
+  // (the keys span out_lo..out_hi) needs no pass
+  const unsigned long long n_sort = *reinterpret_cast<volatile unsigned long long*>(&p.ctr->out_total);
   int src = 0;
   for (int pass = 0; pass < 4; ++pass) {
-    if (!lsd_pass(p, n_out, src, pass * 8, false)) return;
+    const int shift = pass * 8;
+    if (out_lo <= out_hi && (out_lo >> shift) == (out_hi >> shift)) break;
+    if (!lsd_pass(p, n_sort, src, shift, false)) return;
     src ^= 1;
   }
   for (int shift = 0; (p.nq - 1) >> shift; shift += 8) {
-    if (!lsd_pass(p, n_out, src, shift, true)) return;
+    if (!lsd_pass(p, n_sort, src, shift, true)) return;
     src ^= 1;
   }
   STAMP(6);
   // L. ranks within each query's list, then M. emission
-  for (unsigned long long i = tid; i < n_out; i += nth) {
+  for (unsigned long long i = tid; i < n_sort; i += nth) {
     const unsigned q = __ldcg(p.qids[src] + i);
     p.rank_of[__ldcg(p.vals[src] + i)] =
         static_cast<int>(i - __ldcg(&p.q[q].out_off));
   }
   ENG_SYNC();
-  for (unsigned long long i = tid; i < n_out; i += nth) {
+  for (unsigned long long i = tid; i < n_sort; i += nth) {
     const unsigned idx = __ldcg(p.vals[src] + i);
     const float c = __ldcg(p.ps.cost + idx);
     p.out_cost[i] = c;

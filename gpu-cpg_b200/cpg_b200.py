@@ -50,6 +50,7 @@ class Options(C.Structure):
         ("sfxt_level_sync", C.c_int32), ("sfxt_heap_warps", C.c_int32),
         ("sfxt_late_push", C.c_int32), ("batch_caller_order", C.c_int32),
         ("sfxt_heap_mode", C.c_int32), ("engine_ctas", C.c_int32),
+        ("sfxt_claim_sets", C.c_int32),
     ]
 
 
@@ -376,7 +377,8 @@ class CpGen:
                  bvss_tiles: int = TILES_DENSITY, bvss_min_bits: int = 0,
                  bvss_min_slices: int = 0, sfxt_level_sync: bool = False,
                  sfxt_heap_warps: int = 0, sfxt_late_push: bool = False,
-                 sfxt_heap_mode: int = 0, engine_ctas: int = 0):
+                 sfxt_heap_mode: int = 0, engine_ctas: int = 0,
+                 sfxt_claim_sets: int = 0):
         o = Options()
         lib.cpg_options_init(C.byref(o))
         o.device = device
@@ -395,6 +397,7 @@ class CpGen:
         o.sfxt_late_push = 1 if sfxt_late_push else 0
         o.sfxt_heap_mode = sfxt_heap_mode
         o.engine_ctas = engine_ctas
+        o.sfxt_claim_sets = sfxt_claim_sets
         self._h = C.c_void_p()
         st = lib.cpg_create(C.byref(self._h), C.byref(o))
         if st != CPG_OK:

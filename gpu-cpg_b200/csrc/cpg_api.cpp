@@ -464,6 +464,9 @@ SfxtParams sfxt_params(cpg_handle* h, int32_t start_level) {
   p.heap_phase = p.heap_warps > 0 ? 0 : h->opts.sfxt_heap_mode == 1 ? 0
                : h->opts.sfxt_heap_mode == 2 ? 2 : 1;
   p.dl = P<unsigned long long>(h->d_dl);
+  p.claim_sets = h->opts.sfxt_claim_sets < 0 ? 0
+               : h->opts.sfxt_claim_sets == 0 ? kDefaultClaimSets
+               : std::min(h->opts.sfxt_claim_sets, kMaxClaimSets);
   p.orig_id = h->relabeled ? P<int32_t>(h->d_orig_id) : nullptr;
   if (start_level > 0) {
     // a dataflow build allocates heap nodes out of level order, so rebuilt

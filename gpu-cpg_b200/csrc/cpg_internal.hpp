@@ -108,6 +108,9 @@ enum DevErr : int {
 // Hot words sit on their own 128-byte lines: queue appends, the heap-pool
 // cursor, the status word that waiting warps poll and the barrier do not
 // contend for one L2 line.
+constexpr int kMaxClaimSets = 16;
+constexpr int kDefaultClaimSets = 8;
+
 struct SfxtCounters {
   alignas(128) int tail;     // order[] / queue[] append cursor
   int act_n;                 // BVSS: act_list append cursor
@@ -121,12 +124,18 @@ struct SfxtCounters {
   alignas(128) int n_long;   // rows left for the row-sort pass (long_rows[])
   // dataflow build: append cursors of the kSfxtQueues work queues, one line each
   alignas(128) int qtail[8][32];
+  // dataflow build with claimed slots: claim[q][0] hands out the slots of
+  // claim set q (slots q, q + S, q + 2S, ... for S = claim_sets)
+  alignas(128) int claim[kMaxClaimSets][32];
   alignas(128) int sort_blocks;  // dataflow build: blocks whose level histogram is in
   int sort_ready;                // ... and the level offsets are scanned
   alignas(128) unsigned long long vss_tensor;  // BVSS tiles counted on the tensor cores
   unsigned long long vss_scalar;               // ... and with scalar popc
   alignas(128) GridBarrier bar;
 };
+
+// read back whole into the handle's 4 KiB pinned staging
+static_assert(sizeof(SfxtCounters) <= 4096, "SfxtCounters outgrew the pinned staging");
 
 struct SfxtParams {
   int32_t n;
@@ -174,6 +183,8 @@ struct SfxtParams {
   int32_t heap_phase;      // dataflow: chain heaps inserted after every build instead of
                            // by the building warp: 0 never, 1 on large graphs, 2 always
   unsigned long long* dl;  // dataflow: published (level << 32 | dist) per vertex
+  int32_t claim_sets;      // dataflow: 0 = build warp w takes queue slots w, w + W, ...;
+                           // S > 0 = a free warp claims the next slot of its claim set
   // Side-by-side graphs relabelled in level order (batched and served forms):
   // the caller's id of each vertex, for the successor tie-break; null when
   // the ids are the caller's

@@ -1393,6 +1393,38 @@ __device__ __forceinline__ void dataflow_push(const SfxtParams& p, int v) {
   }
 }
 
+// One taken queue slot of the dataflow build: v's Kahn push and build (in
+// either order), then its chain-heap insert unless the heap phase or the heap
+// workers do it.  False when a wait ran out (warp-uniform).
+__device__ __forceinline__ bool dataflow_slot(const SfxtParams& p, int v, bool hp,
+                                              int heap_warps, unsigned long long* chunk,
+                                              int& max_lvl) {
+  const int lane = threadIdx.x & 31;
+  if (p.early_push) {
+    // the tails learn of v before it is built; they wait on its word
+    dataflow_push<false>(p, v);
+    const int lvl = build_vertex_polled(p, v);
+    if (lvl < 0) return false;
+    max_lvl = max(max_lvl, lvl);
+    if (!hp && lane == 0 && wait_heap(p, __ldcg(p.succ + v)))
+      heap_insert<true>(p, v, chunk);
+    __syncwarp();
+    return true;
+  }
+  const int lvl = build_vertex<true>(p, v, 0, false);
+  max_lvl = max(max_lvl, lvl);
+  __syncwarp();
+  if (heap_warps > 0 && lane == 0) {  // publish the build for the heap workers
+    __threadfence();
+    *reinterpret_cast<volatile int*>(p.order + v) = 1;
+  }
+  dataflow_push<true>(p, v);
+  if (heap_warps == 0 && !hp && lane == 0 && wait_heap(p, __ldcg(p.succ + v)))
+    heap_insert<true>(p, v, chunk);
+  __syncwarp();
+  return true;
+}
+
 __global__ void __launch_bounds__(kSfxtThreads)
 sfxt_dataflow_kernel(SfxtParams p) {
   __shared__ int s_hist[kSfxtThreads];
@@ -1437,38 +1469,33 @@ sfxt_dataflow_kernel(SfxtParams p) {
   const bool hp = p.heap_phase == 2 ||
                   (p.heap_phase == 1 && p.n >= 128 * static_cast<int>(gridDim.x) * build_warps);
   if (wib < build_warps) {
-    // build warp bw serves queue bw % kSfxtQueues, taking every nwq-th slot
     const int nbw = gridDim.x * build_warps;
     const int bw = blockIdx.x * build_warps + wib;
-    const int q = bw % kSfxtQueues;
+    // Claimed slots (claim_sets S > 0): a free warp claims the next slot of
+    // its claim set (slots q, q + S, ...), so a slot that fills while some
+    // warp is still building waits for nobody: any idle warp of the set
+    // takes it.  The S counters spread the claims (one atomic per vertex).
+    // Static slots (S = 0): build warp bw serves queue bw % kSfxtQueues,
+    // taking every nwq-th slot.
+    const int S = p.claim_sets;
+    const int q = S > 0 ? bw % S : bw % kSfxtQueues;
+    const int cnt = S > 0 ? (p.n > q ? (p.n - 1 - q) / S + 1 : 0) : queue_count(p, q);
     const int nwq = (nbw - q + kSfxtQueues - 1) / kSfxtQueues;
-    const int cnt_q = queue_count(p, q);
     const int seg0 = q * queue_seg(p);
-    for (int k = bw / kSfxtQueues; k < cnt_q; k += nwq) {
-      const int v = wait_slot(p, seg0 + k, !p.early_push);
-      if (v < 0) break;
-      if (p.early_push) {
-        // the tails learn of v before it is built; they wait on its word
-        dataflow_push<false>(p, v);
-        const int lvl = build_vertex_polled(p, v);
-        if (lvl < 0) break;
-        max_lvl = max(max_lvl, lvl);
-        if (!hp && lane == 0 && wait_heap(p, __ldcg(p.succ + v)))
-          heap_insert<true>(p, v, chunk);
-        __syncwarp();
-        continue;
+    for (int k = bw / kSfxtQueues;; k += nwq) {
+      int slot;
+      if (S > 0) {
+        int t = 0;
+        if (lane == 0) t = atomicAdd(&p.ctr->claim[q][0], 1);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t >= cnt) break;
+        slot = t * S + q;
+      } else {
+        if (k >= cnt) break;
+        slot = seg0 + k;
       }
-      const int lvl = build_vertex<true>(p, v, 0, false);
-      max_lvl = max(max_lvl, lvl);
-      __syncwarp();
-      if (heap_warps > 0 && lane == 0) {  // publish the build for the heap workers
-        __threadfence();
-        *reinterpret_cast<volatile int*>(p.order + v) = 1;
-      }
-      dataflow_push<true>(p, v);
-      if (heap_warps == 0 && !hp && lane == 0 && wait_heap(p, __ldcg(p.succ + v)))
-        heap_insert<true>(p, v, chunk);
-      __syncwarp();
+      const int v = wait_slot(p, slot, !p.early_push);
+      if (v < 0 || !dataflow_slot(p, v, hp, heap_warps, chunk, max_lvl)) break;
     }
   } else {
     const int nhl = gridDim.x * heap_warps * 32;
@@ -1800,15 +1827,22 @@ namespace {
 __global__ void init_sfxt_counters_kernel(SfxtCounters* c,
                                           const unsigned long long* pool_mark,
                                           int start_level, int append_pool) {
-  SfxtCounters z{};
-  if (start_level > 0) z.hnode_used = append_pool ? c->hnode_used : pool_mark[start_level];
-  *c = z;
+  static_assert(sizeof(SfxtCounters) % 4 == 0, "counters are cleared as ints");
+  __shared__ unsigned long long used;
+  if (threadIdx.x == 0)
+    used = start_level > 0 ? (append_pool ? c->hnode_used : pool_mark[start_level]) : 0ull;
+  __syncthreads();
+  int* w = reinterpret_cast<int*>(c);
+  for (int i = threadIdx.x; i < static_cast<int>(sizeof(SfxtCounters) / 4); i += blockDim.x)
+    w[i] = 0;
+  __syncthreads();
+  if (threadIdx.x == 0) c->hnode_used = used;
 }
 }  // namespace
 
 int launch_init_sfxt_counters(SfxtCounters* c, const unsigned long long* pool_mark,
                               int start_level, int append_pool, void* stream) {
-  init_sfxt_counters_kernel<<<1, 1, 0, static_cast<cudaStream_t>(stream)>>>(
+  init_sfxt_counters_kernel<<<1, 256, 0, static_cast<cudaStream_t>(stream)>>>(
       c, pool_mark, start_level, append_pool);
   return cudaGetLastError();
 }

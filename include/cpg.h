@@ -106,6 +106,12 @@ typedef struct {
                                building warp, 2 = always in the heap phase */
   int32_t engine_ctas;      /* single queries: CTAs of the engine launch
                                (0 = chosen from k) */
+  int32_t sfxt_claim_sets;  /* dataflow build: how warps take work-queue
+                               slots.  0 = default (claimed, 8 sets), -1 =
+                               static (warp w takes slots w, w + W, ...; A/B
+                               checks), 1..16 = a free warp claims the next
+                               slot of its set, the slots dealt round-robin
+                               over that many sets */
 } cpg_options;
 
 typedef struct cpg_handle cpg_handle;

@@ -276,7 +276,8 @@ def test_host_stepped_and_engine_agree(name):
 
 
 @pytest.mark.parametrize("mode", ["early_push", "late_push", "heap_warps", "heap_phase",
-                                  "late_heap_phase"])
+                                  "late_heap_phase", "static_slots", "claim1", "claim16",
+                                  "late_static_slots"])
 @pytest.mark.parametrize("name", ["simple", "tv80_unit_wgts", "single20k_f32", "small_int_s13"])
 def test_dataflow_build_equals_level_sync(name, mode):
     """The default full suffix-tree build (dataflow work queue) and the
@@ -292,7 +293,9 @@ def test_dataflow_build_equals_level_sync(name, mode):
                             sfxt_level_sync=level_sync,
                             sfxt_heap_warps=4 if mode == "heap_warps" else 0,
                             sfxt_heap_mode=2 if mode.endswith("heap_phase") else 0,
-                            sfxt_late_push=mode.startswith("late") or mode == "heap_warps") as g:
+                            sfxt_late_push=mode.startswith("late") or mode == "heap_warps",
+                            sfxt_claim_sets={"claim1": 1, "claim16": 16}.get(
+                                mode, -1 if mode.endswith("static_slots") else 0)) as g:
             g.load_edges(n, src, dst, w)
             g.report_paths(2000)
             first = (g.get_sfxt(), g.get_slacks(2000), g.num_levels())

@@ -35,6 +35,8 @@ struct DevMem {
 };
 
 constexpr unsigned int kDefaultSpinLimit = 1u << 24;
+// the handle's pinned staging of counters and small tables
+constexpr size_t kPinnedBytes = 4096;
 // single queries: pending items up to which one CTA runs a phase
 constexpr unsigned long long kEngSoloStop = 4096;
 enum { kRetry = 1000 };  // internal: a bounded buffer overflowed, grow and rerun
@@ -51,6 +53,7 @@ struct cpg_handle {
 
   // graph
   bool has_graph = false;
+  bool build_pending = false;  // cpg_load_csr: the device graph build is left to the first use
   HostGraph g;          // n, m and the fan-out row offsets only
   int32_t n_srcs = 0;
   int32_t max_outdeg = 0;
@@ -277,8 +280,14 @@ Status setup_bvss(cpg_handle* h, int32_t n, const int32_t* adjp, const int32_t* 
 
 // Upload a fan-out CSR and build the rest of the graph on the device: edge
 // words, fan-in CSR and source list.  The host keeps only the row offsets.
+Status finish_graph(cpg_handle* h);
+
+// Uploads a fan-out CSR and builds the device graph from it.  defer: return
+// once the copies have read the caller's buffers and leave the build to the
+// graph's first use (ready_graph), so that a caller streaming uploads through
+// several handles overlaps this one's copies with another's query.
 Status upload_graph(cpg_handle* h, int32_t n, int32_t m, const int32_t* adjp,
-                    const int32_t* adj, const float* w) {
+                    const int32_t* adj, const float* w, bool defer = false) {
   if (n < 0 || m < 0 || !adjp || (m > 0 && (!adj || !w)))
     return fail(h, CPG_ERR_INVALID, "null CSR buffer");
   if (adjp[0] != 0 || adjp[n] != m)
@@ -296,7 +305,6 @@ Status upload_graph(cpg_handle* h, int32_t n, int32_t m, const int32_t* adjp,
   CK(ensure(h->d_iadjp, (nn + 1) * 4), "alloc iadjp");
   CK(ensure(h->d_iadj, mm * 4), "alloc iadj");
   CK(ensure(h->d_srcs, nn * 4 + 8), "alloc srcs");
-  CK(ensure(h->d_big_off, nn * 4), "alloc big_off");
   // suffix tree storage (the deviation array doubles as upload staging)
   CK(ensure(h->d_order, nn * 4), "alloc order");
   CK(ensure(h->d_queue, (nn + 64) * 4), "alloc queue");
@@ -365,11 +373,10 @@ Status upload_graph(cpg_handle* h, int32_t n, int32_t m, const int32_t* adjp,
   int64_t big_total = 0;
   int32_t big_cap = 1;
   if (max_deg > kSmemRow) {
-    big_off.assign(nn, -1);
     for (int32_t v = 0; v < n; ++v) {
       const int32_t od = adjp[v + 1] - adjp[v];
       if (od > kSmemRow) {
-        big_off[v] = static_cast<int32_t>(big_total);
+        big_off.push_back(static_cast<int32_t>(big_total));  // big_tmp offset of row i
         big_total += od;
         big_rows.push_back(v);
         while (big_cap < od) big_cap <<= 1;
@@ -382,11 +389,36 @@ Status upload_graph(cpg_handle* h, int32_t n, int32_t m, const int32_t* adjp,
   CK(ensure(h->d_big_rows, big_rows.size() * 4), "alloc big rows");
   CK(ensure(h->d_big_tmp, static_cast<size_t>(big_total) * sizeof(DevSidetrack)),
      "alloc big rows");
+  CK(ensure(h->d_big_off, big_rows.size() * 4), "alloc big_off");
   if (!big_rows.empty()) {
-    // only the long rows' offsets are ever read
-    CK(cudaMemcpyAsync(h->d_big_off.p, big_off.data(), nn * 4, cudaMemcpyHostToDevice, s), "H2D big_off");
+    CK(cudaMemcpyAsync(h->d_big_off.p, big_off.data(), big_off.size() * 4, cudaMemcpyHostToDevice, s), "H2D big_off");
     CK(cudaMemcpyAsync(h->d_big_rows.p, big_rows.data(), big_rows.size() * 4, cudaMemcpyHostToDevice, s), "H2D big rows");
   }
+  h->has_graph = true;
+  h->sfxt_valid = false;
+  h->h_sfxt_cached = false;
+  h->h_levels_cached = false;
+  h->dirty_level = -1;
+  h->result_valid = false;
+  h->n_result = 0;
+  if (defer) {
+    // the copies read the caller's buffers (and big_off / big_rows above)
+    CK(cudaStreamSynchronize(s), "upload");
+    h->build_pending = true;
+    return CPG_OK;
+  }
+  return finish_graph(h);
+}
+
+// The device graph build of an upload (edge words, fan-in CSR, sources) from
+// the staged adjacency and delays, and the head range check.
+Status finish_graph(cpg_handle* h) {
+  h->build_pending = false;
+  const int32_t n = h->g.n, m = h->g.m;
+  const size_t nn = static_cast<size_t>(n), mm = static_cast<size_t>(m);
+  cudaStream_t s = h->stream;
+  int32_t* stage_adj = reinterpret_cast<int32_t*>(h->d_dev.p);
+  float* stage_w = reinterpret_cast<float*>(stage_adj + mm);
   int32_t* nsrc_dev = P<int32_t>(h->d_srcs) + nn;
   CK(launch_build_graph(P<int32_t>(h->d_adjp), stage_adj, stage_w, n, m,
                         P<DevEdge>(h->d_edges), P<int32_t>(h->d_iadjp),
@@ -395,7 +427,10 @@ Status upload_graph(cpg_handle* h, int32_t n, int32_t m, const int32_t* adjp,
   int32_t* hn = static_cast<int32_t*>(h->pinned);
   CK(cudaMemcpyAsync(hn, nsrc_dev, 8, cudaMemcpyDeviceToHost, s), "D2H sources");
   CK(cudaStreamSynchronize(s), "upload");
-  if (hn[1] != 0) return fail(h, CPG_ERR_INVALID, "edge head out of range");
+  if (hn[1] != 0) {
+    h->has_graph = false;
+    return fail(h, CPG_ERR_INVALID, "edge head out of range");
+  }
   h->n_srcs = *hn;
   // sources in vertex-id order, as the reference's _srcs list (gpucpg.cu:
   // 531-533): G-PathGen's root seeding keeps the first roots in that order
@@ -405,14 +440,16 @@ Status upload_graph(cpg_handle* h, int32_t n, int32_t m, const int32_t* adjp,
     std::sort(srcs.begin(), srcs.end());
     CK(cudaMemcpy(h->d_srcs.p, srcs.data(), srcs.size() * 4, cudaMemcpyHostToDevice), "H2D sources");
   }
-  h->has_graph = true;
-  h->sfxt_valid = false;
-  h->h_sfxt_cached = false;
-  h->h_levels_cached = false;
-  h->dirty_level = -1;
-  h->result_valid = false;
-  h->n_result = 0;
   return CPG_OK;
+}
+
+// A loaded graph, built on the device (the build of a deferred upload runs
+// here, on the handle's stream).
+Status ready_graph(cpg_handle* h) {
+  if (!h->has_graph) return fail(h, CPG_ERR_STATE, "no graph loaded");
+  if (!h->build_pending) return CPG_OK;
+  CK(cudaSetDevice(h->device), "cudaSetDevice");
+  return finish_graph(h);
 }
 
 Status load_edgelist(cpg_handle* h, const EdgeList& el) {
@@ -608,7 +645,10 @@ Status ensure_levels_host(cpg_handle* h) {
 }
 
 Status ensure_sfxt(cpg_handle* h) {
-  if (!h->has_graph) return fail(h, CPG_ERR_STATE, "no graph loaded");
+  {
+    Status st = ready_graph(h);
+    if (st != CPG_OK) return st;
+  }
   if (h->sfxt_valid) return CPG_OK;
   if (h->dirty_level > 0 && h->levels > 0)
     return run_sfxt(h, h->dirty_level);
@@ -929,6 +969,12 @@ Status engine_prepare(cpg_handle* h, const std::vector<EngineQuery>& qs,
   CK(ensure_grow(h->d_esort, (256 * static_cast<size_t>(grid) + 256) * 4), "alloc sort");
   CK(ensure_grow(h->d_equery, nq * sizeof(EngineQuery)), "alloc queries");
   CK(ensure_grow(h->d_ectr, sizeof(EngineCounters)), "alloc counters");
+  if (nq <= static_cast<size_t>(kInlineQueries)) {
+    // no host-to-device copy: a large upload on another stream would hold it
+    CK(launch_set_queries(P<EngineQuery>(h->d_equery), qs.data(), static_cast<int>(nq), h->stream),
+       "queries");
+    return CPG_OK;
+  }
   CK(cudaMemcpyAsync(h->d_equery.p, qs.data(), nq * sizeof(EngineQuery),
                      cudaMemcpyHostToDevice, h->stream), "H2D queries");
   CK(cudaStreamSynchronize(h->stream), "H2D queries");
@@ -1018,8 +1064,14 @@ int engine_finish(cpg_handle* h, std::vector<EngineQuery>& qout, EngineCounters&
                   unsigned long long k_total) {
   const size_t nq = qout.size();
   char* hb = static_cast<char*>(h->pinned);
+  // a few queries' table comes back with the counters, in one pinned copy
+  constexpr size_t kQoff = (sizeof(EngineCounters) + 127) & ~size_t{127};
+  const bool inline_q = kQoff + nq * sizeof(EngineQuery) <= kPinnedBytes;
   CK(cudaMemcpyAsync(hb, h->d_ectr.p, sizeof(EngineCounters), cudaMemcpyDeviceToHost,
                      h->stream), "D2H counters");
+  if (inline_q)
+    CK(cudaMemcpyAsync(hb + kQoff, h->d_equery.p, nq * sizeof(EngineQuery),
+                       cudaMemcpyDeviceToHost, h->stream), "D2H queries");
   CK(cudaStreamSynchronize(h->stream), "engine");
   std::memcpy(&c, hb, sizeof(c));
   if (c.err == kDevTimeout)
@@ -1030,8 +1082,11 @@ int engine_finish(cpg_handle* h, std::vector<EngineQuery>& qout, EngineCounters&
     h->overflow_pend = c.pend_out;
     return kRetry;
   }
-  CK(cudaMemcpy(qout.data(), h->d_equery.p, nq * sizeof(EngineQuery), cudaMemcpyDeviceToHost),
-     "D2H queries");
+  if (inline_q)
+    std::memcpy(qout.data(), hb + kQoff, nq * sizeof(EngineQuery));
+  else
+    CK(cudaMemcpy(qout.data(), h->d_equery.p, nq * sizeof(EngineQuery), cudaMemcpyDeviceToHost),
+       "D2H queries");
   h->stats.paths_accepted = static_cast<int64_t>(c.paths);
   h->stats.items_generated = static_cast<int64_t>(c.paths + c.pend_out);
   h->stats.pending_peak = static_cast<int64_t>(c.pend_out);
@@ -1164,7 +1219,7 @@ cpg_status cpg_create(cpg_handle** out, const cpg_options* opts) {
     }
     h->own_stream = true;
   }
-  if (cudaMallocHost(&h->pinned, 4096) != cudaSuccess) {
+  if (cudaMallocHost(&h->pinned, kPinnedBytes) != cudaSuccess) {
     if (h->own_stream) cudaStreamDestroy(h->stream);
     delete h;
     return CPG_ERR_OOM;
@@ -1256,7 +1311,7 @@ cpg_status cpg_load_csr(cpg_handle* h, int32_t n, int32_t m,
                         const int32_t* adjp, const int32_t* adjncy,
                         const float* w) {
   if (check_handle(h) != CPG_OK) return CPG_ERR_INVALID;
-  return upload_graph(h, n, m, adjp, adjncy, w);
+  return upload_graph(h, n, m, adjp, adjncy, w, true);
 }
 
 int64_t cpg_num_verts(const cpg_handle* h) { return h && h->has_graph ? h->g.n : 0; }
@@ -1267,6 +1322,10 @@ cpg_status cpg_get_csr(const cpg_handle* hc, int32_t* adjp, int32_t* adjncy,
   cpg_handle* h = const_cast<cpg_handle*>(hc);
   if (!h) return CPG_ERR_INVALID;
   if (!h->has_graph) return CPG_ERR_STATE;
+  {
+    Status st = ready_graph(h);
+    if (st != CPG_OK) return st;
+  }
   if (adjp) std::memcpy(adjp, h->g.adjp.data(), (h->g.n + 1) * 4);
   if ((adjncy || w) && h->g.m) {
     std::vector<DevEdge> e(h->g.m);
@@ -1301,7 +1360,10 @@ void cpg_debug_fail_allocs_above(int64_t max_bytes) {
 cpg_status cpg_update_delays(cpg_handle* h, int64_t count, const int32_t* eids,
                              const float* w) {
   if (check_handle(h) != CPG_OK || count < 0) return CPG_ERR_INVALID;
-  if (!h->has_graph) return fail(h, CPG_ERR_STATE, "no graph loaded");
+  {
+    Status st = ready_graph(h);
+    if (st != CPG_OK) return st;
+  }
   if (count == 0) return CPG_OK;
   if (!eids || !w) return fail(h, CPG_ERR_INVALID, "null delay buffer");
   CK(cudaSetDevice(h->device), "cudaSetDevice");

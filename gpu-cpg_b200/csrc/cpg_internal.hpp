@@ -157,7 +157,7 @@ struct SfxtParams {
   unsigned long long hnode_cap;
   unsigned long long* pool_mark;  // per level: heap nodes in use at its start
   int32_t* deps;
-  const int32_t* big_off;  // scratch offset of rows longer than kSmemRow
+  const int32_t* big_off;  // big_tmp offset of big_rows[i]
   DevSidetrack* big_tmp;
   const int32_t* big_rows; // vertices with more than kSmemRow fan-out edges
   int32_t n_big_rows;
@@ -441,6 +441,8 @@ struct EngineParams {
 // host sizes sort_hist as 256 * grid) for a given CTA limit (0: maximum).
 int engine_grid(int device, int limit, int* grid_out);
 int launch_engine(const EngineParams& p, int device, void* stream);
+constexpr int kInlineQueries = 8;
+int launch_set_queries(EngineQuery* dst, const EngineQuery* src, int nq, void* stream);
 
 // ---------------------------------------------------------------- select/sort
 size_t select_state_bytes();

@@ -1221,6 +1221,27 @@ int engine_grid(int device, int limit, int* grid_out) {
   return cudaSuccess;
 }
 
+namespace {
+// A few queries' table, passed by value to the kernel that writes it.
+struct QueryTable {
+  EngineQuery q[kInlineQueries];
+};
+__global__ void set_queries_kernel(EngineQuery* dst, QueryTable t, int nq) {
+  if (static_cast<int>(threadIdx.x) < nq) dst[threadIdx.x] = t.q[threadIdx.x];
+}
+}  // namespace
+
+// Writes up to kInlineQueries queries' table from the launch parameters, so
+// a query starts without a host-to-device copy (which would wait behind any
+// large upload another stream has on the copy engine).
+int launch_set_queries(EngineQuery* dst, const EngineQuery* src, int nq, void* stream) {
+  if (nq < 1 || nq > kInlineQueries) return cudaErrorInvalidValue;
+  QueryTable t{};
+  for (int i = 0; i < nq; ++i) t.q[i] = src[i];
+  set_queries_kernel<<<1, kInlineQueries, 0, static_cast<cudaStream_t>(stream)>>>(dst, t, nq);
+  return cudaGetLastError();
+}
+
 int launch_engine(const EngineParams& p, int device, void* stream) {
   int grid = 0;
   cudaError_t e = static_cast<cudaError_t>(engine_grid(device, p.grid_limit, &grid));

@@ -11,29 +11,24 @@ namespace {
 
 constexpr int kScanTile = 2048;
 
-__global__ void interleave_kernel(const int32_t* adj, const float* w, int64_t m,
-                                  DevEdge* out) {
+// The (head, delay) edge words and the in-degree histogram in one pass over
+// the heads.  Also validates the heads: one outside [0, n) sets *bad and is
+// skipped, so the host learns of it after the build without an O(M) host
+// pass.
+__global__ void interleave_indegree_kernel(const int32_t* adj, const float* w, int64_t m,
+                                           int32_t n, DevEdge* out, int32_t* indeg,
+                                           int32_t* bad) {
   for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < m;
        e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     DevEdge d;
     d.head = adj[e];
     d.w = w[e];
     out[e] = d;
-  }
-}
-
-// Also validates the heads: one outside [0, n) sets *bad and is skipped, so
-// the host learns of it after the build without an O(M) host pass.
-__global__ void indegree_kernel(const int32_t* adj, int64_t m, int32_t n, int32_t* indeg,
-                                int32_t* bad) {
-  for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < m;
-       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int h = adj[e];
-    if (static_cast<unsigned>(h) >= static_cast<unsigned>(n)) {
+    if (static_cast<unsigned>(d.head) >= static_cast<unsigned>(n)) {
       *bad = 1;
       continue;
     }
-    atomicAdd(&indeg[h], 1);
+    atomicAdd(&indeg[d.head], 1);
   }
 }
 
@@ -55,16 +50,42 @@ __global__ void tile_sum_kernel(const int32_t* x, int64_t n, int32_t* sums) {
   }
 }
 
-__global__ void scan_sums_kernel(int32_t* sums, int n) {
-  if (threadIdx.x == 0) {
-    int32_t acc = 0;
-    for (int i = 0; i < n; ++i) {
-      const int32_t v = sums[i];
-      sums[i] = acc;
-      acc += v;
+// exclusive scan of the tile sums in place (one CTA of 1024), sums[n] = total
+__global__ void __launch_bounds__(1024) scan_sums_kernel(int32_t* sums, int n) {
+  __shared__ int32_t wsum[32];
+  __shared__ int32_t carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int b0 = 0; b0 < n; b0 += blockDim.x) {
+    const int i = b0 + threadIdx.x;
+    const int32_t v = i < n ? sums[i] : 0;
+    int32_t incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
     }
-    sums[n] = acc;
+    if (lane == 31) wsum[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+      const int32_t a = wsum[lane];
+      int32_t y = a;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int32_t z = __shfl_up_sync(0xffffffffu, y, o);
+        if (lane >= o) y += z;
+      }
+      wsum[lane] = y - a;
+    }
+    __syncthreads();
+    const int32_t c0 = carry;
+    if (i < n) sums[i] = c0 + wsum[wid] + incl - v;
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) carry = c0 + wsum[wid] + incl;
+    __syncthreads();
   }
+  if (threadIdx.x == 0) sums[n] = carry;
 }
 
 __global__ void tile_scan_kernel(const int32_t* x, int64_t n, const int32_t* sums,
@@ -163,13 +184,12 @@ int launch_build_graph(const int32_t* adjp, const int32_t* adj, const float* w,
   const int ntiles = static_cast<int>((static_cast<int64_t>(n) + kScanTile - 1) / kScanTile);
   cudaMemsetAsync(indeg, 0, static_cast<size_t>(n) * 4, s);
   cudaMemsetAsync(n_srcs, 0, 8, s);  // source count, bad-head flag
-  if (m > 0) {
-    interleave_kernel<<<grid_of(m, 256), 256, 0, s>>>(adj, w, m, edges);
-    indegree_kernel<<<grid_of(m, 256), 256, 0, s>>>(adj, m, n, indeg, n_srcs + 1);
-  }
+  if (m > 0)
+    interleave_indegree_kernel<<<grid_of(m, 256), 256, 0, s>>>(adj, w, m, n, edges, indeg,
+                                                               n_srcs + 1);
   if (n > 0) {
     tile_sum_kernel<<<ntiles, 256, 0, s>>>(indeg, n, sums);
-    scan_sums_kernel<<<1, 32, 0, s>>>(sums, ntiles);
+    scan_sums_kernel<<<1, 1024, 0, s>>>(sums, ntiles);
     tile_scan_kernel<<<ntiles, 256, 0, s>>>(indeg, n, sums, iadjp);
     set_last_kernel<<<1, 1, 0, s>>>(iadjp, n, sums, ntiles);
     sources_kernel<<<grid_of(n, 256), 256, 0, s>>>(indeg, n, srcs, n_srcs);

@@ -1711,7 +1711,7 @@ __global__ void sort_big_rows_kernel(const int32_t* rows, const int32_t* adjp,
   if (cnt <= kSmemRow) return;
   if (vgraph && level_of[v] < graph_from[vgraph[v]]) return;  // not rebuilt
   DevSidetrack* row = dev + adjp[v];
-  DevSidetrack* tmp = big_tmp + big_off[v];
+  DevSidetrack* tmp = big_tmp + big_off[blockIdx.x];
   int n2 = 1;
   while (n2 < cnt) n2 <<= 1;
   if (n2 > cap) n2 = cap;  // host guarantees cnt <= cap

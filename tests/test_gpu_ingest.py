@@ -57,3 +57,34 @@ def test_bad_csr_bin_leaves_handle_usable(tmp_path):
                      np.array([1.0, 2.0, 3.0], np.float32))
         g.report_paths(3)
         assert np.allclose(g.get_slacks(3), [2.0, 4.0])
+
+
+def test_load_csr_builds_on_first_use_and_checks_heads():
+    """cpg_load_csr returns once its copies have read the caller's buffers;
+    the device graph is built by the first call that uses it.  The buffers
+    may be overwritten right after the load, and a head out of range is
+    reported by that first call, after which the handle loads and answers
+    a good graph."""
+    n, src, dst, w = cases.load_case("small_f32_s12")
+    og = oracle.OracleGraph.from_edges(n, src, dst, w)
+    adjp, adj, ww = og.csr()
+    want = og.closure_topk(3000)[0]["slack"]
+    with cpg_b200.CpGen(division=cpg_b200.DIV_IEEE) as g:
+        a, b, c = adjp.copy(), adj.copy(), ww.copy()
+        g.load_csr(n, a, b, c)
+        a[:] = 0
+        b[:] = -7
+        c[:] = np.nan
+        g.report_paths(3000)
+        assert np.array_equal(g.get_slacks(3000).view(np.uint32), want.view(np.uint32))
+        bad = adj.copy()
+        bad[5] = n + 3
+        g.load_csr(n, adjp, bad, ww)
+        with pytest.raises(cpg_b200.CpgError) as e:
+            g.report_paths(10)
+        assert e.value.status == cpg_b200.CPG_ERR_INVALID
+        with pytest.raises(cpg_b200.CpgError):
+            g.report_paths(10)   # no graph is loaded after the failed build
+        g.load_csr(n, adjp, adj, ww)
+        g.report_paths(3000)
+        assert np.array_equal(g.get_slacks(3000).view(np.uint32), want.view(np.uint32))

@@ -114,6 +114,98 @@ __device__ __forceinline__ unsigned long long warp_sort32(unsigned long long x) 
   return x;
 }
 
+// Bitonic sort of 32 C words held C per lane (element c 32 + lane in x[c]),
+// ascending: exchanges with j >= 32 stay inside a lane, the others are
+// shuffles.
+template <int C>
+__device__ __forceinline__ void warp_sort_regs(unsigned long long (&x)[C]) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 2; k <= 32 * C; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      if (j >= 32) {
+        const int jc = j >> 5;
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+          const int d = c ^ jc;
+          if (d > c) {
+            const bool up = ((c * 32) & k) == 0;
+            const unsigned long long a = x[c], b = x[d];
+            if ((a > b) == up) {
+              x[c] = b;
+              x[d] = a;
+            }
+          }
+        }
+      } else {
+        const bool lower = (lane & j) == 0;
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+          const unsigned long long y = __shfl_xor_sync(0xffffffffu, x[c], j);
+          const bool up = ((c * 32 + lane) & k) == 0;
+          x[c] = (lower == up) ? (x[c] < y ? x[c] : y) : (x[c] > y ? x[c] : y);
+        }
+      }
+    }
+  }
+}
+
+// A row the build left unsorted, for sort_rows_kernel.
+__device__ __forceinline__ void list_long_row(const SfxtParams& p, int v) {
+  p.long_rows[atomicAdd(&p.ctr->n_long, 1)] = v;
+}
+
+// C sort words a lane: the row's (key, position) words sorted in registers,
+// then every lane reads the records of its C output slots before any is
+// written.
+template <int C>
+__device__ __forceinline__ void sort_row_words(DevSidetrack* row, int cnt) {
+  const int lane = threadIdx.x & 31;
+  unsigned long long x[C];
+#pragma unroll
+  for (int c = 0; c < C; ++c) {
+    const int t = c * 32 + lane;
+    x[c] = t < cnt ? sort_word(__ldcg(&row[t].key), t) : ~0ull;
+  }
+  warp_sort_regs<C>(x);
+  DevSidetrack o[C];
+#pragma unroll
+  for (int c = 0; c < C; ++c)
+    if (c * 32 + lane < cnt) o[c] = row[static_cast<int>(x[c] & 0xffffffffu)];
+  __syncwarp();
+#pragma unroll
+  for (int c = 0; c < C; ++c)
+    if (c * 32 + lane < cnt) row[c * 32 + lane] = o[c];
+  __syncwarp();
+}
+
+// Sorts a deviation row of at most 128 entries by (key, position) in
+// registers: one word a lane up to 32 entries, four up to 128.  All lanes
+// call.
+__device__ __forceinline__ void sort_row_regs(DevSidetrack* row, int cnt) {
+  const int lane = threadIdx.x & 31;
+  if (cnt <= 32) {
+    DevSidetrack r;
+    unsigned long long x = ~0ull;
+    if (lane < cnt) {
+      r = row[lane];
+      x = sort_word(r.key, lane);
+    }
+    x = warp_sort32(x);
+    // lane i now holds the i-th smallest; fetch that record from its lane
+    const int src = static_cast<int>(x & 0xffffffffu);
+    DevSidetrack o;
+    o.head = __shfl_sync(0xffffffffu, r.head, src & 31);
+    o.w = __shfl_sync(0xffffffffu, r.w, src & 31);
+    o.dist_head = __shfl_sync(0xffffffffu, r.dist_head, src & 31);
+    o.key = __shfl_sync(0xffffffffu, r.key, src & 31);
+    if (lane < cnt) row[lane] = o;
+    return;
+  }
+  sort_row_words<4>(row, cnt);
+}
+
 // A row of at most 32 edges (one per lane) is sorted in registers and
 // written once, in order (write_row64 does the same up to 64 edges); longer
 // rows are written in edge order and sorted by sort_rows_kernel.  Returns the
@@ -384,8 +476,7 @@ __device__ int build_vertex(const SfxtParams& p, int v, int lvl, bool do_kahn) {
     p.dist[v] = best;
     p.succ[v] = s;
     p.dev_cnt[v] = cnt;
-    if (re - rb > 64 && cnt > 1 && cnt <= kSmemRow)  // left for sort_rows_kernel
-      p.long_rows[atomicAdd(&p.ctr->n_long, 1)] = v;
+    if (re - rb > 64 && cnt > 1 && cnt <= kSmemRow) list_long_row(p, v);
     // the chain-heap insert, one level later, takes v's cheapest deviation
     if (cnt > 0) p.best[v] = top;
     if (kLevel) p.level_of[v] = lvl;
@@ -1271,8 +1362,7 @@ __device__ int build_vertex_polled(const SfxtParams& p, int v) {
     p.dist[v] = best;
     p.succ[v] = s;
     p.dev_cnt[v] = cnt;
-    if (re - rb > 64 && cnt > 1 && cnt <= kSmemRow)  // left for sort_rows_kernel
-      p.long_rows[atomicAdd(&p.ctr->n_long, 1)] = v;
+    if (re - rb > 64 && cnt > 1 && cnt <= kSmemRow) list_long_row(p, v);
     if (cnt > 0) p.best[v] = top;
     p.level_of[v] = lmax;
     // the word carries everything a tail's build reads of v, so it needs
@@ -1622,8 +1712,9 @@ sfxt_dataflow_kernel(SfxtParams p) {
 
 // ------------------------------------------------------------ row sorting
 // Orders each rebuilt vertex's deviation list by (key, edge position): one
-// warp per vertex, a register bitonic network for rows up to 32 and a shared
-// memory one up to kSmemRow.  Longer rows go to sort_big_rows_kernel.
+// warp per vertex, a register bitonic network of one or four words a lane for
+// rows up to 32 or 128, a shared-memory one up to kSmemRow.  Longer rows go
+// to sort_big_rows_kernel.
 constexpr int kSortWarps = 8;
 
 __global__ void __launch_bounds__(kSortWarps * 32)
@@ -1638,62 +1729,40 @@ sort_rows_kernel(const int32_t* rows, const int* n_rows, const int32_t* adjp,
     const int v = rows[i];
     const int cnt = dev_cnt[v];
     DevSidetrack* row = dev + adjp[v];
-    if (cnt <= 32) {
-      DevSidetrack r;
-      unsigned long long x = ~0ull;
-      if (lane < cnt) {
-        r = row[lane];
-        x = sort_word(r.key, lane);
+    if (cnt <= 128) {
+      sort_row_regs(row, cnt);
+      continue;
+    }
+    int n2 = 256;
+    for (int t = lane; t < n2; t += 32) {
+      if (t < cnt) {
+        const DevSidetrack r = row[t];
+        srec[w][t] = r;
+        skey[w][t] = sort_word(r.key, t);
+      } else {
+        skey[w][t] = ~0ull;
       }
-      for (int k = 2; k <= 32; k <<= 1) {
-        for (int j = k >> 1; j > 0; j >>= 1) {
-          const unsigned long long y = __shfl_xor_sync(0xffffffffu, x, j);
-          const bool up = (lane & k) == 0;
-          const bool lower = (lane & j) == 0;
-          x = (lower == up) ? (x < y ? x : y) : (x > y ? x : y);
-        }
-      }
-      // lane i now holds the i-th smallest; fetch that record from its lane
-      const int src = static_cast<int>(x & 0xffffffffu);
-      DevSidetrack o;
-      o.head = __shfl_sync(0xffffffffu, r.head, src & 31);
-      o.w = __shfl_sync(0xffffffffu, r.w, src & 31);
-      o.dist_head = __shfl_sync(0xffffffffu, r.dist_head, src & 31);
-      o.key = __shfl_sync(0xffffffffu, r.key, src & 31);
-      if (lane < cnt) row[lane] = o;
-    } else {
-      int n2 = 64;
-      while (n2 < cnt) n2 <<= 1;
-      for (int t = lane; t < n2; t += 32) {
-        if (t < cnt) {
-          const DevSidetrack r = row[t];
-          srec[w][t] = r;
-          skey[w][t] = sort_word(r.key, t);
-        } else {
-          skey[w][t] = ~0ull;
-        }
-      }
-      __syncwarp();
-      for (int k = 2; k <= n2; k <<= 1) {
-        for (int j = k >> 1; j > 0; j >>= 1) {
-          for (int t = lane; t < n2; t += 32) {
-            const int u = t ^ j;
-            if (u > t) {
-              const unsigned long long a = skey[w][t], b = skey[w][u];
-              const bool asc = (t & k) == 0;
-              if ((a > b) == asc) {
-                skey[w][t] = b;
-                skey[w][u] = a;
-              }
+    }
+    __syncwarp();
+    for (int k = 2; k <= n2; k <<= 1) {
+      for (int j = k >> 1; j > 0; j >>= 1) {
+        for (int t = lane; t < n2; t += 32) {
+          const int u = t ^ j;
+          if (u > t) {
+            const unsigned long long a = skey[w][t], b = skey[w][u];
+            const bool asc = (t & k) == 0;
+            if ((a > b) == asc) {
+              skey[w][t] = b;
+              skey[w][u] = a;
             }
           }
-          __syncwarp();
         }
+        __syncwarp();
       }
-      for (int t = lane; t < cnt; t += 32)
-        row[t] = srec[w][static_cast<int>(skey[w][t] & 0xffffffffu)];
-      __syncwarp();
     }
+    for (int t = lane; t < cnt; t += 32)
+      row[t] = srec[w][static_cast<int>(skey[w][t] & 0xffffffffu)];
+    __syncwarp();
   }
 }
 

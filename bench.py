@@ -939,9 +939,34 @@ def run_profile_case(args):
     (suffix tree + engine) on the same workload at --k.  --profile-pins N
     scales the workload's generator down to N pins (same levels, degree and
     delays; sources and sinks in proportion), for captures that must stay
-    small; --form batched runs one warm-up and one measured batched step."""
+    small; --form batched runs one warm-up and one measured batched step;
+    --form e2e runs two end-to-end steps (CSR upload from pinned host buffers,
+    query, cost read-back), the first a warm-up."""
     import cpg_b200
     import cases
+    if args.form == "e2e":
+        import torch
+        c = cases.CASES[WORKLOAD]
+        dag = cpg_b200.generate(cpg_b200.gen_params(**c["gen"]))
+        with cpg_b200.CpGen() as g:
+            g.load_dag(dag)
+            adjp, adj, w = g.get_csr()
+            n = g.num_verts()
+            keep = []
+            for a in (adjp, adj, w, np.zeros(args.k, np.float32)):
+                t = torch.empty(a.size, dtype={np.int32: torch.int32,
+                                               np.float32: torch.float32}[a.dtype.type],
+                                pin_memory=True)
+                t.numpy()[:] = a
+                keep.append(t)
+            p_adjp, p_adj, p_w, out = (t.numpy() for t in keep)
+            for _ in range(2):
+                g.load_csr(n, p_adjp, p_adj, p_w)
+                g.report_paths(args.k)
+                g.get_slacks(args.k, out=out)
+            print(json.dumps({"profile_case": "e2e", "n": n, "m": int(adj.size), "k": args.k,
+                              **g.stats()}))
+        return
     if args.form == "batched":
         # the batch with the level-synchronous build, the autotuner's pick
         dags, ks = batch_workload()
@@ -983,7 +1008,8 @@ def main():
     ap.add_argument("--profile-pins", type=int, default=0,
                     help="profile case: scale the workload down to this many pins")
     ap.add_argument("--form", default="plain",
-                    choices=["plain", "batched", "served", "density", "config1", "bvss", "ingest"])
+                    choices=["plain", "batched", "served", "density", "config1", "bvss", "ingest",
+                             "e2e"])
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="batched form: skip cpg_batch_autotune before timing")
     ap.add_argument("--served-queries", type=int, default=5000)

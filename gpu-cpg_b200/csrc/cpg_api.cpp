@@ -973,6 +973,7 @@ Status engine_prepare(cpg_handle* h, const std::vector<EngineQuery>& qs,
     // no host-to-device copy: a large upload on another stream would hold it
     CK(launch_set_queries(P<EngineQuery>(h->d_equery), qs.data(), static_cast<int>(nq), h->stream),
        "queries");
+    h->stats.kernel_launches += 1;
     return CPG_OK;
   }
   CK(cudaMemcpyAsync(h->d_equery.p, qs.data(), nq * sizeof(EngineQuery),

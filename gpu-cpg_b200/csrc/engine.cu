@@ -544,6 +544,41 @@ __device__ bool run_select(const EngineParams& p, unsigned long long n_paths,
   return true;
 }
 
+// Block-wide appends to two piles (all threads of the block call): this
+// thread's slot in pile A (if a) and in pile B (if b), with one reservation
+// per block and pile instead of one per warp, since every block appends to
+// the same two counters.
+__device__ __forceinline__ void block_append2(unsigned long long* ca, bool a,
+                                              unsigned long long* cb, bool b,
+                                              unsigned long long& sa, unsigned long long& sb) {
+  __shared__ unsigned int s_w[kEngWarps];        // per warp: count A << 16 | count B
+  __shared__ unsigned long long s_base[2];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const unsigned ma = __ballot_sync(0xffffffffu, a), mb = __ballot_sync(0xffffffffu, b);
+  if (lane == 0) s_w[wid] = (static_cast<unsigned>(__popc(ma)) << 16) | __popc(mb);
+  __syncthreads();
+  if (wid == 0) {
+    const unsigned x = lane < kEngWarps ? s_w[lane] : 0u;
+    unsigned incl = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane < kEngWarps) s_w[lane] = incl - x;
+    if (lane == 31) {
+      const unsigned ta = incl >> 16, tb = incl & 0xffffu;
+      s_base[0] = ta ? atomicAdd(ca, static_cast<unsigned long long>(ta)) : 0ull;
+      s_base[1] = tb ? atomicAdd(cb, static_cast<unsigned long long>(tb)) : 0ull;
+    }
+  }
+  __syncthreads();
+  const unsigned pre = s_w[wid];
+  sa = s_base[0] + (pre >> 16) + __popc(ma & lanemask_lt());
+  sb = s_base[1] + (pre & 0xffffu) + __popc(mb & lanemask_lt());
+  __syncthreads();  // s_w and s_base are reused by the next call
+}
+
 // ------------------------------------------------------------------ closure
 // One reservation per warp for n items per lane (all lanes call): returns
 // this lane's first slot.
@@ -947,13 +982,14 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
     STAMP(2);
     // E. promote pending items under their query's limit
     {
-      const unsigned long long pad = (n_pend + 31) & ~31ull;
       const bool single = p.nq == 1;
       const int mode0 = single ? __ldcg(&p.q[0].mode) : 0;
       const int done0 = single ? __ldcg(&p.q[0].done) : 0;
       const float lim0 = single ? __ldcg(&p.q[0].lim) : 0.f;
       unsigned acc_n = 0, acc_nz = 0;
-      for (unsigned long long i = tid; i < pad; i += nth) {
+      // block-uniform trip count: the appends synchronise the block
+      for (unsigned long long b0 = tid - threadIdx.x; b0 < n_pend; b0 += nth) {
+        const unsigned long long i = b0 + threadIdx.x;
         bool take = false, keep = false;
         Item it;
         it.cost = 0.f;
@@ -966,12 +1002,12 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
           take = mode != 0 && it.cost <= (single ? lim0 : __ldcg(&Q.lim));
           keep = !take && !done;
         }
-        const unsigned long long a = warp_append(&p.ctr->frontier[0], take);
+        unsigned long long a = 0, b = 0;
+        block_append2(&p.ctr->frontier[0], take, &p.ctr->pend_out, keep, a, b);
         if (take) {
           if (a < p.front_cap) p.front[0][a] = it;
           else eng_fail(p, kDevCapacity);
         }
-        const unsigned long long b = warp_append(&p.ctr->pend_out, keep);
         if (keep) {
           if (b < p.pend_cap) pend_next[b] = it;
           else eng_fail(p, kDevCapacity);

@@ -1065,9 +1065,10 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
       p.ctr->key_max = 0u;
     }
     ENG_SYNC();
-    const unsigned long long pad = (n_paths + 31) & ~31ull;
     unsigned kmin = 0xffffffffu, kmax = 0u;
-    for (unsigned long long i = tid; i < pad; i += nth) {
+    // block-uniform trip count: the appends synchronise the block
+    for (unsigned long long b0 = tid - threadIdx.x; b0 < n_paths; b0 += nth) {
+      const unsigned long long i = b0 + threadIdx.x;
       bool lt = false, eq = false;
       unsigned key = 0;
       if (i < n_paths) {
@@ -1078,8 +1079,8 @@ __global__ void __launch_bounds__(kEngThreads) engine_kernel(EngineParams p) {
           eq = key == kT;
         }
       }
-      const unsigned long long a = warp_append(&p.ctr->out_below, lt);
-      const unsigned long long b = warp_append(&p.ctr->out_at, eq);
+      unsigned long long a = 0, b = 0;
+      block_append2(&p.ctr->out_below, lt, &p.ctr->out_at, eq, a, b);
       if (lt && a < k_out) {
         p.keys[0][a] = key;
         p.vals[0][a] = static_cast<unsigned>(i);

@@ -650,8 +650,7 @@ template <bool kPublish>
 __device__ __forceinline__ void heap_store(const SfxtParams& p, int v, int root, int size) {
   p.ht_root[v] = root;
   if (kPublish) {
-    __threadfence();
-    *reinterpret_cast<volatile int*>(p.ht_size + v) = size;
+    st_release(p.ht_size + v, size);  // the heap's nodes and root before its size
   } else {
     p.ht_size[v] = size;
   }
@@ -852,7 +851,7 @@ __device__ bool heap_phase(const SfxtParams& p) {
     while (__any_sync(0xffffffffu, pending)) {
       bool ready = false;
       if (pending)
-        ready = s < 0 || *reinterpret_cast<const volatile int*>(p.ht_size + s) >= 0;
+        ready = s < 0 || ld_acquire(p.ht_size + s) >= 0;  // and the heap's nodes after it
       if (!__any_sync(0xffffffffu, ready)) {
         ++it;
         const bool bail = __any_sync(0xffffffffu, it > p.spin_limit ||
@@ -865,7 +864,6 @@ __device__ bool heap_phase(const SfxtParams& p) {
         __nanosleep(32);
         continue;
       }
-      __threadfence();  // the successors' heaps before their nodes are read
       heap_insert_lanes<true>(p, ready ? v : -1);
       pending = pending && !ready;
     }
@@ -1114,8 +1112,7 @@ __device__ __forceinline__ int wait_slot(const SfxtParams& p, int s, bool acquir
 __device__ __forceinline__ bool wait_heap(const SfxtParams& p, int s) {
   if (s < 0) return true;
   unsigned int it = 0;
-  const volatile int* hs = p.ht_size + s;
-  while (*hs < 0) {
+  while (ld_acquire(p.ht_size + s) < 0) {
     if (++it > p.spin_limit ||
         ((it & 31) == 0 && *reinterpret_cast<volatile int*>(&p.ctr->err) != kDevOk)) {
       atomicCAS(&p.ctr->err, kDevOk, kDevTimeout);
@@ -1123,7 +1120,6 @@ __device__ __forceinline__ bool wait_heap(const SfxtParams& p, int s) {
     }
     __nanosleep(32);
   }
-  __threadfence();
   return true;
 }
 

@@ -1131,10 +1131,8 @@ __device__ __forceinline__ unsigned long long ld_dl(const SfxtParams& p, int h) 
   return *reinterpret_cast<const volatile unsigned long long*>(p.dl + h);
 }
 
-__device__ int build_vertex_polled(const SfxtParams& p, int v) {
+__device__ int build_vertex_polled(const SfxtParams& p, int v, int rb, int re, DevEdge ed0) {
   const int lane = threadIdx.x & 31;
-  const int rb = p.adjp[v];
-  const int re = p.adjp[v + 1];
   int best = INT_MAX;
   int s = -1;
   int cnt = 0;
@@ -1145,8 +1143,9 @@ __device__ int build_vertex_polled(const SfxtParams& p, int v) {
   if (re - rb <= kRegChunks * 32) {
     DevEdge ed[kRegChunks];
     int dh[kRegChunks];
+    ed[0] = ed0;  // loaded before the push
 #pragma unroll
-    for (int c = 0; c < kRegChunks; ++c) {
+    for (int c = 1; c < kRegChunks; ++c) {
       const int e = rb + c * 32 + lane;
       ed[c].head = -1;
       ed[c].w = 0.f;
@@ -1441,12 +1440,10 @@ __device__ __forceinline__ void queue_push(const SfxtParams& p, bool on, int u) 
 // ready, so a hub (the super-sink's 2,000 fan-in edges, say) costs a few
 // round trips per 256 tails instead of several per 32.
 template <bool kRelease>
-__device__ __forceinline__ void dataflow_push(const SfxtParams& p, int v) {
+__device__ __forceinline__ void dataflow_push(const SfxtParams& p, int v, int ib, int ie) {
   static_assert(kSfxtQueues == 1, "one reservation per pass assumes one queue");
   constexpr int kC = 8;
   const int lane = threadIdx.x & 31;
-  const int ib = p.iadjp[v];
-  const int ie = p.iadjp[v + 1];
   for (int base = ib; base < ie; base += kC * 32) {
     const int nc = min(kC, (ie - base + 31) / 32);  // warp-uniform
     int u[kC];
@@ -1487,9 +1484,17 @@ __device__ __forceinline__ bool dataflow_slot(const SfxtParams& p, int v, bool h
                                               int& max_lvl) {
   const int lane = threadIdx.x & 31;
   if (p.early_push) {
-    // the tails learn of v before it is built; they wait on its word
-    dataflow_push<false>(p, v);
-    const int lvl = build_vertex_polled(p, v);
+    // the tails learn of v before it is built; they wait on its word.  The
+    // build's row offsets are loaded with the push's, in one round trip ...
+    const int ib = p.iadjp[v], ie = p.iadjp[v + 1];
+    const int rb = p.adjp[v], re = p.adjp[v + 1];
+    // ... and the row's first 32 edge words with the push's tails
+    DevEdge ed0;
+    ed0.head = -1;
+    ed0.w = 0.f;
+    if (rb + lane < re) ed0 = p.edges[rb + lane];
+    dataflow_push<false>(p, v, ib, ie);
+    const int lvl = build_vertex_polled(p, v, rb, re, ed0);
     if (lvl < 0) return false;
     max_lvl = max(max_lvl, lvl);
     if (!hp && lane == 0 && wait_heap(p, __ldcg(p.succ + v)))
@@ -1504,7 +1509,7 @@ __device__ __forceinline__ bool dataflow_slot(const SfxtParams& p, int v, bool h
     __threadfence();
     *reinterpret_cast<volatile int*>(p.order + v) = 1;
   }
-  dataflow_push<true>(p, v);
+  dataflow_push<true>(p, v, p.iadjp[v], p.iadjp[v + 1]);
   if (heap_warps == 0 && !hp && lane == 0 && wait_heap(p, __ldcg(p.succ + v)))
     heap_insert<true>(p, v, chunk);
   __syncwarp();

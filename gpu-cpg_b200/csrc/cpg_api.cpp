@@ -53,7 +53,13 @@ struct cpg_handle {
 
   // graph
   bool has_graph = false;
-  bool build_pending = false;  // cpg_load_csr: the device graph build is left to the first use
+  bool build_pending = false;  // cpg_load_csr: the graph's first use waits for its device build
+  // ... which starts at once on this least-priority stream (build_done marks
+  // its end; the source count and head check land in pinned_build)
+  cudaStream_t build_stream = nullptr;
+  cudaEvent_t build_done = nullptr;
+  int32_t* pinned_build = nullptr;
+  bool build_launched = false;
   HostGraph g;          // n, m and the fan-out row offsets only
   int32_t n_srcs = 0;
   int32_t max_outdeg = 0;
@@ -281,11 +287,13 @@ Status setup_bvss(cpg_handle* h, int32_t n, const int32_t* adjp, const int32_t* 
 // Upload a fan-out CSR and build the rest of the graph on the device: edge
 // words, fan-in CSR and source list.  The host keeps only the row offsets.
 Status finish_graph(cpg_handle* h);
+Status start_graph_build(cpg_handle* h);
 
 // Uploads a fan-out CSR and builds the device graph from it.  defer: return
-// once the copies have read the caller's buffers and leave the build to the
-// graph's first use (ready_graph), so that a caller streaming uploads through
-// several handles overlaps this one's copies with another's query.
+// once the copies have read the caller's buffers, with the build started on
+// the handle's least-priority stream; the graph's first use (ready_graph)
+// waits for it.  A caller streaming uploads through several handles then
+// overlaps this one's copies and build with another's query.
 Status upload_graph(cpg_handle* h, int32_t n, int32_t m, const int32_t* adjp,
                     const int32_t* adj, const float* w, bool defer = false) {
   if (n < 0 || m < 0 || !adjp || (m > 0 && (!adj || !w)))
@@ -293,6 +301,12 @@ Status upload_graph(cpg_handle* h, int32_t n, int32_t m, const int32_t* adjp,
   if (adjp[0] != 0 || adjp[n] != m)
     return fail(h, CPG_ERR_INVALID, "CSR offsets must start at 0 and end at m");
   CK(cudaSetDevice(h->device), "cudaSetDevice");
+  if (h->build_launched) {
+    // an earlier upload's build still reads the staging and writes the graph
+    CK(cudaEventSynchronize(h->build_done), "graph build");
+    h->build_launched = false;
+  }
+  h->build_pending = false;
   h->has_graph = false;
   h->multi_graph = false;  // cpg_batch_commit sets it after the upload
   h->relabeled = false;    // so does it this
@@ -405,18 +419,18 @@ Status upload_graph(cpg_handle* h, int32_t n, int32_t m, const int32_t* adjp,
     // the copies read the caller's buffers (and big_off / big_rows above)
     CK(cudaStreamSynchronize(s), "upload");
     h->build_pending = true;
-    return CPG_OK;
+    return start_graph_build(h);
   }
   return finish_graph(h);
 }
 
 // The device graph build of an upload (edge words, fan-in CSR, sources) from
 // the staged adjacency and delays, and the head range check.
-Status finish_graph(cpg_handle* h) {
-  h->build_pending = false;
+// Enqueues the device graph build on stream s; its source count and head
+// check (two ints) go to hn.
+Status enqueue_graph_build(cpg_handle* h, cudaStream_t s, int32_t* hn) {
   const int32_t n = h->g.n, m = h->g.m;
   const size_t nn = static_cast<size_t>(n), mm = static_cast<size_t>(m);
-  cudaStream_t s = h->stream;
   int32_t* stage_adj = reinterpret_cast<int32_t*>(h->d_dev.p);
   float* stage_w = reinterpret_cast<float*>(stage_adj + mm);
   int32_t* nsrc_dev = P<int32_t>(h->d_srcs) + nn;
@@ -424,9 +438,33 @@ Status finish_graph(cpg_handle* h) {
                         P<DevEdge>(h->d_edges), P<int32_t>(h->d_iadjp),
                         P<int32_t>(h->d_iadj), P<int32_t>(h->d_srcs), nsrc_dev,
                         P<int32_t>(h->d_deps), s), "build graph");
-  int32_t* hn = static_cast<int32_t*>(h->pinned);
   CK(cudaMemcpyAsync(hn, nsrc_dev, 8, cudaMemcpyDeviceToHost, s), "D2H sources");
-  CK(cudaStreamSynchronize(s), "upload");
+  return CPG_OK;
+}
+
+// Starts a deferred upload's build on the handle's least-priority stream, so
+// it runs on whatever SMs the other streams leave idle (another handle's
+// query, say); the graph's first use waits for it.
+Status start_graph_build(cpg_handle* h) {
+  if (!h->build_stream) {
+    int least = 0, greatest = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&least, &greatest), "stream priorities");
+    CK(cudaStreamCreateWithPriority(&h->build_stream, cudaStreamNonBlocking, least),
+       "build stream");
+    CK(cudaEventCreateWithFlags(&h->build_done, cudaEventDisableTiming), "event");
+    void* pb = nullptr;
+    CK(cudaMallocHost(&pb, 64), "pinned");
+    h->pinned_build = static_cast<int32_t*>(pb);
+  }
+  Status st = enqueue_graph_build(h, h->build_stream, h->pinned_build);
+  if (st != CPG_OK) return st;
+  CK(cudaEventRecord(h->build_done, h->build_stream), "event");
+  h->build_launched = true;
+  return CPG_OK;
+}
+
+// The host side of a build: the head check, the source count and order.
+Status complete_graph_build(cpg_handle* h, const int32_t* hn) {
   if (hn[1] != 0) {
     h->has_graph = false;
     return fail(h, CPG_ERR_INVALID, "edge head out of range");
@@ -443,13 +481,27 @@ Status finish_graph(cpg_handle* h) {
   return CPG_OK;
 }
 
-// A loaded graph, built on the device (the build of a deferred upload runs
-// here, on the handle's stream).
+Status finish_graph(cpg_handle* h) {
+  h->build_pending = false;
+  h->build_launched = false;
+  int32_t* hn = static_cast<int32_t*>(h->pinned);
+  Status st = enqueue_graph_build(h, h->stream, hn);
+  if (st != CPG_OK) return st;
+  CK(cudaStreamSynchronize(h->stream), "upload");
+  return complete_graph_build(h, hn);
+}
+
+// A loaded graph, built on the device: the build of a deferred upload, begun
+// on the build stream, is waited for here (or run here if it was not begun).
 Status ready_graph(cpg_handle* h) {
   if (!h->has_graph) return fail(h, CPG_ERR_STATE, "no graph loaded");
   if (!h->build_pending) return CPG_OK;
   CK(cudaSetDevice(h->device), "cudaSetDevice");
-  return finish_graph(h);
+  if (!h->build_launched) return finish_graph(h);
+  h->build_pending = false;
+  h->build_launched = false;
+  CK(cudaEventSynchronize(h->build_done), "graph build");
+  return complete_graph_build(h, h->pinned_build);
 }
 
 Status load_edgelist(cpg_handle* h, const EdgeList& el) {
@@ -1234,6 +1286,7 @@ cpg_status cpg_destroy(cpg_handle* h) {
   if (!h) return CPG_ERR_INVALID;
   cudaSetDevice(h->device);
   cudaStreamSynchronize(h->stream);
+  if (h->build_stream) cudaStreamSynchronize(h->build_stream);  // a graph build still running
   DevMem* all[] = {&h->d_adjp, &h->d_edges, &h->d_iadjp, &h->d_iadj, &h->d_srcs,
                    &h->d_big_off, &h->d_big_tmp, &h->d_big_rows, &h->d_order, &h->d_lvlp,
                    &h->d_level_of, &h->d_dist, &h->d_succ, &h->d_dev_cnt,
@@ -1253,6 +1306,11 @@ cpg_status cpg_destroy(cpg_handle* h) {
   for (auto& e : h->ev)
     if (e) cudaEventDestroy(e);
   if (h->pinned) cudaFreeHost(h->pinned);
+  if (h->build_stream) {
+    cudaStreamDestroy(h->build_stream);
+    cudaEventDestroy(h->build_done);
+    cudaFreeHost(h->pinned_build);
+  }
   if (h->stage) {
     cudaFreeHost(h->stage);
     for (auto& e : h->stage_ev)

@@ -157,10 +157,13 @@ __global__ void sources_kernel(const int32_t* indeg, int32_t n, int32_t* srcs,
   }
 }
 
+// Blocks for n threads' worth of work: one element per thread (short blocks,
+// so a build running beside another stream's kernels gives SMs back soon),
+// capped far above what the loops need.
 int grid_of(int64_t n, int threads) {
   int64_t b = (n + threads - 1) / threads;
   if (b < 1) b = 1;
-  if (b > 148 * 32) b = 148 * 32;
+  if (b > (int64_t{1} << 20)) b = int64_t{1} << 20;
   return static_cast<int>(b);
 }
 

@@ -173,10 +173,11 @@ cpg_status cpg_load_edges(cpg_handle* h, int32_t n, int32_t m,
                           const float* w);
 /* Same graph from a fan-out CSR (_h_fanout_adjp/_adjncy/_wgts).  Returns once
  * the host-to-device copies have read the caller's buffers (they may be
- * reused at once); the device graph (edge words, fan-in CSR, sources) is
- * built by the first call that uses it, on the handle's stream, so a caller
- * streaming graphs through several handles overlaps one handle's upload with
- * another's query.  A head outside [0, n) is reported by that first call
+ * reused at once).  The device graph (edge words, fan-in CSR, sources) is
+ * then built on a least-priority stream the handle owns, and the first call
+ * that uses the graph waits for it, so a caller streaming graphs through
+ * several handles overlaps one handle's upload and build with another's
+ * query.  A head outside [0, n) is reported by that first call
  * (CPG_ERR_INVALID, and the handle then holds no graph). */
 cpg_status cpg_load_csr(cpg_handle* h, int32_t n, int32_t m,
                         const int32_t* adjp, const int32_t* adjncy,

@@ -1477,27 +1477,39 @@ __device__ __forceinline__ void dataflow_push(const SfxtParams& p, int v, int ib
 }
 
 // One taken queue slot of the dataflow build: v's Kahn push and build (in
-// either order), then its chain-heap insert unless the heap phase or the heap
-// workers do it.  False when a wait ran out (warp-uniform).
-__device__ __forceinline__ bool dataflow_slot(const SfxtParams& p, int v, bool hp,
-                                              int heap_warps, unsigned long long* chunk,
-                                              int& max_lvl) {
+// either order), then its chain-heap insert unless the heap phase (kHp) or
+// the heap workers do it.  False when a wait ran out (warp-uniform).
+template <bool kHp>
+__device__ __forceinline__ bool dataflow_slot(const SfxtParams& p, int v, int heap_warps,
+                                              unsigned long long* chunk, int& max_lvl) {
   const int lane = threadIdx.x & 31;
   if (p.early_push) {
-    // the tails learn of v before it is built; they wait on its word.  The
-    // build's row offsets are loaded with the push's, in one round trip ...
+    // the tails learn of v before it is built; they wait on its word.
+    // Graphs big enough for the heap phase keep a backlog of queued vertices
+    // through the wave, which the warps' round trips bound: the build's row
+    // offsets are loaded with the push's, in one round trip, and the row's
+    // first 32 edge words with the push's tails.  Smaller graphs leave warps
+    // waiting on pushes: the push goes first, carrying no loads of the build.
     const int ib = p.iadjp[v], ie = p.iadjp[v + 1];
-    const int rb = p.adjp[v], re = p.adjp[v + 1];
-    // ... and the row's first 32 edge words with the push's tails
+    int rb = 0, re = 0;
     DevEdge ed0;
     ed0.head = -1;
     ed0.w = 0.f;
-    if (rb + lane < re) ed0 = p.edges[rb + lane];
+    if (kHp) {
+      rb = p.adjp[v];
+      re = p.adjp[v + 1];
+      if (rb + lane < re) ed0 = p.edges[rb + lane];
+    }
     dataflow_push<false>(p, v, ib, ie);
+    if (!kHp) {
+      rb = p.adjp[v];
+      re = p.adjp[v + 1];
+      if (rb + lane < re) ed0 = p.edges[rb + lane];
+    }
     const int lvl = build_vertex_polled(p, v, rb, re, ed0);
     if (lvl < 0) return false;
     max_lvl = max(max_lvl, lvl);
-    if (!hp && lane == 0 && wait_heap(p, __ldcg(p.succ + v)))
+    if (!kHp && lane == 0 && wait_heap(p, __ldcg(p.succ + v)))
       heap_insert<true>(p, v, chunk);
     __syncwarp();
     return true;
@@ -1510,10 +1522,45 @@ __device__ __forceinline__ bool dataflow_slot(const SfxtParams& p, int v, bool h
     *reinterpret_cast<volatile int*>(p.order + v) = 1;
   }
   dataflow_push<true>(p, v, p.iadjp[v], p.iadjp[v + 1]);
-  if (heap_warps == 0 && !hp && lane == 0 && wait_heap(p, __ldcg(p.succ + v)))
+  if (heap_warps == 0 && !kHp && lane == 0 && wait_heap(p, __ldcg(p.succ + v)))
     heap_insert<true>(p, v, chunk);
   __syncwarp();
   return true;
+}
+
+// A build warp's loop over the work queue (warp wib of its CTA).
+// Claimed slots (claim_sets S > 0): a free warp claims the next slot of its
+// claim set (slots q, q + S, ...), so a slot that fills while some warp is
+// still building waits for nobody: any idle warp of the set takes it.  The S
+// counters spread the claims (one atomic per vertex).  Static slots (S = 0):
+// build warp bw serves queue bw % kSfxtQueues, taking every nwq-th slot.
+template <bool kHp>
+__device__ __forceinline__ void dataflow_build_warp(const SfxtParams& p, int wib, int build_warps,
+                                                    int heap_warps, unsigned long long* chunk,
+                                                    int& max_lvl) {
+  const int lane = threadIdx.x & 31;
+  const int nbw = gridDim.x * build_warps;
+  const int bw = blockIdx.x * build_warps + wib;
+  const int S = p.claim_sets;
+  const int q = S > 0 ? bw % S : bw % kSfxtQueues;
+  const int cnt = S > 0 ? (p.n > q ? (p.n - 1 - q) / S + 1 : 0) : queue_count(p, q);
+  const int nwq = (nbw - q + kSfxtQueues - 1) / kSfxtQueues;
+  const int seg0 = q * queue_seg(p);
+  for (int k = bw / kSfxtQueues;; k += nwq) {
+    int slot;
+    if (S > 0) {
+      int t = 0;
+      if (lane == 0) t = atomicAdd(&p.ctr->claim[q][0], 1);
+      t = __shfl_sync(0xffffffffu, t, 0);
+      if (t >= cnt) break;
+      slot = t * S + q;
+    } else {
+      if (k >= cnt) break;
+      slot = seg0 + k;
+    }
+    const int v = wait_slot(p, slot, !p.early_push);
+    if (v < 0 || !dataflow_slot<kHp>(p, v, heap_warps, chunk, max_lvl)) break;
+  }
 }
 
 __global__ void __launch_bounds__(kSfxtThreads)
@@ -1560,34 +1607,11 @@ sfxt_dataflow_kernel(SfxtParams p) {
   const bool hp = p.heap_phase == 2 ||
                   (p.heap_phase == 1 && p.n >= 128 * static_cast<int>(gridDim.x) * build_warps);
   if (wib < build_warps) {
-    const int nbw = gridDim.x * build_warps;
-    const int bw = blockIdx.x * build_warps + wib;
-    // Claimed slots (claim_sets S > 0): a free warp claims the next slot of
-    // its claim set (slots q, q + S, ...), so a slot that fills while some
-    // warp is still building waits for nobody: any idle warp of the set
-    // takes it.  The S counters spread the claims (one atomic per vertex).
-    // Static slots (S = 0): build warp bw serves queue bw % kSfxtQueues,
-    // taking every nwq-th slot.
-    const int S = p.claim_sets;
-    const int q = S > 0 ? bw % S : bw % kSfxtQueues;
-    const int cnt = S > 0 ? (p.n > q ? (p.n - 1 - q) / S + 1 : 0) : queue_count(p, q);
-    const int nwq = (nbw - q + kSfxtQueues - 1) / kSfxtQueues;
-    const int seg0 = q * queue_seg(p);
-    for (int k = bw / kSfxtQueues;; k += nwq) {
-      int slot;
-      if (S > 0) {
-        int t = 0;
-        if (lane == 0) t = atomicAdd(&p.ctr->claim[q][0], 1);
-        t = __shfl_sync(0xffffffffu, t, 0);
-        if (t >= cnt) break;
-        slot = t * S + q;
-      } else {
-        if (k >= cnt) break;
-        slot = seg0 + k;
-      }
-      const int v = wait_slot(p, slot, !p.early_push);
-      if (v < 0 || !dataflow_slot(p, v, hp, heap_warps, chunk, max_lvl)) break;
-    }
+    // one copy of the loop per regime, each compiled for its own order
+    if (hp)
+      dataflow_build_warp<true>(p, wib, build_warps, heap_warps, chunk, max_lvl);
+    else
+      dataflow_build_warp<false>(p, wib, build_warps, heap_warps, chunk, max_lvl);
   } else {
     const int nhl = gridDim.x * heap_warps * 32;
     const int seg = queue_seg(p);

@@ -490,7 +490,7 @@ extern "C" cpg_status cpg_select_topk_noalloc(const float* d_costs, int64_t n,
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
     if (!g_noalloc_ptr[dev]) {
       // one-time set-up on this device (the current one): the device address
-      // of the static scratch; do the first call before any stream capture
+      // of the static scratch
       void* ptr = nullptr;
       if (cudaGetSymbolAddress(&ptr, g_topk_scratch) != cudaSuccess || !ptr) {
         cudaGetLastError();

@@ -413,11 +413,14 @@ cpg_status cpg_select_topk(const float* d_costs, int64_t n, int64_t k,
  *    n < 2^32.
  *  - The scratch (about 4.3 MiB) is reserved on every GPU that loads the
  *    library and kept until the process exits.
+ *  - No call can run inside a stream capture: every call reads the count of
+ *    non-zero costs back to the host partway through and synchronises
+ *    `stream` before it returns.
  *  - The first call on a device looks up the scratch's device address (with
- *    that device current); make it before any stream capture.  The address
- *    is kept for the life of the process: after cudaDeviceReset on that
- *    device the module is loaded again and the kept address is stale, so do
- *    not call this entry point across a device reset.
+ *    that device current).  The address is kept for the life of the
+ *    process: after cudaDeviceReset on that device the module is loaded
+ *    again and the kept address is stale, so do not call this entry point
+ *    across a device reset.
  *  - All calls share the one array: calls that overlap on the GPU (from two
  *    streams or threads at once) race and must be serialised by the caller.
  *  - Calls no cudaMalloc/cudaFree; returns after the result is written. */

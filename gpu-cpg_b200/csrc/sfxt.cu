@@ -1131,7 +1131,8 @@ __device__ __forceinline__ unsigned long long ld_dl(const SfxtParams& p, int h) 
   return *reinterpret_cast<const volatile unsigned long long*>(p.dl + h);
 }
 
-__device__ int build_vertex_polled(const SfxtParams& p, int v, int rb, int re, DevEdge ed0) {
+__device__ int build_vertex_polled(const SfxtParams& p, int v, int rb, int re, DevEdge ed0,
+                                   unsigned long long dl0) {
   const int lane = threadIdx.x & 31;
   int best = INT_MAX;
   int s = -1;
@@ -1143,7 +1144,7 @@ __device__ int build_vertex_polled(const SfxtParams& p, int v, int rb, int re, D
   if (re - rb <= kRegChunks * 32) {
     DevEdge ed[kRegChunks];
     int dh[kRegChunks];
-    ed[0] = ed0;  // loaded before the push
+    ed[0] = ed0;  // loaded before the push (dl0: its head's word, or ~0)
 #pragma unroll
     for (int c = 1; c < kRegChunks; ++c) {
       const int e = rb + c * 32 + lane;
@@ -1156,7 +1157,8 @@ __device__ int build_vertex_polled(const SfxtParams& p, int v, int rb, int re, D
     for (int c = 0; c < kRegChunks; ++c) {
       dh[c] = INT_MAX;
       if (ed[c].head >= 0) {
-        const unsigned long long x = ld_dl(p, ed[c].head);
+        // a published word never changes: one read before the push stands
+        const unsigned long long x = c == 0 && dl0 != kNone ? dl0 : ld_dl(p, ed[c].head);
         if (x == kNone) {
           pending |= 1u << c;
         } else {
@@ -1439,8 +1441,15 @@ __device__ __forceinline__ void queue_push(const SfxtParams& p, bool on, int u) 
 // decrements, then one queue reservation for all the tails that became
 // ready, so a hub (the super-sink's 2,000 fan-in edges, say) costs a few
 // round trips per 256 tails instead of several per 32.
-template <bool kRelease>
-__device__ __forceinline__ void dataflow_push(const SfxtParams& p, int v, int ib, int ie) {
+// `before_counts` runs once, between the first pass's tail loads and its
+// decrements, so loads it issues travel with the decrements.
+struct NoHook {
+  __device__ __forceinline__ void operator()() const {}
+};
+
+template <bool kRelease, class Hook = NoHook>
+__device__ __forceinline__ void dataflow_push(const SfxtParams& p, int v, int ib, int ie,
+                                              Hook before_counts = Hook()) {
   static_assert(kSfxtQueues == 1, "one reservation per pass assumes one queue");
   constexpr int kC = 8;
   const int lane = threadIdx.x & 31;
@@ -1452,6 +1461,7 @@ __device__ __forceinline__ void dataflow_push(const SfxtParams& p, int v, int ib
       const int e = base + c * 32 + lane;
       u[c] = c < nc && e < ie ? p.iadj[e] : -1;
     }
+    if (base == ib) before_counts();
     if (kRelease) __threadfence();  // release: v's dist and level before the counts
     unsigned ready = 0;  // bit c: this lane's tail of chunk c reached zero
 #pragma unroll
@@ -1495,18 +1505,23 @@ __device__ __forceinline__ bool dataflow_slot(const SfxtParams& p, int v, int he
     DevEdge ed0;
     ed0.head = -1;
     ed0.w = 0.f;
+    unsigned long long dl0 = ~0ull;
     if (kHp) {
       rb = p.adjp[v];
       re = p.adjp[v + 1];
       if (rb + lane < re) ed0 = p.edges[rb + lane];
-    }
-    dataflow_push<false>(p, v, ib, ie);
-    if (!kHp) {
+      // the first heads' words are read with the push's decrements (with a
+      // backlog the heads are almost always built by then)
+      dataflow_push<false>(p, v, ib, ie, [&] {
+        if (ed0.head >= 0) dl0 = ld_dl(p, ed0.head);
+      });
+    } else {
+      dataflow_push<false>(p, v, ib, ie);
       rb = p.adjp[v];
       re = p.adjp[v + 1];
       if (rb + lane < re) ed0 = p.edges[rb + lane];
     }
-    const int lvl = build_vertex_polled(p, v, rb, re, ed0);
+    const int lvl = build_vertex_polled(p, v, rb, re, ed0, dl0);
     if (lvl < 0) return false;
     max_lvl = max(max_lvl, lvl);
     if (!kHp && lane == 0 && wait_heap(p, __ldcg(p.succ + v)))

@@ -100,3 +100,56 @@ def test_cpp_shim_compiles():
     r = subprocess.run([gxx, "-std=c++17", "-fsyntax-only", "-I", os.path.join(ROOT, "include"), src],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+# ctypes mirror in cpg_b200.py -> the C typedef it must match byte for byte
+_STRUCTS = {
+    "Options": "cpg_options", "PathNode": "cpg_path_node", "Stats": "cpg_stats",
+    "BatchStats": "cpg_batch_stats", "ServerOptions": "cpg_server_options",
+    "ServerStats": "cpg_server_stats", "BvssInfo": "cpg_bvss_info",
+    "BvssOpts": "cpg_bvss_opts", "BvssRunStats": "cpg_bvss_run_stats",
+    "GenParams": "cpg_gen_params",
+}
+
+
+def test_ctypes_structs_match_header_layout(tmp_path):
+    """Every struct the Python binding passes through the C ABI has the
+    header's size and field offsets (a field added on one side only would
+    silently shift the ones after it)."""
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("no gcc")
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "cpg.h"', "int main(void) {"]
+    expect = []
+    for py, c in _STRUCTS.items():
+        cls = getattr(cpg_b200, py)
+        lines.append(f'  printf("{py} size %zu\\n", sizeof({c}));')
+        expect.append(f"{py} size {C.sizeof(cls)}")
+        for f in cls._fields_:
+            name = f[0]
+            cname = name[:-1] if name.endswith("_") else name  # from_ -> from
+            lines.append(f'  printf("{py}.{name} %zu\\n", offsetof({c}, {cname}));')
+            expect.append(f"{py}.{name} {getattr(cls, name).offset}")
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    r = subprocess.run([gcc, "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    got = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    got = [g for g in got if g]
+    diff = [(e, g) for e, g in zip(expect, got) if e != g]
+    assert len(got) == len(expect) and not diff, diff
+
+
+def test_options_init_defaults():
+    """cpg_options_init gives the defaults the header documents."""
+    o = cpg_b200.Options()
+    cpg_b200.lib.cpg_options_init(C.byref(o))
+    assert o.device == 0 and not o.stream
+    assert o.division == cpg_b200.DIV_REFERENCE and o.frontier == cpg_b200.FRONTIER_AUTO
+    assert o.hbm_budget_bytes == 0 and o.spin_limit == 0  # no cap; default poll limit
+    assert o.host_stepped == 0 and o.bvss_min_bits == 0 and o.bvss_min_slices == 0
+    assert o.sfxt_level_sync == 0 and o.sfxt_heap_warps == 0 and o.sfxt_late_push == 0
+    assert o.sfxt_heap_mode == 0 and o.sfxt_claim_sets == 0 and o.engine_ctas == 0

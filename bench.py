@@ -57,8 +57,8 @@ METRIC = "K-paths/sec"
 # workload, from the one-pass ncu capture summarised in
 # profiles/sfxt_dataflow_kernel_large400k.md (the suffix-tree build does not
 # depend on K; the engine's figure is its two launches at K = 1e6).
-KERNEL_TRAFFIC = {"sfxt_dataflow_kernel": 708_436_992 + 625_532_672,
-                  "engine_kernel": 732_416 + 102_091_520 + 188_976_128}
+KERNEL_TRAFFIC = {"sfxt_dataflow_kernel": 708_980_736 + 625_738_752,
+                  "engine_kernel": 757_760 + 102_573_056 + 188_904_960}
 
 
 def peaks():

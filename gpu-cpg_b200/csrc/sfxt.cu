@@ -1496,10 +1496,12 @@ __device__ __forceinline__ bool dataflow_slot(const SfxtParams& p, int v, int he
   if (p.early_push) {
     // the tails learn of v before it is built; they wait on its word.
     // Graphs big enough for the heap phase keep a backlog of queued vertices
-    // through the wave, which the warps' round trips bound: the build's row
-    // offsets are loaded with the push's, in one round trip, and the row's
-    // first 32 edge words with the push's tails.  Smaller graphs leave warps
-    // waiting on pushes: the push goes first, carrying no loads of the build.
+    // through most of the wave, so the warps' round trips count: the build's
+    // row offsets are loaded with the push's, in one round trip, and the
+    // row's first 32 edge words with the push's tails.  Smaller graphs leave
+    // warps waiting on pushes: the push goes first, carrying no loads of the
+    // build.  (The push is never deferred past the build: that puts every
+    // build on the level-to-level path.)
     const int ib = p.iadjp[v], ie = p.iadjp[v + 1];
     int rb = 0, re = 0;
     DevEdge ed0;
@@ -1617,8 +1619,9 @@ sfxt_dataflow_kernel(SfxtParams p) {
   const int heap_warps = p.heap_warps;  // 0: the build warp inserts the heap itself
   const int build_warps = kSfxtThreads / 32 - heap_warps;
   // The heap phase pays once the build warps have over ~128 vertices each
-  // (measured: it loses 0.3-0.45 ms up to 400,000 vertices, where its chain
-  // of successor heaps is not hidden, and wins 0.35 ms at 1,000,000)
+  // (measured: it loses 0.25-0.45 ms from 200,000 to 400,000 vertices,
+  // where its chain of successor heaps is not hidden, and wins 0.2-0.35 ms
+  // at 1,000,000)
   const bool hp = p.heap_phase == 2 ||
                   (p.heap_phase == 1 && p.n >= 128 * static_cast<int>(gridDim.x) * build_warps);
   if (wib < build_warps) {

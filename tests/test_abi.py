@@ -102,6 +102,29 @@ def test_cpp_shim_compiles():
     assert r.returncode == 0, r.stderr
 
 
+def test_cpp_shim_links_and_fails_loudly_without_device(tmp_path):
+    """The reference-style C++ caller links against the library (every
+    symbol the shim uses resolves) and, with no device, stops with the
+    library's error instead of falling back to anything."""
+    from conftest import gpu_available
+    if gpu_available():
+        pytest.skip("a device is present")
+    gxx = shutil.which("g++")
+    if gxx is None:
+        pytest.skip("no g++")
+    libdir = os.path.dirname(cpg_b200.LIB_PATH)
+    exe = str(tmp_path / "shim_example")
+    r = subprocess.run([gxx, "-std=c++17", "-I", os.path.join(ROOT, "include"),
+                        os.path.join(ROOT, "tests", "cpp", "shim_example.cpp"),
+                        "-L", libdir, "-lcpg_b200", f"-Wl,-rpath,{libdir}", "-o", exe],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    run = subprocess.run([exe, str(tmp_path / "no_graph.txt"), "10"], capture_output=True, text=True)
+    assert run.returncode == 1
+    assert "no cuda device" in run.stderr
+    assert run.stdout == ""
+
+
 # ctypes mirror in cpg_b200.py -> the C typedef it must match byte for byte
 _STRUCTS = {
     "Options": "cpg_options", "PathNode": "cpg_path_node", "Stats": "cpg_stats",
